@@ -1,0 +1,425 @@
+#!/usr/bin/env python
+"""Benchmark of the RA execution layer on B200.
+
+Workload (one step): the filter-project-aggregate scan over a 60M-row fact table of
+Tuple<32,64,64,64,64,8,8> (64-byte rows): select date <= 2475, append the exact int64
+products price*(100-discount) and price*(100-discount)*(100+tax), group by
+(flag1, flag2) into 6 groups with SUM/COUNT.  One fused kernel per step.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+value  = rows/s with the table resident in HBM (3.84 GB per GPU, larger than L2, so no
+         flush is needed between steps), timed with CUDA events, max over ranks.
+e2e    = the same through the public API with the table in pinned host memory: each
+         step copies it to the device, runs the plan and reads the groups back.
+N > 1  = weak scaling: every rank scans its own 60M-row partition; the 6-group partial
+         results are summed with one all-reduce inside each step.
+--impl reference times the reference's own code for this plan (its Tuple.h / select /
+arith / project device code and thrust reduce_by_key, compiled for the host in
+oracle/_ref) on the host cores, or the C oracle where that library is absent.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+ROWS = 60_000_000
+WORKLOAD = ("filter-project-aggregate: 60M rows Tuple<32,64,64,64,64,8,8> (64 B), "
+            "select date<=2475 (~98%), 2 int64 products, group by (flag1,flag2) -> 6 groups SUM/COUNT")
+METRIC = "tuples/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--rows", type=int, default=ROWS)
+    ap.add_argument("--e2e-steps", type=int, default=5)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clock / throttle samples while the timed region runs."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.QUERY,
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sms, maxes, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm, mx = float(parts[1]), float(parts[2])
+            except ValueError:
+                continue
+            sms.append(sm)
+            maxes.append(mx)
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sms) if sms else None,
+                "sm_max_mhz": max(maxes) if maxes else None,
+                "reasons": sorted(reasons), "samples": len(sms)}
+
+
+def measured_peak_hbm():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profiled_traffic(rows):
+    """DRAM bytes per launch from the committed ncu summary, scaled to `rows`."""
+    path = os.path.join(REPO, "profiles", "fact_filter_aggregate.md")
+    try:
+        with open(path) as f:
+            for ln in f:
+                if ln.startswith("dram_bytes_per_row:"):
+                    return float(ln.split(":")[1]) * rows
+    except OSError:
+        pass
+    return None
+
+
+# ------------------------------------------------------------------------------ CPU legs
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def fact_oracle_descriptors():
+    import oracle as O
+    from redfox_b200 import workloads as WL
+
+    def oarith(e):
+        return O.make_arith([(e.nodes[i].kind, e.nodes[i].op, e.nodes[i].type, e.nodes[i].left, e.nodes[i].right,
+                              e.nodes[i].value) for i in range(e.nnodes)], e.root, e.dest_type, e.dest_bits)
+    cmps = [{"op": op, "a": a, "b": b, "type": vt} for (op, a, b, vt) in WL.fact_predicate()]
+    return cmps, [oarith(a) for a in WL.fact_ariths()]
+
+
+def cpu_rows_sample(n):
+    import oracle as O
+    from redfox_b200 import workloads as WL
+    cols = [O.uniform(n, WL.FACT_SEED, f, WL.FACT_LO[f], WL.FACT_HI[f]) for f in range(7)]
+    return O.pack(WL.FACT_WIDTHS, cols)
+
+
+def time_oracle_port(rows, threads, reps=3):
+    import oracle as O
+    from redfox_b200 import workloads as WL
+    cmps, ariths = fact_oracle_descriptors()
+    ts = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        O.filter_aggregate(rows, WL.FACT_WIDTHS, cmps, ariths, WL.FACT_GROUP_FIELDS, WL.FACT_SUM_FIELDS,
+                           threads=threads)
+        ts.append(time.perf_counter() - t0)
+    return len(rows) / statistics.median(ts)
+
+
+def reference_plan_fn():
+    """ref_fact_plan from oracle/_ref (the reference's code built for the host), or None."""
+    import ctypes as C
+    import oracle as O
+    ref = O.ref_lib()
+    if ref is None:
+        return None
+    fn = ref.ref_fact_plan
+    fn.restype = C.c_int64
+    fn.argtypes = [C.c_void_p, C.c_size_t, C.c_uint, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    return fn
+
+
+def run_reference_plan(fn, rows, threads):
+    """The reference plan over `threads` row partitions in parallel, partial groups summed."""
+    import ctypes as C
+    from concurrent.futures import ThreadPoolExecutor
+
+    import numpy as np
+    from redfox_b200 import workloads as WL
+    parts = np.array_split(np.arange(len(rows)), threads)
+
+    def one(idx):
+        sub = np.ascontiguousarray(rows[idx[0]:idx[-1] + 1]) if len(idx) else rows[:0]
+        ok = np.zeros(16, np.uint64)
+        s1 = np.zeros(16, np.int64)
+        s2 = np.zeros(16, np.int64)
+        cnt = np.zeros(16, np.uint64)
+        g = fn(sub.ctypes.data_as(C.c_void_p), len(sub), WL.FACT_CUTOFF, ok.ctypes.data_as(C.c_void_p),
+               s1.ctypes.data_as(C.c_void_p), s2.ctypes.data_as(C.c_void_p), cnt.ctypes.data_as(C.c_void_p))
+        return {int(k): (int(a), int(b), int(c)) for k, a, b, c in zip(ok[:g], s1[:g], s2[:g], cnt[:g])}
+
+    merged = {}
+    with ThreadPoolExecutor(max_workers=threads) as ex:
+        for part in ex.map(one, parts):
+            for k, (a, b, c) in part.items():
+                x = merged.get(k, (0, 0, 0))
+                merged[k] = (x[0] + a, x[1] + b, x[2] + c)
+    return merged
+
+
+def cpu_baseline_line(budget_s=12.0):
+    """The oracle port on a bounded sample of the same table, all host threads."""
+    threads = cpu_threads()
+    probe = cpu_rows_sample(200_000)
+    rate = time_oracle_port(probe, threads, reps=1)
+    n = int(min(max(rate * budget_s / 3.0, 200_000), 16_000_000))
+    rows = cpu_rows_sample(n)
+    v = time_oracle_port(rows, threads, reps=3)
+    return {"value": v, "unit": "tuples/s", "cores": threads, "kind": "port",
+            "sample": "first %d rows of the same seeded table, C oracle (OpenMP), median of 3" % n}
+
+
+# ------------------------------------------------------------------------------ reference arm
+def main_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    threads = cpu_threads()
+    fn = reference_plan_fn()
+    kind = "reference" if fn is not None else "port"
+    sample = 4_000_000 if fn is not None else 8_000_000
+    rows = cpu_rows_sample(sample)
+
+    def step():
+        if fn is not None:
+            run_reference_plan(fn, rows, threads)
+        else:
+            time_oracle_port(rows, threads, reps=1)
+
+    for _ in range(max(args.warmup, 1)):
+        step()
+    ts = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        step()
+        ts.append(time.perf_counter() - t0)
+    sec = sum(ts) / len(ts)
+    value = sample / sec
+    what = ("reference Tuple.h/Comparisons.h/Project.h device code + thrust reduce_by_key built for the host "
+            "(oracle/_ref), %d row partitions in parallel" % threads) if fn is not None else "C oracle (OpenMP)"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "tuples/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "rows_per_step": sample, "parallelism": "host threads"},
+        "cpu_baseline": {"value": value, "unit": "tuples/s", "cores": threads, "kind": kind,
+                         "sample": "%d rows of the seeded table per step; %s" % (sample, what)},
+        "e2e": {"value": value, "unit": "tuples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------------------ our arm
+def main_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    from redfox_b200 import rfx as R
+    from redfox_b200 import workloads as WL
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+    n = args.rows
+    stream = torch.cuda.current_stream()
+
+    # each rank's partition: rows [rank*n, (rank+1)*n) of the seeded table, made on device
+    rows = R.gen_uniform_rows(n, WL.FACT_WIDTHS, WL.FACT_SEED + rank, WL.FACT_LO, WL.FACT_HI, device=dev)
+    plan = WL.fact_plan(n, device=dev)
+    nacc = plan.G * (plan.nsum + 1)
+    gacc = plan.ws[: nacc * 8].view(torch.int64)
+    torch.cuda.synchronize()
+
+    def step():
+        plan.launch(rows)
+        if world > 1:
+            dist.all_reduce(gacc)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    assert R.device_status() == R.OK
+    # correctness spot check against the oracle on the first rows (not timed)
+    check_n = 1_000_000
+    chk = WL.fact_plan(check_n, device=dev)
+    chk.launch(rows)
+    keys, sums, counts = chk.result()
+
+    if world > 1:
+        dist.barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    time.sleep(0.3)
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    k_ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    for i in range(args.steps):
+        k_ev[i][0].record(stream)
+        plan.launch(rows)
+        k_ev[i][1].record(stream)
+        if world > 1:
+            dist.all_reduce(gacc)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clocks = sampler.stop()
+    ms_total = ev0.elapsed_time(ev1)
+    kernel_ms = [a.elapsed_time(b) for a, b in k_ev]
+    t = torch.tensor([ms_total, statistics.mean(kernel_ms)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_total, kms = float(t[0]), float(t[1])
+    ms_step = ms_total / args.steps
+    value = world * n / (ms_step / 1e3)
+
+    # ---- end to end: host table -> device -> plan -> groups back to host
+    host = torch.empty((n, WL.fact_row_bytes()), dtype=torch.uint8, pin_memory=True)
+    host.copy_(rows)
+    dev_in = torch.empty_like(rows)
+    out_k = torch.empty(plan.G, dtype=torch.int64, pin_memory=True)
+    out_s = torch.empty((plan.G, plan.nsum), dtype=torch.int64, pin_memory=True)
+    out_c = torch.empty(plan.G, dtype=torch.int64, pin_memory=True)
+    out_g = torch.empty(1, dtype=torch.int64, pin_memory=True)
+
+    def e2e_step():
+        dev_in.copy_(host, non_blocking=True)
+        plan.launch(dev_in)
+        if world > 1:
+            dist.all_reduce(gacc)
+        out_k.copy_(plan.keys, non_blocking=True)
+        out_s.copy_(plan.sums[:, :plan.nsum], non_blocking=True)
+        out_c.copy_(plan.counts, non_blocking=True)
+        out_g.copy_(plan.ngroups, non_blocking=True)
+
+    e2e_step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.e2e_steps):
+        e2e_step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    te = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_ms = float(te[0]) / args.e2e_steps
+    d2h = (plan.G * (2 + plan.nsum) + 1) * 8
+    del host, dev_in
+
+    ok = R.device_status() == R.OK
+    result = None
+    if rank == 0:
+        peak, peak_kind = measured_peak_hbm()
+        bytes_alg = n * WL.fact_row_bytes()
+        achieved = bytes_alg / (kms / 1e3) / 1e9
+        traffic = profiled_traffic(n)
+        cpu = None
+        if not args.no_cpu_baseline and world == 1:
+            try:
+                import numpy as np
+                import oracle as O
+                cmps, ariths = fact_oracle_descriptors()
+                sub = rows[:check_n].cpu().numpy()
+                ek, es, ec = O.filter_aggregate(sub, WL.FACT_WIDTHS, cmps, ariths, WL.FACT_GROUP_FIELDS,
+                                                WL.FACT_SUM_FIELDS)
+                ok = ok and np.array_equal(keys, ek) and np.array_equal(sums, es) and np.array_equal(counts, ec)
+                cpu = cpu_baseline_line()
+            except Exception as e:  # the baseline is reported, never required
+                cpu = {"value": None, "unit": "tuples/s", "cores": cpu_threads(), "kind": "port",
+                       "sample": "failed: %s" % e}
+        result = {
+            "metric": METRIC, "value": value, "unit": "tuples/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "rows_per_gpu": n, "row_bytes": WL.fact_row_bytes(),
+                       "l2": "inputs larger than L2 (%.2f GB per GPU), no flush" % (bytes_alg / 1e9),
+                       "parallelism": "dp%d (row partitions, 6-group all-reduce)" % world if world > 1 else "1 GPU"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel": "scan_aggregate_kernel<64,true>", "kernel_ms": kms,
+                         "algorithmic_bytes_per_launch": bytes_alg},
+            "cpu_baseline": cpu,
+            "e2e": {"value": world * n / (e2e_ms / 1e3), "unit": "tuples/s", "ms_per_step": e2e_ms,
+                    "h2d_bytes_per_step": n * WL.fact_row_bytes(), "d2h_bytes_per_step": d2h},
+            "gpu_launches": args.steps,
+            "clocks": clocks,
+            "parity": "ok" if ok else "MISMATCH",
+        }
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if result is not None:
+        print(json.dumps(result), flush=True)
+    return 0 if ok else 1
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return main_reference(args)
+    return main_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

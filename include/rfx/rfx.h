@@ -1,0 +1,157 @@
+/*
+ * rfx.h -- C ABI of redfox_b200, a B200-native (sm_100a) implementation of the Red Fox
+ * relational-algebra kernel library.
+ *
+ * Every entry point takes plain device pointers, element counts and a CUDA stream
+ * (passed as void*), enqueues its kernels and returns without synchronising.  Buffers
+ * are owned by the caller.  Entries that need scratch memory take a caller-provided
+ * workspace whose size a matching *_workspace() query reports.  Output sizes are written
+ * to device-resident uint64 counters, as the reference's kernels write theirs, so whole
+ * plans can be captured in CUDA graphs.  Kernels never trap: a bounded wait that gives
+ * up or an input outside a declared bound sets the per-device error word, which
+ * rfx_device_status() reads.
+ *
+ * Each declaration names the reference interface it replaces (paths within the
+ * sidharth87/redfox tree).
+ */
+#ifndef RFX_RFX_H
+#define RFX_RFX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  The reference aborts on CUDA errors (b40cSort.cu:48-56) and silently
+ * ignores unsupported widths (b40cSort.cu:85-800); these entries report instead. */
+typedef enum rfx_status {
+    RFX_OK = 0,
+    RFX_ERR_INVALID = 1,     /* null pointer, bad descriptor or size */
+    RFX_ERR_UNSUPPORTED = 2, /* width / type combination not provided */
+    RFX_ERR_CAPACITY = 3,    /* output larger than the caller's capacity */
+    RFX_ERR_TIMEOUT = 4,     /* a bounded device-side wait gave up */
+    RFX_ERR_CUDA = 5,        /* CUDA runtime error */
+    RFX_ERR_WORKSPACE = 6    /* workspace smaller than the *_workspace() size */
+} rfx_status;
+
+/* Data type codes = nvcc::RelationalAlgebraKernel::DataType
+ * (redfox/nvcc/interface/RelationalAlgebraKernel.h:81-95). */
+enum { RFX_I8 = 1, RFX_I16 = 2, RFX_I32 = 3, RFX_I64 = 4, RFX_I128 = 5, RFX_I256 = 6, RFX_I512 = 7 };
+
+/* Comparison codes = RelationalAlgebraKernel::Comparison (RelationalAlgebraKernel.h:157-172). */
+enum { RFX_EQ = 1, RFX_NE, RFX_SLT, RFX_LT, RFX_SLE, RFX_LE, RFX_SGT, RFX_GT, RFX_SGE, RFX_GE };
+/* Operand kinds = ComparisonOperandType (RelationalAlgebraKernel.h:174-180). */
+enum { RFX_OPND_CONSTANT = 0, RFX_OPND_VARIABLE = 2 };
+/* Arithmetic = ArithmeticOp and ArithExpNodeKind (RelationalAlgebraKernel.h:121-138). */
+enum { RFX_ADD = 0, RFX_MUL, RFX_SUB, RFX_DIV, RFX_MOD };
+enum { RFX_NODE_OP = 0, RFX_NODE_CONST, RFX_NODE_INDEX };
+
+/* A packed tuple type: up to 16 unsigned bit-fields, field 0 in the most significant used
+ * bits, stored in a container of 1/2/4/8/16/32/64 bytes (ra::tuple::Tuple, Tuple.h:714-741;
+ * BasicTypeWithBits / PackedNBytes, Tuple.h:231-672). */
+typedef struct rfx_tuple {
+    uint32_t nfields;
+    uint32_t widths[16];
+} rfx_tuple;
+
+/* One ANDed comparison of a ComparisonVector (RelationalAlgebraKernel.h:182-208):
+ * field-vs-constant or field-vs-field, compared as the unsigned C type `value_type`. */
+typedef struct rfx_cmp {
+    uint32_t op;
+    uint32_t a_kind, b_kind;
+    uint32_t a_field, b_field;
+    uint32_t value_type;
+    uint64_t a_const, b_const;
+} rfx_cmp;
+
+/* An ArithExpNode (RelationalAlgebraKernel.h:140-149) in array form. */
+typedef struct rfx_arith_node {
+    uint32_t kind;
+    uint32_t op;
+    uint32_t type;
+    int32_t left, right;
+    uint32_t pad;
+    uint64_t value; /* constant, or field index */
+} rfx_arith_node;
+
+/* set_arith (RelationalAlgebraKernel.cpp:2001-2150): appends one field computed by an
+ * expression tree over the tuple's fields with C integer semantics. */
+typedef struct rfx_arith_expr {
+    const rfx_arith_node* nodes; /* host memory, read at call time */
+    uint32_t nnodes;
+    uint32_t root;
+    uint32_t dest_type;
+    uint32_t dest_bits;
+} rfx_arith_expr;
+
+/* ---------------------------------------------------------------- device status */
+/* Reads and clears the error word of the current device after synchronising `stream`. */
+rfx_status rfx_device_status(void* stream);
+/* Library version string. */
+const char* rfx_version(void);
+
+/* ---------------------------------------------------------------- select / project */
+/* Workspace for the compaction entries below (tile status words). */
+size_t rfx_select_workspace(uint64_t n, const rfx_tuple* in);
+
+/* set_select<id> + scan<id> + select_get_result_size<id> + select_gather<id>
+ * (ra/interface/Select.h:30-1127; RelationalAlgebraKernel.cpp:1399-1419, :2302-2593) in
+ * one order-preserving pass.  Writes the selected rows to `out` and their count to
+ * *d_count. */
+rfx_status rfx_select(void* out, uint64_t* d_count, const void* in, uint64_t n,
+                      const rfx_tuple* in_type, const rfx_cmp* cmps, uint32_t ncmp,
+                      void* workspace, size_t workspace_bytes, void* stream);
+
+/* set_arith<id> (RelationalAlgebraKernel.cpp:2001-2150): out = in << dest_bits with the
+ * expression in the new last field. */
+rfx_status rfx_arith(void* out, const void* in, uint64_t n, const rfx_tuple* in_type,
+                     const rfx_arith_expr* arith, void* stream);
+
+/* set_project<id> = ra::cuda::permute (ra/interface/Project.h:58-121): out field k =
+ * in field map[k]; map entries >= 16 give 0. */
+rfx_status rfx_project(void* out, const void* in, uint64_t n, const rfx_tuple* in_type,
+                       const rfx_tuple* out_type, const uint32_t* map, void* stream);
+
+/* Fused select -> arith* -> project with compaction: the rows passing `cmps` get
+ * `narith` appended fields (each may read the earlier ones), then `out_type`'s field k
+ * is taken from extended field map[k].  Same rows and order as running the reference's
+ * select, arith and project kernels one after another. */
+rfx_status rfx_select_project(void* out, uint64_t* d_count, const void* in, uint64_t n,
+                              const rfx_tuple* in_type, const rfx_cmp* cmps, uint32_t ncmp,
+                              const rfx_arith_expr* ariths, uint32_t narith,
+                              const rfx_tuple* out_type, const uint32_t* map,
+                              void* workspace, size_t workspace_bytes, void* stream);
+
+/* Fused select -> arith* -> group-by SUM(int64)/COUNT over a small key domain: the plan
+ * that addAgg builds from project + sort_pair + reduce + count
+ * (RelationalAlgebraCompiler.cpp:7852-8643; Reduce.cu), in one pass over the rows.
+ * Group field k (an extended field index) must be < group_domain[k]; the groups are the
+ * mixed-radix combinations (at most 4096).  Outputs, for the groups that occur, in
+ * ascending packed-key order: out_keys[g] = packed group key (group fields concatenated,
+ * first field most significant), out_sums[g * nsum + j], out_counts[g]; *d_groups = the
+ * number of groups.  A row outside the declared domains sets RFX_ERR_CAPACITY in the
+ * device error word. */
+size_t rfx_filter_aggregate_workspace(uint64_t n, const rfx_tuple* in_type,
+                                      const uint32_t* group_domain, uint32_t ngroup,
+                                      uint32_t nsum);
+rfx_status rfx_filter_aggregate(const void* in, uint64_t n, const rfx_tuple* in_type,
+                                const rfx_cmp* cmps, uint32_t ncmp,
+                                const rfx_arith_expr* ariths, uint32_t narith,
+                                const uint32_t* group_fields, const uint32_t* group_domain,
+                                uint32_t ngroup, const uint32_t* sum_fields, uint32_t nsum,
+                                uint64_t* out_keys, int64_t* out_sums, uint64_t* out_counts,
+                                uint64_t* d_groups, void* workspace, size_t workspace_bytes,
+                                void* stream);
+
+/* ---------------------------------------------------------------- synthetic data */
+/* Column j of row i = lo[j] + mulhi64(rand(seed, stream_j, i), hi[j] - lo[j]) with the
+ * SplitMix64 stream below, packed as `type`.  The generator behind the benchmarks. */
+rfx_status rfx_gen_uniform_rows(void* out, uint64_t n, const rfx_tuple* type, uint64_t seed,
+                                const uint64_t* lo, const uint64_t* hi, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,98 @@
+// host_common.cpp -- see host_common.h.
+#include "host_common.h"
+
+#include <mutex>
+#include <unordered_map>
+
+namespace rfx {
+
+rfx_status cuda_fail(cudaError_t e) {
+  (void)cudaGetLastError();  // clear a non-sticky error so the next call starts clean
+  return e == cudaSuccess ? RFX_OK : RFX_ERR_CUDA;
+}
+
+namespace {
+std::mutex g_mu;
+std::unordered_map<int, int> g_sms;
+std::unordered_map<int, uint32_t*> g_err;
+struct OccKey {
+  const void* k;
+  int threads;
+  size_t smem;
+  bool operator==(const OccKey& o) const { return k == o.k && threads == o.threads && smem == o.smem; }
+};
+struct OccHash {
+  size_t operator()(const OccKey& o) const {
+    return std::hash<const void*>()(o.k) ^ (o.smem * 131) ^ ((size_t)o.threads << 20);
+  }
+};
+std::unordered_map<OccKey, int, OccHash> g_occ;
+std::unordered_map<const void*, size_t> g_smem_set;
+}  // namespace
+
+int device_sms() {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(g_mu);
+  auto it = g_sms.find(dev);
+  if (it != g_sms.end()) return it->second;
+  int sms = 0;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+  g_sms[dev] = sms;
+  return sms;
+}
+
+uint32_t* device_error_word() {
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lk(g_mu);
+  auto it = g_err.find(dev);
+  if (it != g_err.end()) return it->second;
+  uint32_t* p = nullptr;
+  if (cudaMalloc(&p, sizeof(uint32_t)) != cudaSuccess) return nullptr;
+  cudaMemset(p, 0, sizeof(uint32_t));
+  cudaDeviceSynchronize();
+  g_err[dev] = p;
+  return p;
+}
+
+cudaError_t allow_smem(const void* kernel, size_t bytes) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  auto it = g_smem_set.find(kernel);
+  if (it != g_smem_set.end() && it->second >= bytes) return cudaSuccess;
+  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) g_smem_set[kernel] = bytes;
+  return e;
+}
+
+int persistent_grid(const void* kernel, int threads, size_t dyn_smem, uint64_t work_blocks) {
+  int per_sm = 0;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    auto it = g_occ.find(OccKey{kernel, threads, dyn_smem});
+    if (it != g_occ.end()) per_sm = it->second;
+  }
+  if (per_sm == 0) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, dyn_smem) != cudaSuccess || per_sm <= 0)
+      per_sm = 1;
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_occ[OccKey{kernel, threads, dyn_smem}] = per_sm;
+  }
+  uint64_t cap = (uint64_t)device_sms() * (uint64_t)per_sm;
+  uint64_t g = work_blocks < cap ? work_blocks : cap;
+  return (int)(g ? g : 1);
+}
+
+}  // namespace rfx
+
+extern "C" rfx_status rfx_device_status(void* stream) {
+  uint32_t* w = rfx::device_error_word();
+  if (!w) return RFX_ERR_CUDA;
+  uint32_t v = 0;
+  RFX_CUDA_TRY(cudaStreamSynchronize(rfx::as_stream(stream)));
+  RFX_CUDA_TRY(cudaMemcpy(&v, w, sizeof(v), cudaMemcpyDeviceToHost));
+  if (v) RFX_CUDA_TRY(cudaMemset(w, 0, sizeof(uint32_t)));
+  return static_cast<rfx_status>(v);
+}
+
+extern "C" const char* rfx_version(void) { return "redfox_b200 0.1 (sm_100a)"; }

@@ -1,0 +1,97 @@
+// rfx_device.cuh -- device-side building blocks shared by every redfox_b200 kernel:
+// packed-tuple limb access, vectorised row loads/stores, decoupled look-back with
+// bounded waits, and the device error word.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "rfx/rfx.h"
+
+namespace rfx {
+
+// ------------------------------------------------------------------ errors
+// Kernels never trap.  A bounded wait that gives up, or an input that violates a
+// declared bound, records a code in the per-device error word and the kernel carries
+// on (its output is then unspecified); the host reads the word with rfx_device_status.
+enum : uint32_t {
+  kErrNone = 0,
+  kErrTimeout = RFX_ERR_TIMEOUT,
+  kErrCapacity = RFX_ERR_CAPACITY,
+  kErrInvalid = RFX_ERR_INVALID,
+};
+
+__device__ __forceinline__ void raise_error(uint32_t* err, uint32_t code) {
+  if (err) atomicCAS(err, 0u, code);
+}
+
+// Upper bound on polls of a look-back predecessor before giving up (about 0.5 s with
+// the back-off below); a healthy predecessor publishes within microseconds.
+constexpr uint32_t kSpinLimit = 1u << 22;
+
+// ------------------------------------------------------------------ memory order
+__device__ __forceinline__ uint64_t ld_relaxed_u64(const uint64_t* p) {
+  uint64_t v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_relaxed_u64(uint64_t* p, uint64_t v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_u32(uint32_t* p, uint32_t v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// ------------------------------------------------------------------ look-back (64-bit)
+// One status word per tile: bits 63..62 = 0 not ready, 1 aggregate, 2 inclusive prefix;
+// bits 61..0 = the value.  Used for counts (compaction offsets, join output offsets).
+constexpr uint64_t kFlagAgg = 1ull << 62;
+constexpr uint64_t kFlagInc = 2ull << 62;
+constexpr uint64_t kValMask = (1ull << 62) - 1;
+
+// Called by the whole warp 0 of a tile.  Publishes `aggregate`, walks predecessors 32
+// at a time and returns the exclusive prefix (same value in every lane).
+__device__ __forceinline__ uint64_t lookback_exclusive(uint64_t* status, uint32_t tile,
+                                                       uint64_t aggregate, uint32_t* err) {
+  const uint32_t lane = threadIdx.x & 31;
+  if (tile == 0) {
+    if (lane == 0) st_relaxed_u64(&status[0], kFlagInc | (aggregate & kValMask));
+    return 0;
+  }
+  if (lane == 0) st_relaxed_u64(&status[tile], kFlagAgg | (aggregate & kValMask));
+  uint64_t prefix = 0;
+  int64_t base = (int64_t)tile - 1;  // highest predecessor not yet folded in
+  uint32_t spins = 0;
+  while (true) {
+    int64_t idx = base - (int64_t)lane;
+    uint64_t s = idx >= 0 ? ld_relaxed_u64(&status[idx]) : kFlagInc;
+    uint64_t flag = s & ~kValMask;
+    unsigned not_ready = __ballot_sync(0xffffffffu, flag == 0);
+    unsigned inc = __ballot_sync(0xffffffffu, flag == kFlagInc);
+    // lanes up to (and including) the first inclusive one are usable if none of them
+    // is still unpublished
+    unsigned upto = inc ? ((inc & (0u - inc)) << 1) - 1 : 0xffffffffu;  // lanes 0..first_inc
+    if (not_ready & upto) {
+      if (++spins > kSpinLimit) {
+        raise_error(err, kErrTimeout);
+        break;
+      }
+      __nanosleep(spins < 64 ? 20 : 200);
+      continue;
+    }
+    uint64_t v = ((upto >> lane) & 1u) ? (s & kValMask) : 0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    prefix += v;
+    if (inc) break;
+    base -= 32;
+  }
+  if (lane == 0) st_relaxed_u64(&status[tile], kFlagInc | ((prefix + aggregate) & kValMask));
+  return prefix;
+}
+
+}  // namespace rfx

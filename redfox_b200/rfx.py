@@ -1,0 +1,272 @@
+"""ctypes binding of librfx.so, the redfox_b200 C ABI (include/rfx/rfx.h).
+
+Device buffers are torch tensors (plumbing only: memory and streams); every computation
+runs in the CUDA kernels of librfx.so.  There is no CPU fallback: if the library is
+missing, importing this module raises.
+"""
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "librfx.so")
+
+OK, ERR_INVALID, ERR_UNSUPPORTED, ERR_CAPACITY, ERR_TIMEOUT, ERR_CUDA, ERR_WORKSPACE = range(7)
+STATUS_NAMES = {0: "OK", 1: "INVALID", 2: "UNSUPPORTED", 3: "CAPACITY", 4: "TIMEOUT", 5: "CUDA", 6: "WORKSPACE"}
+I8, I16, I32, I64, I128, I256, I512 = range(1, 8)
+EQ, NE, SLT, LT, SLE, LE, SGT, GT, SGE, GE = range(1, 11)
+OPND_CONST, OPND_VAR = 0, 2
+ADD, MUL, SUB, DIV, MOD = range(5)
+NODE_OP, NODE_CONST, NODE_INDEX = 0, 1, 2
+
+
+class RfxError(RuntimeError):
+    def __init__(self, fn, code):
+        super().__init__("%s failed: RFX_ERR_%s (%d)" % (fn, STATUS_NAMES.get(code, "?"), code))
+        self.code = code
+
+
+class Tuple(C.Structure):
+    _fields_ = [("nfields", C.c_uint32), ("widths", C.c_uint32 * 16)]
+
+    @classmethod
+    def of(cls, widths):
+        t = cls()
+        t.nfields = len(widths)
+        for i, w in enumerate(widths):
+            t.widths[i] = w
+        return t
+
+
+class Cmp(C.Structure):
+    _fields_ = [("op", C.c_uint32), ("a_kind", C.c_uint32), ("b_kind", C.c_uint32),
+                ("a_field", C.c_uint32), ("b_field", C.c_uint32), ("value_type", C.c_uint32),
+                ("a_const", C.c_uint64), ("b_const", C.c_uint64)]
+
+
+class ArithNode(C.Structure):
+    _fields_ = [("kind", C.c_uint32), ("op", C.c_uint32), ("type", C.c_uint32),
+                ("left", C.c_int32), ("right", C.c_int32), ("pad", C.c_uint32),
+                ("value", C.c_uint64)]
+
+
+class ArithExpr(C.Structure):
+    _fields_ = [("nodes", C.POINTER(ArithNode)), ("nnodes", C.c_uint32), ("root", C.c_uint32),
+                ("dest_type", C.c_uint32), ("dest_bits", C.c_uint32)]
+
+
+def container_bytes(bits):
+    for c in (8, 16, 32, 64, 128, 256, 512):
+        if bits <= c:
+            return c // 8
+    raise ValueError("tuples wider than 512 bits are not supported")
+
+
+def _load():
+    if not os.path.exists(_LIB_PATH):
+        raise ImportError("redfox_b200/librfx.so is not built; run __graft_entry__.build()")
+    lib = C.CDLL(_LIB_PATH)
+    P, u32, u64, sz, st = C.c_void_p, C.c_uint32, C.c_uint64, C.c_size_t, C.c_int
+    sig = {
+        "rfx_device_status": (st, [P]),
+        "rfx_version": (C.c_char_p, []),
+        "rfx_select_workspace": (sz, [u64, P]),
+        "rfx_select": (st, [P, P, P, u64, P, P, u32, P, sz, P]),
+        "rfx_arith": (st, [P, P, u64, P, P, P]),
+        "rfx_project": (st, [P, P, u64, P, P, P, P]),
+        "rfx_select_project": (st, [P, P, P, u64, P, P, u32, P, u32, P, P, P, sz, P]),
+        "rfx_filter_aggregate_workspace": (sz, [u64, P, P, u32, u32]),
+        "rfx_filter_aggregate": (st, [P, u64, P, P, u32, P, u32, P, P, u32, P, u32, P, P, P, P, P, sz, P]),
+        "rfx_gen_uniform_rows": (st, [P, u64, P, u64, P, P, P]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    return lib
+
+
+LIB = _load()
+
+
+def check(fn, code):
+    if code != OK:
+        raise RfxError(fn, code)
+
+
+def declared_symbols():
+    """Entry points declared in include/rfx/*.h (parsed from the headers)."""
+    import re
+    inc = os.path.join(os.path.dirname(_HERE), "include", "rfx")
+    names = []
+    for h in sorted(os.listdir(inc)):
+        if h.endswith(".h"):
+            text = open(os.path.join(inc, h)).read()
+            names += re.findall(r"^\s*(?:rfx_status|size_t|const char\*|void|uint64_t)\s+(rfx_\w+)\s*\(", text, re.M)
+    return names
+
+
+# ---------------------------------------------------------------------------- helpers
+def _ptr(t):
+    return C.c_void_p(t.data_ptr()) if t is not None else None
+
+
+def _stream(stream=None):
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return C.c_void_p(s.cuda_stream)
+
+
+def device_status(stream=None):
+    """Synchronise the stream and return (and clear) the device error word."""
+    return LIB.rfx_device_status(_stream(stream))
+
+
+def make_cmps(cmps):
+    """cmps: list of (op, (kind, field_or_const), (kind, field_or_const), value_type)."""
+    arr = (Cmp * max(1, len(cmps)))()
+    for i, (op, a, b, vt) in enumerate(cmps):
+        arr[i].op, arr[i].value_type = op, vt
+        for side, (kind, val) in (("a", a), ("b", b)):
+            setattr(arr[i], side + "_kind", kind)
+            setattr(arr[i], side + ("_field" if kind == OPND_VAR else "_const"), val)
+    return arr
+
+
+def make_arith(nodes, root, dest_type, dest_bits):
+    """nodes: list of (kind, op, type, left, right, value)."""
+    arr = (ArithNode * len(nodes))()
+    for i, (kind, op, typ, left, right, value) in enumerate(nodes):
+        arr[i].kind, arr[i].op, arr[i].type = kind, op, typ
+        arr[i].left, arr[i].right, arr[i].value = left, right, value
+    e = ArithExpr()
+    e.nodes = arr
+    e.nnodes, e.root, e.dest_type, e.dest_bits = len(nodes), root, dest_type, dest_bits
+    e._keep = arr
+    return e
+
+
+def _arith_array(ariths):
+    arr = (ArithExpr * max(1, len(ariths)))()
+    for i, a in enumerate(ariths):
+        arr[i] = a
+    arr._keep = [a._keep for a in ariths]
+    return arr
+
+
+def _empty_bytes(nbytes, device):
+    import torch
+    return torch.empty(max(1, nbytes), dtype=torch.uint8, device=device)
+
+
+# ---------------------------------------------------------------------------- entries
+def gen_uniform_rows(n, widths, seed, lo, hi, device="cuda", stream=None):
+    import torch
+    W = container_bytes(sum(widths))
+    out = torch.empty((n, W), dtype=torch.uint8, device=device)
+    lo_a = (C.c_uint64 * len(widths))(*lo)
+    hi_a = (C.c_uint64 * len(widths))(*hi)
+    check("rfx_gen_uniform_rows", LIB.rfx_gen_uniform_rows(_ptr(out), n, C.byref(Tuple.of(widths)), seed,
+                                                           lo_a, hi_a, _stream(stream)))
+    return out
+
+
+def select(rows, widths, cmps, stream=None):
+    """Order-preserving filter; returns (selected rows view, count)."""
+    import torch
+    n = rows.shape[0]
+    t = Tuple.of(widths)
+    out = torch.empty_like(rows)
+    cnt = torch.zeros(1, dtype=torch.int64, device=rows.device)
+    wsb = LIB.rfx_select_workspace(n, C.byref(t))
+    ws = _empty_bytes(wsb, rows.device)
+    carr = make_cmps(cmps)
+    check("rfx_select", LIB.rfx_select(_ptr(out), _ptr(cnt), _ptr(rows), n, C.byref(t), carr, len(cmps),
+                                       _ptr(ws), wsb, _stream(stream)))
+    k = int(cnt.item())
+    return out[:k], k
+
+
+def arith(rows, widths, expr, stream=None):
+    import torch
+    n = rows.shape[0]
+    W = container_bytes(sum(widths) + expr.dest_bits)
+    out = torch.empty((n, W), dtype=torch.uint8, device=rows.device)
+    check("rfx_arith", LIB.rfx_arith(_ptr(out), _ptr(rows), n, C.byref(Tuple.of(widths)), C.byref(expr),
+                                     _stream(stream)))
+    return out
+
+
+def project(rows, in_widths, out_widths, fmap, stream=None):
+    import torch
+    n = rows.shape[0]
+    W = container_bytes(sum(out_widths))
+    out = torch.empty((n, W), dtype=torch.uint8, device=rows.device)
+    m = (C.c_uint32 * 16)(*(list(fmap) + [100] * (16 - len(fmap))))
+    check("rfx_project", LIB.rfx_project(_ptr(out), _ptr(rows), n, C.byref(Tuple.of(in_widths)),
+                                         C.byref(Tuple.of(out_widths)), m, _stream(stream)))
+    return out
+
+
+def select_project(rows, widths, cmps, ariths, out_widths, fmap, stream=None):
+    import torch
+    n = rows.shape[0]
+    t = Tuple.of(widths)
+    W = container_bytes(sum(out_widths))
+    out = torch.empty((n, W), dtype=torch.uint8, device=rows.device)
+    cnt = torch.zeros(1, dtype=torch.int64, device=rows.device)
+    wsb = LIB.rfx_select_workspace(n, C.byref(t))
+    ws = _empty_bytes(wsb, rows.device)
+    m = (C.c_uint32 * 16)(*(list(fmap) + [100] * (16 - len(fmap))))
+    check("rfx_select_project", LIB.rfx_select_project(
+        _ptr(out), _ptr(cnt), _ptr(rows), n, C.byref(t), make_cmps(cmps), len(cmps), _arith_array(ariths),
+        len(ariths), C.byref(Tuple.of(out_widths)), m, _ptr(ws), wsb, _stream(stream)))
+    k = int(cnt.item())
+    return out[:k], k
+
+
+class FilterAggregate:
+    """A prepared rfx_filter_aggregate call: descriptors, outputs and workspace allocated
+    once so that repeated launches (benchmarks, serving) allocate nothing."""
+
+    def __init__(self, n, widths, cmps, ariths, group_fields, group_domain, sum_fields, device="cuda"):
+        import torch
+        self.n = n
+        self.t = Tuple.of(widths)
+        self.cmps = make_cmps(cmps)
+        self.ncmp = len(cmps)
+        self.ariths = _arith_array(ariths)
+        self.narith = len(ariths)
+        self.gf = (C.c_uint32 * 4)(*group_fields)
+        self.gd = (C.c_uint32 * 4)(*group_domain)
+        self.ngroup = len(group_fields)
+        self.sf = (C.c_uint32 * 4)(*sum_fields)
+        self.nsum = len(sum_fields)
+        G = 1
+        for d in group_domain:
+            G *= d
+        self.G = G
+        self.keys = torch.zeros(G, dtype=torch.int64, device=device)
+        self.sums = torch.zeros((G, max(1, self.nsum)), dtype=torch.int64, device=device)
+        self.counts = torch.zeros(G, dtype=torch.int64, device=device)
+        self.ngroups = torch.zeros(1, dtype=torch.int64, device=device)
+        self.wsb = LIB.rfx_filter_aggregate_workspace(n, C.byref(self.t), self.gd, self.ngroup, self.nsum)
+        self.ws = _empty_bytes(self.wsb, device)
+
+    def launch(self, rows, n=None, stream=None):
+        n = self.n if n is None else n
+        check("rfx_filter_aggregate", LIB.rfx_filter_aggregate(
+            _ptr(rows), n, C.byref(self.t), self.cmps, self.ncmp, self.ariths, self.narith, self.gf, self.gd,
+            self.ngroup, self.sf, self.nsum, _ptr(self.keys), _ptr(self.sums), _ptr(self.counts),
+            _ptr(self.ngroups), _ptr(self.ws), self.wsb, _stream(stream)))
+
+    def result(self):
+        g = int(self.ngroups.item())
+        return (self.keys[:g].cpu().numpy().astype("uint64"), self.sums[:g, :self.nsum].cpu().numpy(),
+                self.counts[:g].cpu().numpy().astype("uint64"))
+
+
+def filter_aggregate(rows, widths, cmps, ariths, group_fields, group_domain, sum_fields, stream=None):
+    fa = FilterAggregate(rows.shape[0], widths, cmps, ariths, group_fields, group_domain, sum_fields,
+                         device=rows.device)
+    fa.launch(rows, stream=stream)
+    return fa.result()

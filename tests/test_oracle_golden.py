@@ -1,0 +1,152 @@
+"""The oracle pinned against the reference: golden fixtures made by the reference's own
+code (tests/golden/make_golden.py) and the reference's known-answer tests.  CPU only."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+
+from helpers import fact_oracle, fact_rows_oracle
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def load(name):
+    return np.load(os.path.join(GOLD, name))
+
+
+def test_tpch_fixture_A_packing():
+    """TPC-H/data/A = TC.tbl rows (1,6)..(5,10) packed as Tuple<32,32> (field 0 high)."""
+    raw = np.fromfile(os.path.join(GOLD, "tpch_A.bin"), dtype=np.uint8).reshape(5, 8)
+    cols = [np.arange(1, 6, dtype=np.uint64), np.arange(6, 11, dtype=np.uint64)]
+    assert np.array_equal(O.pack([32, 32], cols), raw)
+    back = O.unpack([32, 32], raw)
+    assert np.array_equal(back[0], cols[0]) and np.array_equal(back[1], cols[1])
+    assert raw.view("<u8")[0, 0] == 0x0000000100000006
+
+
+def test_tuple_packing_matches_reference_insert():
+    g = load("tuple_pack.npz")
+    names = sorted({k.rsplit("_", 1)[0] for k in g.files})
+    assert len(names) >= 10
+    for name in names:
+        widths = [int(w) for w in g[name + "_widths"]]
+        cols = list(g[name + "_cols"])
+        ref = g[name + "_bytes"]
+        assert np.array_equal(O.pack(widths, cols), ref), name
+        for a, b in zip(O.unpack(widths, ref), cols):
+            assert np.array_equal(a, b), name
+
+
+def _setcases(g):
+    return sorted({k.rsplit("_", 1)[0] for k in g.files if k.endswith("_a")})
+
+
+def test_set_union_difference_match_reference():
+    g = load("setops.npz")
+    for key in _setcases(g):
+        a, b = g[key + "_a"], g[key + "_b"]
+        assert np.array_equal(O.set_union(a, b), g[key + "_union"]), key
+        assert np.array_equal(O.set_difference(a, b), g[key + "_difference"]), key
+        if key + "_intersection" in g.files:
+            assert np.array_equal(O.set_intersection(a, b), g[key + "_intersection"]), key
+        if key + "_unique" in g.files:
+            assert np.array_equal(O.unique(a), g[key + "_unique"]), key
+
+
+def test_reduce_count_match_reference():
+    g = load("reduce.npz")
+    for e in (1, 2, 4, 16):
+        ok, oc = O.reduce_count(g["count%d_keys" % e], g["count%d_vals" % e])
+        assert np.array_equal(ok, g["count%d_okeys" % e]) and np.array_equal(oc, g["count%d_ocounts" % e]), e
+    # total_64_32: u64 keys, u32 sums; the oracle's int64 sums agree modulo 2^32
+    ok, os_ = O.reduce_sum_i64(g["total64_32_keys"], g["total64_32_vals"].astype(np.int64))
+    assert np.array_equal(ok, g["total64_32_okeys"])
+    assert np.array_equal(os_.astype(np.uint64) & np.uint64(0xffffffff), g["total64_32_osums"].astype(np.uint64))
+    ok, os_ = O.reduce_sum_i64(g["sum_i64_keys"], g["sum_i64_vals"])
+    assert np.array_equal(ok, g["sum_i64_okeys"]) and np.array_equal(os_, g["sum_i64_osums"])
+
+
+def test_sort_matches_reference():
+    g = load("sort.npz")
+    for e in (1, 2, 4, 8):
+        assert np.array_equal(O.sort_pairs(g["e%d_in" % e]), g["e%d_out" % e]), e
+
+
+def test_fact_plan_matches_reference_composition():
+    g = load("fact_plan.npz")
+    rows = fact_rows_oracle(int(g["n"][0]))
+    keys, sums, counts = fact_oracle(rows)
+    assert np.array_equal(keys, g["keys"])
+    assert np.array_equal(sums[:, 0], g["s1"]) and np.array_equal(sums[:, 1], g["s2"])
+    assert np.array_equal(counts, g["counts"])
+
+
+def test_testjoin_identity_self_join():
+    """TestJoin.cu:107-156: self-join of 2^15 ushort keys 0..32767 yields (i << 16) | i."""
+    n = 1 << 15
+    keys = np.arange(n, dtype=np.uint16)
+    lb, scan, total = O.find_bounds(keys, keys)
+    assert total == n
+    li, ri = O.join_expand(lb, scan, total)
+    out = O.join_gather(4, li, ri, keys, None, 0, keys, 16).view(np.uint32).ravel()
+    assert np.array_equal(out, (np.arange(n, dtype=np.uint32) << 16) | np.arange(n, dtype=np.uint32))
+
+
+def _cpujoin(a, b):
+    """moderngpu CPUJoin (tests/benchmarkjoin.cu:40-128), inner join, as a literal loop."""
+    a_lb = np.searchsorted(b, a, side="left")
+    a_ub = np.searchsorted(b, a, side="right")
+    counts = a_ub - a_lb
+    scan = np.concatenate([[0], np.cumsum(counts)[:-1]]) if len(a) else np.zeros(0, np.int64)
+    total = int(counts.sum())
+    ai, bi = np.zeros(total, np.int32), np.zeros(total, np.int32)
+    a_index = b_index = 0
+    while a_index < total:
+        p = True if b_index >= len(a) else a_index < scan[b_index]
+        if not p:
+            b_index += 1
+            continue
+        src = b_index - 1
+        ai[a_index] = src
+        bi[a_index] = a_lb[src] + (a_index - scan[src])
+        a_index += 1
+    return ai, bi
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2])
+def test_join_order_matches_cpujoin(seed):
+    rng = np.random.default_rng(seed)
+    a = np.sort(rng.integers(0, 300, 500)).astype(np.uint32)
+    b = np.sort(rng.integers(0, 300, 400)).astype(np.uint32)
+    lb, scan, total = O.find_bounds(a, b)
+    li, ri = O.join_expand(lb, scan, total)
+    ai, bi = _cpujoin(a, b)
+    assert np.array_equal(li, ai) and np.array_equal(ri, bi)
+
+
+def test_generators_are_counter_based():
+    a = O.uniform(1000, 7, 3, 10, 20)
+    b = O.uniform(2000, 7, 3, 10, 20)
+    assert np.array_equal(a, b[:1000]) and a.min() >= 10 and a.max() < 20
+
+
+@pytest.mark.skipif(O.ref_lib() is None, reason="reference code not built here")
+def test_oracle_against_reference_code_random():
+    """Fresh random cases straight through the reference's compiled entry files."""
+    import ctypes as C
+    ref = O.ref_lib()
+    ref.ref_set_union.restype = C.c_uint64
+    ref.ref_difference.restype = C.c_uint64
+    rng = np.random.default_rng(99)
+    for _ in range(20):
+        a = np.sort(rng.integers(0, 1000, rng.integers(0, 3000))).astype(np.uint64)
+        b = np.sort(rng.integers(0, 1000, rng.integers(0, 3000))).astype(np.uint64)
+        out = np.zeros(len(a) + len(b) + 1, np.uint64)
+        k = ref.ref_set_union(out.ctypes.data_as(C.c_void_p), a.ctypes.data_as(C.c_void_p), C.c_size_t(len(a)),
+                              b.ctypes.data_as(C.c_void_p), C.c_size_t(len(b)), 8, 4)
+        assert np.array_equal(O.set_union(a, b), out[:k])
+        k = ref.ref_difference(out.ctypes.data_as(C.c_void_p), a.ctypes.data_as(C.c_void_p), C.c_size_t(len(a)),
+                               b.ctypes.data_as(C.c_void_p), C.c_size_t(len(b)), 8, 4)
+        assert np.array_equal(O.set_difference(a, b), out[:k])

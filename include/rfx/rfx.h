@@ -145,6 +145,43 @@ rfx_status rfx_filter_aggregate(const void* in, uint64_t n, const rfx_tuple* in_
                                 uint64_t* d_groups, void* workspace, size_t workspace_bytes,
                                 void* stream);
 
+/* ---------------------------------------------------------------- sort */
+/* Flag for rfx_sort_pairs: read the digit histogram back and skip digit passes whose
+ * digit is constant over the input (synchronises the stream once per 128-bit chunk). */
+#define RFX_SORT_SKIP_TRIVIAL 1u
+
+/* Workspace of rfx_sort_pairs: the alternate key/value buffers plus histogram and
+ * look-back words. */
+size_t rfx_sort_workspace(uint64_t n, uint32_t key_bytes, uint32_t value_bytes,
+                          uint32_t begin_bit, uint32_t end_bit);
+
+/* Stable ascending LSD radix sort, in place, of n keys of key_bytes (1/2/4/8/16/32/64)
+ * on their bits [begin_bit, end_bit) as an unsigned integer (limb a[0] lowest), moving
+ * values of value_bytes (0 = keys only, 1/2/4/8/16) with them.  Replaces
+ * redfox::sort_pair / sort_key of b40cSort.cu:58-1022 (LSD, bits [0, key_bits)) and of
+ * ModernGPUSort.cu:238-548 (stable merge sort on the whole key): both orders are the
+ * unique stable order this produces.  Packed tuples sort by a field range directly
+ * (no split into key and value arrays).  n < 2^30. */
+rfx_status rfx_sort_pairs(void* keys, void* values, uint64_t n, uint32_t key_bytes,
+                          uint32_t value_bytes, uint32_t begin_bit, uint32_t end_bit,
+                          uint32_t flags, void* workspace, size_t workspace_bytes, void* stream);
+
+/* redfox::sort_pair / sort_key of b40cSort.cu:58 / :828 with the reference's argument
+ * meaning: the key container follows key_bits (<=8: 1 byte, <=16: 2, <=32: 4, <=64: 8),
+ * the value container follows value_type (a DataType code), the sort covers bits
+ * [0, key_bits).  Every (bits, type) pair is supported, where the reference silently
+ * skips all but a fixed list.  Allocates its scratch and synchronises, as the
+ * reference does (default stream). */
+rfx_status rfx_b40c_sort_pair(void* keys, void* values, uint64_t n, uint64_t key_bits,
+                              uint64_t value_type);
+rfx_status rfx_b40c_sort_key(void* keys, uint64_t n, uint64_t bits);
+
+/* redfox::sort_pair / sort_key of ModernGPUSort.cu:238 / :484: key and value containers
+ * from DataType codes (keys I8..I512, values I8..I128), whole-key stable order. */
+rfx_status rfx_mgpu_sort_pair(void* keys, void* values, uint64_t n, uint64_t key_type,
+                              uint64_t value_type);
+rfx_status rfx_mgpu_sort_key(void* keys, uint64_t n, uint64_t key_type);
+
 /* ---------------------------------------------------------------- synthetic data */
 /* Column j of row i = lo[j] + mulhi64(rand(seed, stream_j, i), hi[j] - lo[j]) with the
  * SplitMix64 stream below, packed as `type`.  The generator behind the benchmarks. */

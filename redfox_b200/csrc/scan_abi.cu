@@ -6,6 +6,12 @@
 
 namespace rfx {
 
+rfx_status jit_aggregate(const ScanProgram& p, const void* in, uint64_t n, unsigned long long* gacc, uint32_t* done,
+                         uint64_t* out_keys, int64_t* out_sums, uint64_t* out_counts, uint64_t* d_groups, uint32_t* err,
+                         cudaStream_t stream);
+rfx_status jit_compact(const ScanProgram& p, int mode, const void* in, uint64_t n, void* out, uint64_t* d_count,
+                       uint64_t* status, uint32_t* counter, uint32_t* err, cudaStream_t stream, uint64_t tile_rows);
+
 template <int W>
 rfx_status launch_compact(int, uint32_t, const ScanLaunch&);
 template <int W>
@@ -54,7 +60,12 @@ size_t compact_workspace(uint64_t n) {
 
 rfx_status run_compact(int mode, const ScanProgram& p, void* out, uint64_t* d_count, const void* in,
                        uint64_t n, void* ws, size_t ws_bytes, void* stream) {
-  if (!out || !in || !d_count) return RFX_ERR_INVALID;
+  if (!d_count) return RFX_ERR_INVALID;
+  if (n == 0) {  // empty relation: nothing to read, the count is 0
+    RFX_CUDA_TRY(cudaMemsetAsync(d_count, 0, sizeof(uint64_t), as_stream(stream)));
+    return RFX_OK;
+  }
+  if (!out || !in) return RFX_ERR_INVALID;
   if (!aligned(in, p.in_bytes) || !aligned(out, mode == 0 ? p.in_bytes : p.out_bytes)) return RFX_ERR_INVALID;
   cudaStream_t s = as_stream(stream);
   uint32_t* err = device_error_word();
@@ -65,6 +76,9 @@ rfx_status run_compact(int mode, const ScanProgram& p, void* out, uint64_t* d_co
   uint32_t* counter = c.take<uint32_t>(1);
   if (!ws || ws_bytes < c.used) return RFX_ERR_WORKSPACE;
   RFX_CUDA_TRY(cudaMemsetAsync(ws, 0, c.used, s));
+  // the plan-specialised kernel when runtime compilation is available
+  rfx_status st = jit_compact(p, mode, in, n, out, d_count, status, counter, err, s, kScanTile);
+  if (st != RFX_ERR_UNSUPPORTED) return st;
   ScanLaunch a{&p, in, n, out, d_count, status, counter, err, s};
   return dispatch_compact(p.in_bytes, mode, mode == 0 ? p.in_bytes : p.out_bytes, a);
 }
@@ -110,6 +124,8 @@ rfx_status run_map(const ScanProgram& p, void* out, const void* in, uint64_t n, 
   if (!aligned(in, p.in_bytes) || !aligned(out, p.out_bytes)) return RFX_ERR_INVALID;
   uint32_t* err = device_error_word();
   if (!err) return RFX_ERR_CUDA;
+  rfx_status st = jit_compact(p, 2, in, n, out, nullptr, nullptr, nullptr, err, as_stream(stream), kScanTile);
+  if (st != RFX_ERR_UNSUPPORTED) return st;
   ScanLaunch a{&p, in, n, out, nullptr, nullptr, nullptr, err, as_stream(stream)};
   return dispatch_compact(p.in_bytes, 2, p.out_bytes, a);
 }
@@ -178,6 +194,8 @@ extern "C" rfx_status rfx_filter_aggregate(const void* in, uint64_t n, const rfx
   uint32_t* done = c.take<uint32_t>(1);
   if (!workspace || workspace_bytes < c.used) return RFX_ERR_WORKSPACE;
   RFX_CUDA_TRY(cudaMemsetAsync(workspace, 0, c.used, s));
+  st = jit_aggregate(p, in, n, gacc, done, out_keys, out_sums, out_counts, d_groups, err, s);
+  if (st != RFX_ERR_UNSUPPORTED) return st;
   AggLaunch a{&p, in, n, gacc, done, out_keys, out_sums, out_counts, d_groups, err, s};
   return dispatch_aggregate(p.in_bytes, a);
 }

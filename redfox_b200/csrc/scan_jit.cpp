@@ -1,0 +1,453 @@
+// scan_jit.cpp -- generates plan-specialised CUDA source for the scan kernels
+// (select / arith / project with compaction, and the fused filter-aggregate) from a
+// compiled ScanProgram.  The generated code computes exactly what the interpreting
+// kernels of scan_kernels.cuh compute -- same integer semantics, same row order, same
+// accumulation -- with every descriptor choice turned into a constant: fields are cut
+// from fixed limb positions of the row held in registers and each expression
+// instruction becomes one C statement.
+#include <cstdio>
+#include <sstream>
+#include <string>
+
+#include "host_common.h"
+#include "jit.h"
+#include "scan_program.h"
+
+namespace rfx {
+
+namespace {
+
+// Device helpers shared by all generated kernels (no headers are available to NVRTC).
+const char* kPreamble = R"RFX(
+typedef unsigned long long u64;
+typedef long long i64;
+typedef unsigned int u32;
+typedef int i32;
+typedef unsigned short u16;
+typedef unsigned char u8;
+struct __align__(16) U2 { u64 x, y; };
+
+static __device__ __forceinline__ u64 s32(u64 v) { return (u64)(i64)(i32)(u32)v; }
+static __device__ __forceinline__ u64 u32v(u64 v) { return (u64)(u32)v; }
+static __device__ __forceinline__ u64 divmod_s32(u64 a, u64 b, bool mod) {
+  const i32 x = (i32)(u32)a, y = (i32)(u32)b;
+  i32 r;
+  if (y == 0) r = 0;
+  else if (x == (i32)0x80000000u && y == -1) r = mod ? 0 : x;
+  else r = mod ? x % y : x / y;
+  return (u64)(i64)r;
+}
+static __device__ __forceinline__ u64 divmod_u32(u64 a, u64 b, bool mod) {
+  const u32 x = (u32)a, y = (u32)b;
+  return y == 0 ? 0ull : (u64)(mod ? x % y : x / y);
+}
+static __device__ __forceinline__ u64 divmod_s64(u64 a, u64 b, bool mod) {
+  const i64 x = (i64)a, y = (i64)b;
+  i64 r;
+  if (y == 0) r = 0;
+  else if (x == (i64)0x8000000000000000ull && y == -1) r = mod ? 0 : x;
+  else r = mod ? x % y : x / y;
+  return (u64)r;
+}
+static __device__ __forceinline__ u64 divmod_u64(u64 a, u64 b, bool mod) {
+  return b == 0 ? 0ull : (mod ? a % b : a / b);
+}
+static __device__ __forceinline__ void raise_error(u32* err, u32 code) {
+  if (err) atomicCAS(err, 0u, code);
+}
+static __device__ __forceinline__ u64 ld_relaxed_u64(const u64* p) {
+  u64 v;
+  asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+static __device__ __forceinline__ void st_relaxed_u64(u64* p, u64 v) {
+  asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+#define FLAG_AGG (1ull << 62)
+#define FLAG_INC (2ull << 62)
+#define VAL_MASK ((1ull << 62) - 1)
+#define SPIN_LIMIT (1u << 22)
+// warp 0 of a tile: publish the aggregate, return the exclusive prefix (bounded waits)
+static __device__ __forceinline__ u64 lookback(u64* status, u32 tile, u64 agg, u32* err) {
+  const u32 lane = threadIdx.x & 31;
+  if (tile == 0) {
+    if (lane == 0) st_relaxed_u64(&status[0], FLAG_INC | (agg & VAL_MASK));
+    return 0;
+  }
+  if (lane == 0) st_relaxed_u64(&status[tile], FLAG_AGG | (agg & VAL_MASK));
+  u64 prefix = 0;
+  long long base = (long long)tile - 1;
+  u32 spins = 0;
+  while (true) {
+    const long long idx = base - (long long)lane;
+    const u64 s = idx >= 0 ? ld_relaxed_u64(&status[idx]) : FLAG_INC;
+    const u64 flag = s & ~VAL_MASK;
+    const unsigned not_ready = __ballot_sync(0xffffffffu, flag == 0);
+    const unsigned inc = __ballot_sync(0xffffffffu, flag == FLAG_INC);
+    const unsigned upto = inc ? ((inc & (0u - inc)) << 1) - 1 : 0xffffffffu;
+    if (not_ready & upto) {
+      if (++spins > SPIN_LIMIT) { raise_error(err, 4u); break; }
+      __nanosleep(spins < 64 ? 20 : 200);
+      continue;
+    }
+    u64 v = ((upto >> lane) & 1u) ? (s & VAL_MASK) : 0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    prefix += v;
+    if (inc) break;
+    base -= 32;
+  }
+  if (lane == 0) st_relaxed_u64(&status[tile], FLAG_INC | ((prefix + agg) & VAL_MASK));
+  return prefix;
+}
+)RFX";
+
+std::string hex(uint64_t v) {
+  char b[32];
+  std::snprintf(b, sizeof(b), "0x%llxull", (unsigned long long)v);
+  return b;
+}
+
+uint64_t wmask(uint32_t w) { return w >= 64 ? ~0ull : ((1ull << w) - 1); }
+
+int limbs(uint32_t bytes) { return bytes <= 8 ? 1 : (int)(bytes / 8); }
+
+// Row load into u64 L[NL] / store from u64 O[NL].
+std::string load_code(uint32_t W, const std::string& dst, const std::string& idx) {
+  std::ostringstream s;
+  switch (W) {
+    case 1: s << dst << "[0] = __ldg(in + " << idx << ");"; break;
+    case 2: s << dst << "[0] = __ldg((const u16*)in + " << idx << ");"; break;
+    case 4: s << dst << "[0] = __ldg((const u32*)in + " << idx << ");"; break;
+    case 8: s << dst << "[0] = __ldg((const u64*)in + " << idx << ");"; break;
+    default: {
+      s << "{ const U2* p_ = (const U2*)(in + (" << idx << ") * " << W << "ull);";
+      for (uint32_t k = 0; k < W / 16; ++k)
+        s << " { U2 v_ = p_[" << k << "]; " << dst << "[" << 2 * k << "] = v_.x; " << dst << "[" << 2 * k + 1
+          << "] = v_.y; }";
+      s << " }";
+    }
+  }
+  return s.str();
+}
+
+std::string store_code(uint32_t W, const std::string& src, const std::string& idx) {
+  std::ostringstream s;
+  switch (W) {
+    case 1: s << "out[" << idx << "] = (u8)" << src << "[0];"; break;
+    case 2: s << "((u16*)out)[" << idx << "] = (u16)" << src << "[0];"; break;
+    case 4: s << "((u32*)out)[" << idx << "] = (u32)" << src << "[0];"; break;
+    case 8: s << "((u64*)out)[" << idx << "] = " << src << "[0];"; break;
+    default: {
+      s << "{ U2* p_ = (U2*)(out + (" << idx << ") * " << W << "ull);";
+      for (uint32_t k = 0; k < W / 16; ++k)
+        s << " { U2 v_; v_.x = " << src << "[" << 2 * k << "]; v_.y = " << src << "[" << 2 * k + 1 << "]; p_[" << k
+          << "] = v_; }";
+      s << " }";
+    }
+  }
+  return s.str();
+}
+
+std::string field_expr(const FieldLoc& f, int nl, const std::string& L) {
+  std::ostringstream s;
+  if (f.width == 0) return "0ull";
+  if (f.off == 0) {
+    s << "(" << L << "[" << (int)f.limb << "] & " << hex(wmask(f.width)) << ")";
+  } else if ((uint32_t)f.off + f.width <= 64 || f.limb + 1 >= nl) {
+    s << "((" << L << "[" << (int)f.limb << "] >> " << (int)f.off << ") & " << hex(wmask(f.width)) << ")";
+  } else {
+    s << "(((" << L << "[" << (int)f.limb << "] >> " << (int)f.off << ") | (" << L << "[" << (int)f.limb + 1 << "] << "
+      << 64 - f.off << ")) & " << hex(wmask(f.width)) << ")";
+  }
+  return s.str();
+}
+
+// Virtual field v as an expression (input field or appended field E<j>).
+std::string vfield(const ScanProgram& p, uint32_t v) {
+  if (v < p.nfields) return "F" + std::to_string(v);
+  return "E" + std::to_string(v - p.nfields);
+}
+
+// Per-row body: defines F<i>, `keep`, and (inside `if (keep)`) the E<j> values.
+std::string row_body(const ScanProgram& p, const std::string& L) {
+  std::ostringstream s;
+  const int nl = limbs(p.in_bytes);
+  for (uint32_t i = 0; i < p.nfields; ++i) s << "const u64 F" << i << " = " << field_expr(p.in_loc[i], nl, L) << ";\n";
+  s << "bool keep = true;\n";
+  static const char* ops[] = {"", "==", "!=", "<", "<", "<=", "<=", ">", ">", ">=", ">="};
+  for (uint32_t c = 0; c < p.ncmp; ++c) {
+    const CmpDesc& d = p.cmps[c];
+    std::string a = d.a_var ? "F" + std::to_string(d.a_field) : hex(d.a_const);
+    std::string b = d.b_var ? "F" + std::to_string(d.b_field) : hex(d.b_const);
+    s << "keep = keep && (((" << a << ") & " << hex(d.tmask) << ") " << ops[d.op] << " ((" << b << ") & "
+      << hex(d.tmask) << "));\n";
+  }
+  for (uint32_t j = 0; j < p.narith; ++j) s << "u64 E" << j << " = 0;\n";
+  if (p.ninstr) {
+    s << "if (keep) {\n";
+    for (int r = 0; r < kMaxRegs; ++r) s << "u64 R" << r << " = 0;\n";
+    for (uint32_t k = 0; k < p.ninstr; ++k) {
+      const Instr& in = p.code[k];
+      const std::string d = "R" + std::to_string(in.dst), a = "R" + std::to_string(in.a), b = "R" + std::to_string(in.b);
+      switch (in.op) {
+        case OP_FIELD: s << d << " = " << vfield(p, in.field) << " & " << hex(in.imm) << ";\n"; break;
+        case OP_CONST: s << d << " = " << hex(in.imm) << ";\n"; break;
+        case OP_ADD64: s << d << " = " << a << " + " << b << ";\n"; break;
+        case OP_SUB64: s << d << " = " << a << " - " << b << ";\n"; break;
+        case OP_MUL64: s << d << " = " << a << " * " << b << ";\n"; break;
+        case OP_ADD_S32: s << d << " = s32(" << a << " + " << b << ");\n"; break;
+        case OP_SUB_S32: s << d << " = s32(" << a << " - " << b << ");\n"; break;
+        case OP_MUL_S32: s << d << " = s32(" << a << " * " << b << ");\n"; break;
+        case OP_ADD_U32: s << d << " = u32v(" << a << " + " << b << ");\n"; break;
+        case OP_SUB_U32: s << d << " = u32v(" << a << " - " << b << ");\n"; break;
+        case OP_MUL_U32: s << d << " = u32v(" << a << " * " << b << ");\n"; break;
+        case OP_DIV_S32: s << d << " = divmod_s32(" << a << ", " << b << ", false);\n"; break;
+        case OP_MOD_S32: s << d << " = divmod_s32(" << a << ", " << b << ", true);\n"; break;
+        case OP_DIV_U32: s << d << " = divmod_u32(" << a << ", " << b << ", false);\n"; break;
+        case OP_MOD_U32: s << d << " = divmod_u32(" << a << ", " << b << ", true);\n"; break;
+        case OP_DIV_S64: s << d << " = divmod_s64(" << a << ", " << b << ", false);\n"; break;
+        case OP_MOD_S64: s << d << " = divmod_s64(" << a << ", " << b << ", true);\n"; break;
+        case OP_DIV_U64: s << d << " = divmod_u64(" << a << ", " << b << ", false);\n"; break;
+        case OP_MOD_U64: s << d << " = divmod_u64(" << a << ", " << b << ", true);\n"; break;
+        case OP_STORE_EXT: s << "E" << in.field << " = " << a << " & " << hex(in.imm) << ";\n"; break;
+        default: break;
+      }
+    }
+    s << "}\n";
+  }
+  return s.str();
+}
+
+constexpr int kJitThreads = 256;
+
+std::string gen_aggregate(const ScanProgram& p, bool priv) {
+  const int nl = limbs(p.in_bytes);
+  const uint32_t nv = p.nsum + 1;
+  std::ostringstream s;
+  s << kPreamble;
+  s << "#define NT " << kJitThreads << "\n#define NL " << nl << "\n#define G " << p.ngroups_total << "\n#define NV " << nv
+    << "\n#define NS " << p.nsum << "\n#define NACC (G * NV)\n";
+  s << "static __device__ __forceinline__ void process(const u64 (&L)[NL], u64* acc, u32 t, u32* err) {\n";
+  s << row_body(p, "L");
+  s << "if (!keep) return;\n";
+  s << "u32 g = 0;\nbool ok = true;\n";
+  for (uint32_t k = 0; k < p.ngroup; ++k) {
+    s << "{ const u64 gv = " << vfield(p, p.group_src[k]) << "; ok = ok && gv < " << p.group_domain[k] << "ull; g += (u32)gv * "
+      << p.group_stride[k] << "u; }\n";
+  }
+  s << "if (!ok) { raise_error(err, 3u); return; }\n";
+  s << "const u32 b = g * NV;\n";
+  for (uint32_t j = 0; j < p.nsum; ++j) {
+    if (priv)
+      s << "acc[(b + " << j << ") * NT + t] += " << vfield(p, p.sum_src[j]) << ";\n";
+    else
+      s << "atomicAdd((unsigned long long*)&acc[b + " << j << "], (unsigned long long)" << vfield(p, p.sum_src[j]) << ");\n";
+  }
+  if (priv) s << "acc[(b + NS) * NT + t] += 1ull;\n";
+  else s << "atomicAdd((unsigned long long*)&acc[b + NS], 1ull);\n";
+  s << "}\n";
+  s << R"RFX(
+extern "C" __global__ void __launch_bounds__(NT) rfx_plan_aggregate(
+    const u8* __restrict__ in, u64 n, unsigned long long* __restrict__ gacc, u32* __restrict__ done,
+    u64* __restrict__ out_keys, i64* __restrict__ out_sums, u64* __restrict__ out_counts,
+    u64* __restrict__ d_groups, u32* err) {
+  extern __shared__ __align__(16) u64 acc[];
+  __shared__ bool s_last;
+  const u32 t = threadIdx.x, lane = t & 31, warp = t >> 5;
+)RFX";
+  if (priv)
+    s << "  for (u32 k = 0; k < NACC; ++k) acc[k * NT + t] = 0;\n";
+  else
+    s << "  for (u32 k = t; k < NACC; k += NT) acc[k] = 0;\n  __syncthreads();\n";
+  s << "  const u64 stride = (u64)gridDim.x * NT;\n";
+  s << "  for (u64 i = (u64)blockIdx.x * NT + t; i < n; i += 2 * stride) {\n";
+  s << "    u64 L0[NL], L1[NL];\n    const u64 i1 = i + stride;\n";
+  s << "    " << load_code(p.in_bytes, "L0", "i") << "\n";
+  s << "    if (i1 < n) { " << load_code(p.in_bytes, "L1", "i1") << " }\n";
+  s << "    process(L0, acc, t, err);\n    if (i1 < n) process(L1, acc, t, err);\n  }\n  __syncthreads();\n";
+  if (priv)
+    s << R"RFX(
+  for (u32 k = warp; k < NACC; k += NT / 32) {
+    unsigned long long v = 0;
+    for (u32 tt = lane; tt < NT; tt += 32) v += acc[k * NT + tt];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0 && v) atomicAdd(&gacc[k], v);
+  }
+)RFX";
+  else
+    s << "  for (u32 k = t; k < NACC; k += NT) if (acc[k]) atomicAdd(&gacc[k], (unsigned long long)acc[k]);\n";
+  s << R"RFX(
+  __threadfence();
+  __syncthreads();
+  if (t == 0) s_last = atomicAdd(done, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  if (warp == 0) {
+    u64 written = 0;
+    for (u32 g0 = 0; g0 < G; g0 += 32) {
+      const u32 g = g0 + lane;
+      unsigned long long cnt = 0;
+      if (g < G) cnt = atomicAdd(&gacc[g * NV + NS], 0ull);
+      const unsigned m = __ballot_sync(0xffffffffu, cnt != 0);
+      if (cnt) {
+        const u64 pos = written + __popc(m & ((1u << lane) - 1u));
+        u64 key = 0;
+        u32 rem = g;
+)RFX";
+  for (uint32_t k = 0; k < p.ngroup; ++k) {
+    s << "        { const u32 v = rem / " << p.group_stride[k] << "u; rem -= v * " << p.group_stride[k] << "u; key = "
+      << (p.group_bits[k] >= 64 ? "(u64)v" : "(key << " + std::to_string(p.group_bits[k]) + ") | v") << "; }\n";
+  }
+  s << R"RFX(
+        out_keys[pos] = key;
+        out_counts[pos] = cnt;
+        for (u32 j = 0; j < NS; ++j) out_sums[pos * NS + j] = (i64)atomicAdd(&gacc[g * NV + j], 0ull);
+      }
+      written += __popc(m);
+    }
+    if (lane == 0) *d_groups = written;
+  }
+}
+)RFX";
+  return s.str();
+}
+
+// Compaction / map kernel.  mode 0: select (row unchanged), 1: select + project,
+// 2: map (no predicate, no compaction).
+std::string gen_compact(const ScanProgram& p, int mode, uint32_t wout, int rows_per_thread) {
+  const int nl = limbs(p.in_bytes);
+  const int no = limbs(wout);
+  std::ostringstream s;
+  s << kPreamble;
+  s << "#define NT " << kJitThreads << "\n#define NL " << nl << "\n#define NO " << no << "\n#define IPT "
+    << rows_per_thread << "\n#define TILE (NT * IPT)\n";
+  s << "static __device__ __forceinline__ bool process(const u64 (&L)[NL], u64 (&O)[NO]) {\n";
+  s << row_body(p, "L");
+  if (mode == 0) {
+    s << "for (int l = 0; l < NO; ++l) O[l] = L[l];\n";
+  } else {
+    s << "if (keep) {\n";
+    s << "for (int l = 0; l < NO; ++l) O[l] = 0;\n";
+    for (uint32_t k = 0; k < p.nout; ++k) {
+      const FieldLoc f = p.out_loc[k];
+      if (p.out_src[k] == 0xff || f.width == 0) continue;
+      const std::string v = "(" + vfield(p, p.out_src[k]) + " & " + hex(wmask(f.width)) + ")";
+      s << "O[" << (int)f.limb << "] |= " << v << " << " << (int)f.off << ";\n";
+      if (f.off && (uint32_t)f.off + f.width > 64 && f.limb + 1 < no)
+        s << "O[" << (int)f.limb + 1 << "] |= " << v << " >> " << 64 - f.off << ";\n";
+    }
+    s << "}\n";
+  }
+  s << "return keep;\n}\n";
+  s << R"RFX(
+extern "C" __global__ void __launch_bounds__(NT) rfx_plan_compact(
+    const u8* __restrict__ in, u64 n, u8* __restrict__ out, u64* __restrict__ d_count,
+    u64* __restrict__ status, u32* __restrict__ tile_counter, u32* err) {
+  __shared__ u32 s_cnt[IPT][NT / 32];
+  __shared__ u64 s_prefix;
+  __shared__ u32 s_tile;
+  const u32 t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const u64 num_tiles = (n + TILE - 1) / TILE;
+  for (u64 iter = 0;; ++iter) {
+)RFX";
+  if (mode == 2) {
+    s << "    const u64 tile = iter * gridDim.x + blockIdx.x;\n    if (tile >= num_tiles) break;\n";
+  } else {
+    s << "    if (t == 0) s_tile = atomicAdd(tile_counter, 1u);\n    __syncthreads();\n    const u64 tile = s_tile;\n"
+         "    if (tile >= num_tiles) break;\n";
+  }
+  s << "    u64 L[IPT][NL];\n    u64 O[IPT][NO];\n    bool sel[IPT];\n";
+  s << "#pragma unroll\n    for (int j = 0; j < IPT; ++j) {\n      const u64 i = tile * TILE + (u64)j * NT + t;\n"
+       "      if (i < n) { "
+    << load_code(p.in_bytes, "L[j]", "i") << " }\n    }\n";
+  s << "#pragma unroll\n    for (int j = 0; j < IPT; ++j) {\n      const u64 i = tile * TILE + (u64)j * NT + t;\n"
+       "      sel[j] = i < n ? process(L[j], O[j]) : false;\n    }\n";
+  if (mode == 2) {
+    s << "#pragma unroll\n    for (int j = 0; j < IPT; ++j) {\n      const u64 i = tile * TILE + (u64)j * NT + t;\n"
+         "      if (i < n) { "
+      << store_code(wout, "O[j]", "i") << " }\n    }\n  }\n}\n";
+    return s.str();
+  }
+  s << R"RFX(
+    u32 rank[IPT];
+#pragma unroll
+    for (int j = 0; j < IPT; ++j) {
+      const unsigned b = __ballot_sync(0xffffffffu, sel[j]);
+      rank[j] = __popc(b & ((1u << lane) - 1u));
+      if (lane == 0) s_cnt[j][warp] = __popc(b);
+    }
+    __syncthreads();
+    if (warp == 0) {
+      const u32 NC = IPT * (NT / 32);
+      u32 c = lane < NC ? s_cnt[lane / (NT / 32)][lane % (NT / 32)] : 0u;
+      u32 incl = c;
+      for (int o = 1; o < 32; o <<= 1) {
+        const u32 v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (u32)o) incl += v;
+      }
+      const u32 total = __shfl_sync(0xffffffffu, incl, 31);
+      if (lane < NC) s_cnt[lane / (NT / 32)][lane % (NT / 32)] = incl - c;
+      const u64 prefix = lookback(status, (u32)tile, total, err);
+      if (lane == 0) {
+        s_prefix = prefix;
+        if (tile == num_tiles - 1) *d_count = prefix + total;
+      }
+    }
+    __syncthreads();
+    const u64 base = s_prefix;
+#pragma unroll
+    for (int j = 0; j < IPT; ++j) {
+      if (sel[j]) {
+        const u64 pos = base + s_cnt[j][warp] + rank[j];
+        if (pos < n) {
+)RFX";
+  s << "          " << store_code(wout, "O[j]", "pos") << "\n";
+  s << R"RFX(
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+)RFX";
+  return s.str();
+}
+
+}  // namespace
+
+// Launches the specialised aggregate kernel; RFX_ERR_UNSUPPORTED when it cannot be
+// compiled (the caller falls back to the interpreting kernel).
+rfx_status jit_aggregate(const ScanProgram& p, const void* in, uint64_t n, unsigned long long* gacc, uint32_t* done,
+                         uint64_t* out_keys, int64_t* out_sums, uint64_t* out_counts, uint64_t* d_groups, uint32_t* err,
+                         cudaStream_t stream) {
+  const uint32_t nacc = p.ngroups_total * (p.nsum + 1);
+  const bool priv = nacc <= 24;
+  cudaKernel_t k;
+  rfx_status st = jit_kernel(gen_aggregate(p, priv), "rfx_plan_aggregate", &k);
+  if (st != RFX_OK) return st;
+  const size_t smem = (priv ? (size_t)nacc * kJitThreads : (size_t)nacc) * sizeof(uint64_t);
+  RFX_CUDA_TRY(allow_smem((const void*)k, smem));
+  const uint64_t blocks = (n + 2ull * kJitThreads - 1) / (2ull * kJitThreads);
+  const int grid = persistent_grid((const void*)k, kJitThreads, smem, blocks ? blocks : 1);
+  void* args[] = {(void*)&in, (void*)&n, (void*)&gacc, (void*)&done, (void*)&out_keys, (void*)&out_sums,
+                  (void*)&out_counts, (void*)&d_groups, (void*)&err};
+  RFX_CUDA_TRY(cudaLaunchKernel((const void*)k, dim3(grid), dim3(kJitThreads), args, smem, stream));
+  return RFX_OK;
+}
+
+rfx_status jit_compact(const ScanProgram& p, int mode, const void* in, uint64_t n, void* out, uint64_t* d_count,
+                       uint64_t* status, uint32_t* counter, uint32_t* err, cudaStream_t stream, uint64_t tile_rows) {
+  const uint32_t wout = mode == 0 ? p.in_bytes : p.out_bytes;
+  const int ipt = (int)(tile_rows / kJitThreads);
+  cudaKernel_t k;
+  rfx_status st = jit_kernel(gen_compact(p, mode, wout, ipt), "rfx_plan_compact", &k);
+  if (st != RFX_OK) return st;
+  const uint64_t tiles = (n + tile_rows - 1) / tile_rows;
+  const int grid = persistent_grid((const void*)k, kJitThreads, 0, tiles ? tiles : 1);
+  void* args[] = {(void*)&in, (void*)&n, (void*)&out, (void*)&d_count, (void*)&status, (void*)&counter, (void*)&err};
+  RFX_CUDA_TRY(cudaLaunchKernel((const void*)k, dim3(grid), dim3(kJitThreads), args, 0, stream));
+  return RFX_OK;
+}
+
+}  // namespace rfx

@@ -1,0 +1,327 @@
+// sort_kernels.cuh -- stable LSD radix sort of packed keys (with optional values):
+// one histogram pass over the keys for every digit, then one "onesweep" kernel per 8-bit
+// digit that ranks a tile with warp match/ballot, publishes per-digit tile counts through
+// decoupled look-back, and scatters through shared memory so that global writes go out
+// in digit runs.
+//
+// Keys are containers of K bytes (1..64), sorted on bits [begin_bit, end_bit) as
+// unsigned integers, values V bytes (0 = keys only).  The sort is stable, so it orders
+// exactly like b40c's LSD sort on bits [0, key_bits) (b40cSort.cu:58-1022) and like
+// moderngpu's stable merge sort when the range covers the whole key (ModernGPUSort.cu).
+#pragma once
+
+#include "rfx_device.cuh"
+
+namespace rfx {
+
+constexpr int kSortThreads = 256;
+constexpr int kRadix = 256;
+constexpr int kSortWarps = kSortThreads / 32;
+constexpr int kMaxSortPasses = 16;  // up to 128 key bits per call
+
+// Items per thread by the bytes moved per item.
+template <int K, int V>
+struct SortTuning {
+  static constexpr int B = K + V;
+  static constexpr int IPT = B <= 8 ? 16 : B <= 16 ? 12 : B <= 32 ? 8 : B <= 64 ? 4 : 2;
+  static constexpr int TILE = kSortThreads * IPT;
+  static constexpr int SBYTES = (K > V ? K : V);
+};
+
+// A K-byte element as 32-bit words (1- and 2-byte elements zero-extended into w[0]).
+template <int B>
+struct Elem {
+  static constexpr int NW = B <= 4 ? 1 : B / 4;
+  uint32_t w[NW];
+};
+
+template <int B>
+__device__ __forceinline__ Elem<B> load_elem(const uint8_t* base, uint64_t i) {
+  Elem<B> e;
+  if constexpr (B == 1) {
+    e.w[0] = base[i];
+  } else if constexpr (B == 2) {
+    e.w[0] = reinterpret_cast<const uint16_t*>(base)[i];
+  } else if constexpr (B == 4) {
+    e.w[0] = reinterpret_cast<const uint32_t*>(base)[i];
+  } else if constexpr (B == 8) {
+    uint2 v = reinterpret_cast<const uint2*>(base)[i];
+    e.w[0] = v.x;
+    e.w[1] = v.y;
+  } else {
+    const uint4* p = reinterpret_cast<const uint4*>(base + i * B);
+#pragma unroll
+    for (int k = 0; k < B / 16; ++k) {
+      uint4 v = p[k];
+      e.w[4 * k] = v.x;
+      e.w[4 * k + 1] = v.y;
+      e.w[4 * k + 2] = v.z;
+      e.w[4 * k + 3] = v.w;
+    }
+  }
+  return e;
+}
+
+template <int B>
+__device__ __forceinline__ void store_elem(uint8_t* base, uint64_t i, const Elem<B>& e) {
+  if constexpr (B == 1) {
+    base[i] = (uint8_t)e.w[0];
+  } else if constexpr (B == 2) {
+    reinterpret_cast<uint16_t*>(base)[i] = (uint16_t)e.w[0];
+  } else if constexpr (B == 4) {
+    reinterpret_cast<uint32_t*>(base)[i] = e.w[0];
+  } else if constexpr (B == 8) {
+    reinterpret_cast<uint2*>(base)[i] = make_uint2(e.w[0], e.w[1]);
+  } else {
+    uint4* p = reinterpret_cast<uint4*>(base + i * B);
+#pragma unroll
+    for (int k = 0; k < B / 16; ++k) p[k] = make_uint4(e.w[4 * k], e.w[4 * k + 1], e.w[4 * k + 2], e.w[4 * k + 3]);
+  }
+}
+
+// Bits [shift, shift + 8) of the element (the caller masks to the digit width).
+template <int K>
+__device__ __forceinline__ uint32_t elem_bits(const Elem<K>& e, uint32_t shift) {
+  if constexpr (Elem<K>::NW == 1) {
+    return e.w[0] >> shift;
+  } else {
+    const uint32_t q = shift >> 5, r = shift & 31;
+    uint32_t lo = 0, hi = 0;
+#pragma unroll
+    for (int k = 0; k < Elem<K>::NW; ++k) {
+      lo = (k == (int)q) ? e.w[k] : lo;
+      hi = (k == (int)q + 1) ? e.w[k] : hi;
+    }
+    return r ? ((lo >> r) | (hi << (32 - r))) : lo;
+  }
+}
+
+struct SortPassArgs {
+  const uint8_t* keys_in;
+  uint8_t* keys_out;
+  const uint8_t* vals_in;
+  uint8_t* vals_out;
+  uint64_t n;
+  uint32_t shift;       // first bit of this digit
+  uint32_t mask;        // digit mask (0xff, or fewer bits for the last digit)
+  const uint32_t* gexcl;  // exclusive global digit offsets of this pass [256]
+  uint32_t* status;     // [tiles][256] look-back words of this pass
+  uint32_t* tile_counter;
+  uint32_t* err;
+};
+
+// 32-bit look-back words: bits 31..30 flag (1 aggregate, 2 inclusive), 29..0 value.
+constexpr uint32_t kSFlagAgg = 1u << 30;
+constexpr uint32_t kSFlagInc = 2u << 30;
+constexpr uint32_t kSValMask = (1u << 30) - 1;
+
+__device__ __forceinline__ uint32_t ld_relaxed_u32(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.relaxed.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_relaxed_u32(uint32_t* p, uint32_t v) {
+  asm volatile("st.relaxed.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// ------------------------------------------------------------------ histogram
+// Counts every pass's digits in one read of the keys (warp-aggregated shared atomics),
+// then the last block turns the counts into exclusive offsets and flags trivial passes.
+template <int K>
+__global__ void __launch_bounds__(kSortThreads)
+sort_histogram_kernel(const uint8_t* __restrict__ keys, uint64_t n, uint32_t begin_bit, uint32_t end_bit,
+                      uint32_t passes, uint32_t* __restrict__ ghist, uint32_t* __restrict__ trivial,
+                      uint32_t* __restrict__ done_counter) {
+  __shared__ uint32_t h[kMaxSortPasses][kRadix];
+  __shared__ bool s_last;
+  const uint32_t t = threadIdx.x, lane = t & 31;
+  for (uint32_t k = t; k < passes * kRadix; k += kSortThreads) (&h[0][0])[k] = 0;
+  __syncthreads();
+  const uint64_t stride = (uint64_t)gridDim.x * kSortThreads;
+  const uint64_t nround = (n + stride - 1) / stride * stride;  // whole warps stay converged
+  for (uint64_t i = (uint64_t)blockIdx.x * kSortThreads + t; i < nround; i += stride) {
+    const bool valid = i < n;
+    Elem<K> e;
+    if (valid) e = load_elem<K>(keys, i);
+    for (uint32_t p = 0; p < passes; ++p) {
+      const uint32_t shift = begin_bit + 8 * p;
+      const uint32_t w = end_bit - shift < 8 ? end_bit - shift : 8;
+      const uint32_t d = valid ? (elem_bits<K>(e, shift) & ((1u << w) - 1)) : kRadix;
+      const unsigned peers = __match_any_sync(0xffffffffu, d);
+      if (valid && (peers & ((1u << lane) - 1)) == 0) atomicAdd(&h[p][d], (uint32_t)__popc(peers));
+    }
+  }
+  __syncthreads();
+  for (uint32_t k = t; k < passes * kRadix; k += kSortThreads) {
+    const uint32_t c = (&h[0][0])[k];
+    if (c) atomicAdd(&ghist[k], c);
+  }
+  __threadfence();
+  __syncthreads();
+  if (t == 0) s_last = atomicAdd(done_counter, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  // exclusive scan per pass (one warp per pass)
+  const uint32_t warp = t >> 5;
+  for (uint32_t p = warp; p < passes; p += kSortWarps) {
+    uint32_t run = 0, maxc = 0;
+    for (uint32_t d0 = 0; d0 < kRadix; d0 += 32) {
+      const uint32_t c = atomicAdd(&ghist[p * kRadix + d0 + lane], 0u);
+      maxc = max(maxc, c);
+      uint32_t incl = c;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (uint32_t)o) incl += v;
+      }
+      ghist[p * kRadix + d0 + lane] = run + incl - c;
+      run += __shfl_sync(0xffffffffu, incl, 31);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) maxc = max(maxc, __shfl_xor_sync(0xffffffffu, maxc, o));
+    if (lane == 0) trivial[p] = (uint64_t)maxc == n ? 1u : 0u;
+  }
+}
+
+// ------------------------------------------------------------------ onesweep pass
+template <int K, int V>
+__global__ void __launch_bounds__(kSortThreads)
+sort_pass_kernel(const SortPassArgs a) {
+  using T = SortTuning<K, V>;
+  constexpr int IPT = T::IPT;
+  constexpr int TILE = T::TILE;
+  extern __shared__ __align__(16) uint8_t sbuf[];              // TILE * SBYTES scatter buffer
+  __shared__ uint32_t whist[kSortWarps][kRadix];               // per-warp digit counts
+  __shared__ uint32_t s_local[kRadix];                         // tile-local digit start
+  __shared__ uint32_t s_global[kRadix];                        // global base of the digit run
+  __shared__ uint8_t s_dig[TILE];                              // digit of each sorted slot
+  __shared__ uint32_t s_scan[kSortWarps];
+  __shared__ uint32_t s_tile;
+  const uint32_t t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const uint64_t num_tiles = (a.n + TILE - 1) / TILE;
+
+  while (true) {
+    if (t == 0) s_tile = atomicAdd(a.tile_counter, 1u);
+    for (uint32_t k = t; k < kSortWarps * kRadix; k += kSortThreads) (&whist[0][0])[k] = 0;
+    __syncthreads();
+    const uint64_t tile = s_tile;
+    if (tile >= num_tiles) break;
+    const uint64_t tbase = tile * TILE;
+    const uint32_t tcount = (uint32_t)min((uint64_t)TILE, a.n - tbase);
+    // warp w owns items [w*32*IPT, (w+1)*32*IPT) of the tile, item j of lane l at j*32+l
+    const uint32_t wbase = warp * 32 * IPT;
+    Elem<K> key[IPT];
+    uint32_t dig[IPT], rank[IPT];
+#pragma unroll
+    for (int j = 0; j < IPT; ++j) {
+      const uint32_t li = wbase + j * 32 + lane;
+      if (li < tcount) key[j] = load_elem<K>(a.keys_in, tbase + li);
+    }
+#pragma unroll
+    for (int j = 0; j < IPT; ++j) {
+      const uint32_t li = wbase + j * 32 + lane;
+      const bool valid = li < tcount;
+      const uint32_t d = valid ? (elem_bits<K>(key[j], a.shift) & a.mask) : kRadix + 1;
+      dig[j] = d;
+      const unsigned peers = __match_any_sync(0xffffffffu, d);
+      const unsigned lower = peers & ((1u << lane) - 1);
+      uint32_t base = 0;
+      if (valid) base = whist[warp][d];
+      rank[j] = base + __popc(lower);
+      __syncwarp();
+      if (valid && lower == 0) whist[warp][d] = base + __popc(peers);
+      __syncwarp();
+    }
+    __syncthreads();
+    // per digit: exclusive over warps, tile count, tile-local start, look-back
+    uint32_t count = 0;
+    if (t < kRadix) {
+#pragma unroll
+      for (int w = 0; w < kSortWarps; ++w) {
+        const uint32_t c = whist[w][t];
+        whist[w][t] = count;
+        count += c;
+      }
+    }
+    // block exclusive scan of count over the 256 digits
+    uint32_t incl = count;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= (uint32_t)o) incl += v;
+    }
+    if (lane == 31) s_scan[warp] = incl;
+    __syncthreads();
+    if (t < kRadix) {
+      uint32_t wpre = 0;
+      for (uint32_t w = 0; w < warp; ++w) wpre += s_scan[w];
+      s_local[t] = wpre + incl - count;
+      // decoupled look-back for this digit
+      uint32_t* st = a.status + tile * kRadix + t;
+      uint32_t prefix = 0;
+      if (tile == 0) {
+        st_relaxed_u32(st, kSFlagInc | count);
+      } else {
+        st_relaxed_u32(st, kSFlagAgg | count);
+        int64_t p = (int64_t)tile - 1;
+        uint32_t spins = 0;
+        while (p >= 0) {
+          const uint32_t s = ld_relaxed_u32(a.status + (uint64_t)p * kRadix + t);
+          if ((s & ~kSValMask) == 0) {
+            if (++spins > kSpinLimit) {
+              raise_error(a.err, kErrTimeout);
+              break;
+            }
+            __nanosleep(spins < 64 ? 20 : 100);
+            continue;
+          }
+          prefix += s & kSValMask;
+          if (s & kSFlagInc) break;
+          --p;
+        }
+        st_relaxed_u32(st, kSFlagInc | ((prefix + count) & kSValMask));
+      }
+      s_global[t] = a.gexcl[t] + prefix;
+    }
+    __syncthreads();
+    // keys: scatter into tile order in shared memory, then out in digit runs
+    Elem<K>* skeys = reinterpret_cast<Elem<K>*>(sbuf);
+    uint32_t lpos[IPT];
+#pragma unroll
+    for (int j = 0; j < IPT; ++j) {
+      const uint32_t li = wbase + j * 32 + lane;
+      if (li < tcount) {
+        const uint32_t d = dig[j];
+        lpos[j] = s_local[d] + whist[warp][d] + rank[j];
+        skeys[lpos[j]] = key[j];
+      }
+    }
+    __syncthreads();
+    for (uint32_t i = t; i < tcount; i += kSortThreads) {
+      const Elem<K> k = skeys[i];
+      const uint32_t d = elem_bits<K>(k, a.shift) & a.mask;
+      s_dig[i] = (uint8_t)d;
+      const uint64_t pos = (uint64_t)s_global[d] + (i - s_local[d]);
+      if (pos < a.n) store_elem<K>(a.keys_out, pos, k);
+    }
+    if constexpr (V > 0) {
+      __syncthreads();
+      Elem<V>* svals = reinterpret_cast<Elem<V>*>(sbuf);
+#pragma unroll
+      for (int j = 0; j < IPT; ++j) {
+        const uint32_t li = wbase + j * 32 + lane;
+        if (li < tcount) svals[lpos[j]] = load_elem<V>(a.vals_in, tbase + li);
+      }
+      __syncthreads();
+      for (uint32_t i = t; i < tcount; i += kSortThreads) {
+        const uint32_t d = s_dig[i];
+        const uint64_t pos = (uint64_t)s_global[d] + (i - s_local[d]);
+        if (pos < a.n) store_elem<V>(a.vals_out, pos, svals[i]);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace rfx

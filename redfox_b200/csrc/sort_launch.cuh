@@ -1,0 +1,124 @@
+// sort_launch.cuh -- host launchers of the radix sort, instantiated per key width in
+// sort_k{1,2,4,8,16,32,64}.cu.
+#pragma once
+
+#include "host_common.h"
+#include "sort_kernels.cuh"
+
+namespace rfx {
+
+struct SortPlan {
+  uint8_t* keys;
+  uint8_t* vals;
+  uint8_t* alt_keys;
+  uint8_t* alt_vals;
+  uint64_t n;
+  uint32_t begin_bit;
+  uint32_t end_bit;     // end_bit - begin_bit <= 128
+  uint32_t passes;
+  uint32_t* ghist;      // [passes][256]
+  uint32_t* trivial;    // [passes]
+  uint32_t* done;       // 1
+  uint32_t* counters;   // [passes]
+  uint32_t* status;     // [passes][tiles][256]
+  uint64_t tiles;
+  bool skip_trivial;
+  uint32_t* host_trivial;  // pinned or pageable host copy for skip_trivial
+  uint32_t* err;
+  cudaStream_t stream;
+  int executed;         // out: passes run
+  bool in_alt;          // out: the sorted data ended in the alternate buffers
+};
+
+template <int K, int V>
+uint64_t sort_tiles(uint64_t n) {
+  return (n + SortTuning<K, V>::TILE - 1) / SortTuning<K, V>::TILE;
+}
+
+template <int K, int V>
+rfx_status run_sort_kv(SortPlan& s) {
+  using T = SortTuning<K, V>;
+  // histogram of every digit
+  {
+    auto hk = sort_histogram_kernel<K>;
+    const uint64_t blocks = (s.n + kSortThreads * 8 - 1) / (kSortThreads * 8);
+    const int grid = persistent_grid((const void*)hk, kSortThreads, 0, blocks ? blocks : 1);
+    hk<<<grid, kSortThreads, 0, s.stream>>>(s.keys, s.n, s.begin_bit, s.end_bit, s.passes, s.ghist, s.trivial, s.done);
+    RFX_CUDA_TRY(cudaGetLastError());
+  }
+  uint32_t triv[kMaxSortPasses] = {0};
+  if (s.skip_trivial) {
+    RFX_CUDA_TRY(cudaMemcpyAsync(s.host_trivial, s.trivial, s.passes * sizeof(uint32_t), cudaMemcpyDeviceToHost, s.stream));
+    RFX_CUDA_TRY(cudaStreamSynchronize(s.stream));
+    for (uint32_t p = 0; p < s.passes; ++p) triv[p] = s.host_trivial[p];
+  }
+  constexpr size_t ek = sizeof(Elem<K>), ev = V > 0 ? sizeof(Elem<V>) : 0;
+  const size_t smem = (size_t)T::TILE * (ek > ev ? ek : ev);
+  auto pk = sort_pass_kernel<K, V>;
+  RFX_CUDA_TRY(allow_smem((const void*)pk, smem));
+  const int grid = persistent_grid((const void*)pk, kSortThreads, smem, s.tiles ? s.tiles : 1);
+  const uint8_t* kin = s.keys;
+  const uint8_t* vin = s.vals;
+  uint8_t* kout = s.alt_keys;
+  uint8_t* vout = s.alt_vals;
+  s.executed = 0;
+  s.in_alt = false;
+  for (uint32_t p = 0; p < s.passes; ++p) {
+    if (triv[p]) continue;
+    SortPassArgs a;
+    a.keys_in = kin;
+    a.keys_out = kout;
+    a.vals_in = vin;
+    a.vals_out = vout;
+    a.n = s.n;
+    a.shift = s.begin_bit + 8 * p;
+    const uint32_t w = s.end_bit - a.shift < 8 ? s.end_bit - a.shift : 8;
+    a.mask = (1u << w) - 1;
+    a.gexcl = s.ghist + p * kRadix;
+    a.status = s.status + (uint64_t)p * s.tiles * kRadix;
+    a.tile_counter = s.counters + p;
+    a.err = s.err;
+    pk<<<grid, kSortThreads, smem, s.stream>>>(a);
+    RFX_CUDA_TRY(cudaGetLastError());
+    ++s.executed;
+    s.in_alt = !s.in_alt;
+    const uint8_t* tk = kout;
+    const uint8_t* tv = vout;
+    kout = const_cast<uint8_t*>(kin);
+    vout = const_cast<uint8_t*>(vin);
+    kin = tk;
+    vin = tv;
+  }
+  return RFX_OK;
+}
+
+template <int K>
+rfx_status run_sort(SortPlan& s, uint32_t vbytes) {
+  switch (vbytes) {
+    case 0: return run_sort_kv<K, 0>(s);
+    case 1: return run_sort_kv<K, 1>(s);
+    case 2: return run_sort_kv<K, 2>(s);
+    case 4: return run_sort_kv<K, 4>(s);
+    case 8: return run_sort_kv<K, 8>(s);
+    case 16: return run_sort_kv<K, 16>(s);
+    default: return RFX_ERR_UNSUPPORTED;
+  }
+}
+
+template <int K>
+uint64_t sort_tiles_for(uint64_t n, uint32_t vbytes) {
+  switch (vbytes) {
+    case 0: return sort_tiles<K, 0>(n);
+    case 1: return sort_tiles<K, 1>(n);
+    case 2: return sort_tiles<K, 2>(n);
+    case 4: return sort_tiles<K, 4>(n);
+    case 8: return sort_tiles<K, 8>(n);
+    default: return sort_tiles<K, 16>(n);
+  }
+}
+
+#define RFX_INSTANTIATE_SORT(K)                                  \
+  template rfx_status run_sort<K>(SortPlan&, uint32_t);          \
+  template uint64_t sort_tiles_for<K>(uint64_t, uint32_t);
+
+}  // namespace rfx

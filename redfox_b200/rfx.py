@@ -77,6 +77,12 @@ def _load():
         "rfx_filter_aggregate_workspace": (sz, [u64, P, P, u32, u32]),
         "rfx_filter_aggregate": (st, [P, u64, P, P, u32, P, u32, P, P, u32, P, u32, P, P, P, P, P, sz, P]),
         "rfx_gen_uniform_rows": (st, [P, u64, P, u64, P, P, P]),
+        "rfx_sort_workspace": (sz, [u64, u32, u32, u32, u32]),
+        "rfx_sort_pairs": (st, [P, P, u64, u32, u32, u32, u32, u32, P, sz, P]),
+        "rfx_b40c_sort_pair": (st, [P, P, u64, u64, u64]),
+        "rfx_b40c_sort_key": (st, [P, u64, u64]),
+        "rfx_mgpu_sort_pair": (st, [P, P, u64, u64, u64]),
+        "rfx_mgpu_sort_key": (st, [P, u64, u64]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -270,3 +276,35 @@ def filter_aggregate(rows, widths, cmps, ariths, group_fields, group_domain, sum
                          device=rows.device)
     fa.launch(rows, stream=stream)
     return fa.result()
+
+
+# ---------------------------------------------------------------------------- sort
+SORT_SKIP_TRIVIAL = 1
+
+
+def _width(t):
+    """Bytes per element of a 1-D (dtype) or 2-D (uint8 rows) tensor."""
+    return t.element_size() if t.dim() == 1 else t.shape[1] * t.element_size()
+
+
+class Sorter:
+    """A prepared stable radix sort (workspace allocated once)."""
+
+    def __init__(self, n, key_bytes, value_bytes=0, begin_bit=0, end_bit=None, device="cuda"):
+        self.n, self.kb, self.vb = n, key_bytes, value_bytes
+        self.begin = begin_bit
+        self.end = key_bytes * 8 if end_bit is None else end_bit
+        self.wsb = LIB.rfx_sort_workspace(n, key_bytes, value_bytes, self.begin, self.end)
+        self.ws = _empty_bytes(self.wsb, device)
+
+    def __call__(self, keys, values=None, flags=0, stream=None):
+        check("rfx_sort_pairs", LIB.rfx_sort_pairs(_ptr(keys), _ptr(values), self.n, self.kb, self.vb, self.begin,
+                                                   self.end, flags, _ptr(self.ws), self.wsb, _stream(stream)))
+
+
+def sort_pairs(keys, values=None, begin_bit=0, end_bit=None, flags=0, stream=None):
+    """Sort keys (and values) in place; returns them."""
+    n = keys.shape[0]
+    s = Sorter(n, _width(keys), 0 if values is None else _width(values), begin_bit, end_bit, device=keys.device)
+    s(keys, values, flags, stream)
+    return keys, values

@@ -11,6 +11,17 @@ from helpers import fact_oracle, fact_rows_oracle, oracle_arith, oracle_cmps, to
 pytestmark = pytest.mark.gpu
 
 
+@pytest.fixture(autouse=True, params=["jit", "interp"])
+def kernel_path(request, monkeypatch):
+    """Every case runs on the plan-specialised (runtime-compiled) kernels and on the
+    interpreting kernels (RFX_JIT=0)."""
+    if request.param == "interp":
+        monkeypatch.setenv("RFX_JIT", "0")
+    else:
+        monkeypatch.delenv("RFX_JIT", raising=False)
+    return request.param
+
+
 def _rows_to_dev(rows, cuda):
     import torch
     return torch.from_numpy(np.ascontiguousarray(rows)).to(cuda)

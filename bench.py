@@ -397,7 +397,7 @@ def main_ours(args):
                        "parallelism": "dp%d (row partitions, 6-group all-reduce)" % world if world > 1 else "1 GPU"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": "scan_aggregate_kernel<64,true>", "kernel_ms": kms,
+                         "kernel": "rfx_plan_aggregate (plan-specialised scan_aggregate_kernel<64>)", "kernel_ms": kms,
                          "algorithmic_bytes_per_launch": bytes_alg},
             "cpu_baseline": cpu,
             "e2e": {"value": world * n / (e2e_ms / 1e3), "unit": "tuples/s", "ms_per_step": e2e_ms,

@@ -182,6 +182,43 @@ rfx_status rfx_mgpu_sort_pair(void* keys, void* values, uint64_t n, uint64_t key
                               uint64_t value_type);
 rfx_status rfx_mgpu_sort_key(void* keys, uint64_t n, uint64_t key_type);
 
+/* ---------------------------------------------------------------- reduce / count */
+/* Value kinds of rfx_reduce_by_key. */
+enum { RFX_VAL_NONE = 0, RFX_VAL_U32 = 1, RFX_VAL_I64 = 2 };
+
+size_t rfx_reduce_by_key_workspace(uint64_t n);
+
+/* Reduce-by-key over runs of equal keys (thrust::reduce_by_key with equal_to / plus, the
+ * body of every Reduce.cu entry: count_* :175-660, total_* :665-1536).  keys: n
+ * containers of key_bytes (1/2/4/8/16/32), compared bitwise; values: int64
+ * (RFX_VAL_I64, exact int64 sums -- the reference has only double and u32 sums), u32
+ * (RFX_VAL_U32, u32 sums as count_* computes them) or none (RFX_VAL_NONE).  Writes, per
+ * run in input order, the run key, its sum (out_values, same type as the values; may be
+ * NULL) and its length (out_counts, u32; may be NULL), and *d_groups = the number of
+ * runs.  If d_n is not NULL the element count is min(n, *d_n), read on the device (n is
+ * then the capacity the launch is sized for). */
+rfx_status rfx_reduce_by_key(const void* keys, uint64_t n, const uint64_t* d_n, uint32_t key_bytes,
+                             const void* values, uint32_t value_kind, void* out_keys,
+                             void* out_values, uint32_t* out_counts, uint64_t* d_groups,
+                             void* workspace, size_t workspace_bytes, void* stream);
+
+/* redfox::count_{8,16,32,128,256} (Reduce.cu:175-660, Reduce.h:43-83) with the reference's
+ * argument meaning: *key_size / *value_size are device-resident byte counts, read on
+ * entry and replaced by the output byte counts; the u32 value column is summed per run.
+ * key_bytes = 1, 2, 4, 16 or 32.  Synchronous on the default stream, like the reference. */
+rfx_status rfx_count_compat(const void* key_begin, const void* value_begin, void* result_key_begin,
+                            void* result_value_begin, uint64_t* key_size, uint64_t* value_size,
+                            uint32_t key_bytes);
+/* redfox::total_64_32 (Reduce.cu:1138-1215): u64 keys, u32 value sums. */
+rfx_status rfx_total_64_32_compat(const void* key_begin, const void* value_begin,
+                                  void* result_key_begin, void* result_value_begin,
+                                  uint64_t* key_size, uint64_t* value_size);
+/* The exact int64 SUM with the same byte-size convention (no reference counterpart: the
+ * reference's total_* entries sum doubles). */
+rfx_status rfx_total_i64_compat(const void* key_begin, const void* value_begin,
+                                void* result_key_begin, void* result_value_begin,
+                                uint64_t* key_size, uint64_t* value_size, uint32_t key_bytes);
+
 /* ---------------------------------------------------------------- synthetic data */
 /* Column j of row i = lo[j] + mulhi64(rand(seed, stream_j, i), hi[j] - lo[j]) with the
  * SplitMix64 stream below, packed as `type`.  The generator behind the benchmarks. */

@@ -1,0 +1,181 @@
+// reduce_abi.cu -- C ABI of reduce-by-key / count, and the reference-compatible
+// count_* / total_64_32 entries with device-resident byte sizes (Reduce.cu).
+#include <cstring>
+
+#include "host_common.h"
+#include "reduce_kernels.cuh"
+
+namespace rfx {
+namespace {
+
+struct RedLayout {
+  uint32_t* flags;
+  uint32_t* counter;
+  SegPair* agg;
+  SegPair* inc;
+  SegPair* cagg;
+  SegPair* cinc;
+  size_t clear_bytes;
+  size_t total;
+};
+
+RedLayout red_layout(void* ws, uint64_t n) {
+  RedLayout L;
+  const uint64_t tiles = (n + kRedTile - 1) / kRedTile + 1;
+  Carver c(ws);
+  L.flags = c.take<uint32_t>(tiles);
+  L.counter = c.take<uint32_t>(1);
+  L.clear_bytes = align_up(c.used, 256);
+  c.used = L.clear_bytes;
+  L.agg = c.take<SegPair>(tiles);
+  L.inc = c.take<SegPair>(tiles);
+  L.cagg = c.take<SegPair>(tiles);
+  L.cinc = c.take<SegPair>(tiles);
+  L.total = align_up(c.used, 256);
+  return L;
+}
+
+template <int K, int VK>
+rfx_status launch(ReduceArgs& a, cudaStream_t s) {
+  auto k = reduce_by_key_kernel<K, VK>;
+  const uint64_t tiles = (a.n_max + kRedTile - 1) / kRedTile;
+  const int grid = persistent_grid((const void*)k, kRedThreads, 0, tiles ? tiles : 1);
+  k<<<grid, kRedThreads, 0, s>>>(a);
+  RFX_CUDA_TRY(cudaGetLastError());
+  return RFX_OK;
+}
+
+template <int K>
+rfx_status launch_k(ReduceArgs& a, int vk, cudaStream_t s) {
+  switch (vk) {
+    case VAL_NONE: return launch<K, VAL_NONE>(a, s);
+    case VAL_U32: return launch<K, VAL_U32>(a, s);
+    case VAL_I64: return launch<K, VAL_I64>(a, s);
+    default: return RFX_ERR_UNSUPPORTED;
+  }
+}
+
+rfx_status run_reduce(ReduceArgs& a, uint32_t kb, int vk, void* ws, size_t ws_bytes, cudaStream_t s) {
+  RedLayout L = red_layout(ws, a.n_max);
+  if (!ws || ws_bytes < L.total) return RFX_ERR_WORKSPACE;
+  a.flags = L.flags;
+  a.tile_counter = L.counter;
+  a.agg = L.agg;
+  a.inc = L.inc;
+  a.cagg = L.cagg;
+  a.cinc = L.cinc;
+  a.err = device_error_word();
+  if (!a.err) return RFX_ERR_CUDA;
+  RFX_CUDA_TRY(cudaMemsetAsync(ws, 0, L.clear_bytes, s));
+  switch (kb) {
+    case 1: return launch_k<1>(a, vk, s);
+    case 2: return launch_k<2>(a, vk, s);
+    case 4: return launch_k<4>(a, vk, s);
+    case 8: return launch_k<8>(a, vk, s);
+    case 16: return launch_k<16>(a, vk, s);
+    case 32: return launch_k<32>(a, vk, s);
+    default: return RFX_ERR_UNSUPPORTED;
+  }
+}
+
+bool aligned_to(const void* p, uint32_t b) {
+  return (reinterpret_cast<uintptr_t>(p) % (b < 16 ? b : 16)) == 0;
+}
+
+}  // namespace
+
+size_t reduce_workspace_impl(uint64_t n) { return red_layout(nullptr, n).total; }
+
+rfx_status reduce_impl(const void* keys, uint64_t n, const uint64_t* d_n, uint32_t kb, const void* vals, uint32_t vk,
+                       void* out_keys, void* out_vals, uint32_t* out_counts, uint64_t* d_groups, void* ws,
+                       size_t ws_bytes, cudaStream_t s) {
+  if (!d_groups || (!keys && n) || (!out_keys && n)) return RFX_ERR_INVALID;
+  if (vk > VAL_I64 || (vk != VAL_NONE && !vals && n)) return RFX_ERR_INVALID;
+  if (n && (!aligned_to(keys, kb) || !aligned_to(out_keys, kb))) return RFX_ERR_INVALID;
+  ReduceArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.keys = static_cast<const uint8_t*>(keys);
+  a.vals = vals;
+  a.n_max = n;
+  a.d_n = d_n;
+  a.n_div = 1;
+  a.out_keys = static_cast<uint8_t*>(out_keys);
+  a.out_vals = out_vals;
+  a.out_counts = out_counts;
+  a.d_groups = d_groups;
+  return run_reduce(a, kb, (int)vk, ws, ws_bytes, s);
+}
+
+}  // namespace rfx
+
+using namespace rfx;
+
+extern "C" size_t rfx_reduce_by_key_workspace(uint64_t n) { return reduce_workspace_impl(n); }
+
+extern "C" rfx_status rfx_reduce_by_key(const void* keys, uint64_t n, const uint64_t* d_n, uint32_t key_bytes,
+                                        const void* values, uint32_t value_kind, void* out_keys, void* out_values,
+                                        uint32_t* out_counts, uint64_t* d_groups, void* workspace,
+                                        size_t workspace_bytes, void* stream) {
+  return reduce_impl(keys, n, d_n, key_bytes, values, value_kind, out_keys, out_values, out_counts, d_groups,
+                     workspace, workspace_bytes, as_stream(stream));
+}
+
+namespace {
+// Reference byte-size convention (Reduce.cu): *key_size / *value_size hold bytes on the
+// device on entry and are overwritten with the output byte sizes.  The reference reads
+// them back to the host first (a synchronous copy); so does this entry, to size the
+// launch, then it runs on the default stream and synchronises.
+rfx_status count_like(const void* k, const void* v, void* ok, void* ov, uint64_t* key_size, uint64_t* value_size,
+                      uint32_t kb, int vk) {
+  if (!key_size || !value_size) return RFX_ERR_INVALID;
+  uint64_t kbytes = 0;
+  RFX_CUDA_TRY(cudaMemcpy(&kbytes, key_size, sizeof(kbytes), cudaMemcpyDeviceToHost));
+  const uint64_t n = kbytes / kb;
+  const size_t need = reduce_workspace_impl(n);
+  void* ws = nullptr;
+  cudaStream_t s = 0;
+  RFX_CUDA_TRY(cudaMallocAsync(&ws, need, s));
+  uint64_t* groups = nullptr;
+  RFX_CUDA_TRY(cudaMallocAsync(&groups, sizeof(uint64_t), s));
+  ReduceArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.keys = static_cast<const uint8_t*>(k);
+  a.vals = v;
+  a.n_max = n;  // read above; *key_size is overwritten with the output size
+  a.d_n = nullptr;
+  a.n_div = 1;
+  a.out_keys = static_cast<uint8_t*>(ok);
+  a.out_vals = ov;
+  a.d_groups = groups;
+  a.d_groups_bytes_k = key_size;
+  a.d_groups_bytes_v = value_size;
+  rfx_status st = run_reduce(a, kb, vk, ws, need, s);
+  cudaFreeAsync(ws, s);
+  cudaFreeAsync(groups, s);
+  if (st != RFX_OK) return st;
+  RFX_CUDA_TRY(cudaStreamSynchronize(s));
+  return RFX_OK;
+}
+}  // namespace
+
+// count_{8,16,32,128,256} (Reduce.cu:175-660): u32 column summed per run of keys.
+extern "C" rfx_status rfx_count_compat(const void* key_begin, const void* value_begin, void* result_key_begin,
+                                       void* result_value_begin, uint64_t* key_size, uint64_t* value_size,
+                                       uint32_t key_bytes) {
+  return count_like(key_begin, value_begin, result_key_begin, result_value_begin, key_size, value_size, key_bytes,
+                    VAL_U32);
+}
+
+// total_64_32 (Reduce.cu:1138-1215): u64 keys, u32 values summed.
+extern "C" rfx_status rfx_total_64_32_compat(const void* key_begin, const void* value_begin, void* result_key_begin,
+                                             void* result_value_begin, uint64_t* key_size, uint64_t* value_size) {
+  return count_like(key_begin, value_begin, result_key_begin, result_value_begin, key_size, value_size, 8, VAL_U32);
+}
+
+// The exact int64 SUM the reference lacks, with the same byte-size convention.
+extern "C" rfx_status rfx_total_i64_compat(const void* key_begin, const void* value_begin, void* result_key_begin,
+                                           void* result_value_begin, uint64_t* key_size, uint64_t* value_size,
+                                           uint32_t key_bytes) {
+  return count_like(key_begin, value_begin, result_key_begin, result_value_begin, key_size, value_size, key_bytes,
+                    VAL_I64);
+}

@@ -219,6 +219,94 @@ rfx_status rfx_total_i64_compat(const void* key_begin, const void* value_begin,
                                 void* result_key_begin, void* result_value_begin,
                                 uint64_t* key_size, uint64_t* value_size, uint32_t key_bytes);
 
+/* ---------------------------------------------------------------- join */
+size_t rfx_join_find_bounds_workspace(uint64_t nl);
+
+/* redfox::find_bounds_{8,16,32,64,128} (ModernGPUJoin.cu:109-663) in one pass: for each
+ * sorted left key, lower_bound[i] = first right index with an equal-or-greater key
+ * (SortedSearch), and left_count[i] = the exclusive scan of the equal-key counts
+ * (SortedEqualityCount + Scan); *d_total = the number of matches.  Keys are containers
+ * of key_bytes (1/2/4/8/16) compared whole, high limb first (ModernGPUJoin.cu:27-39).
+ * Both inputs sorted ascending; nl, nr < 2^31 (int32 outputs, as the reference's). */
+rfx_status rfx_join_find_bounds(int32_t* lower_bound, int32_t* left_count, uint64_t* d_total,
+                                const void* left_keys, uint64_t nl, const void* right_keys,
+                                uint64_t nr, uint32_t key_bytes, void* workspace,
+                                size_t workspace_bytes, void* stream);
+
+/* redfox::join (ModernGPUJoin.cu:665-733, KernelLeftJoin<Tuning, false>): the (left,
+ * right) index pairs of the inner join, left ascending then right ascending.  nout
+ * sizes the launch; if d_nout is not NULL the pair count is min(nout, *d_nout). */
+rfx_status rfx_join_expand(int32_t* left_idx, int32_t* right_idx, uint64_t nout,
+                           const uint64_t* d_nout, const int32_t* lower_bound,
+                           const int32_t* left_count_scan, uint64_t nl, void* stream);
+
+/* mgpu_join_gather<id> = redfox::gather_{key_key,key_value,value_key,value_value}
+ * (ModernGPUJoin.h:43-200): out[k] = lkey[li] << (lval_bits + rval_bits)
+ * | lval[li] << rval_bits | rval[ri]; lval / rval may be NULL (their bits are then 0).
+ * Containers of 1..64 bytes. */
+rfx_status rfx_join_gather(void* out, uint32_t out_bytes, uint64_t nout, const uint64_t* d_nout,
+                           const int32_t* left_idx, const int32_t* right_idx, const void* lkey,
+                           uint32_t lkey_bytes, const void* lval, uint32_t lval_bytes,
+                           uint32_t lval_bits, const void* rval, uint32_t rval_bytes,
+                           uint32_t rval_bits, void* stream);
+
+/* Fused sort-merge join of packed tuples sorted on their key fields: the key of a tuple is
+ * the tuple shifted right by its value bits (Tuple.h keeps keys in the high fields).
+ * Writes out[k] = (L[i] << right_value_bits) | (R[j] & mask(right_value_bits))
+ * (combine<>, Tuple.h:942-955 -- the bytes gather_value_value produces after split +
+ * find_bounds + join), for the first min(total, capacity) matches in the reference's
+ * order, and *d_count = total.  Containers of 4/8/16 bytes. */
+size_t rfx_join_tuples_workspace(uint64_t nl);
+rfx_status rfx_join_tuples(void* out, uint32_t out_bytes, uint64_t capacity, uint64_t* d_count,
+                           const void* left, uint64_t nl, uint32_t left_bytes,
+                           uint32_t left_value_bits, const void* right, uint64_t nr,
+                           uint32_t right_bytes, uint32_t right_value_bits, void* workspace,
+                           size_t workspace_bytes, void* stream);
+
+/* redfox::find_bounds_* and redfox::join with the reference's argument meaning (element
+ * counts; *result_size on the device).  Own their scratch, synchronous (default
+ * stream), as the reference. */
+rfx_status rfx_find_bounds_compat(int32_t* lower_bound, int32_t* left_count,
+                                  uint64_t* result_size, const void* left_key,
+                                  uint64_t left_size, const void* right_key,
+                                  uint64_t right_size, uint32_t key_bytes);
+rfx_status rfx_join_compat(int32_t* left_indices, int32_t* right_indices, uint64_t result_size,
+                           const int32_t* lower_bound, const int32_t* left_count,
+                           uint64_t input_size);
+
+/* ---------------------------------------------------------------- set operations */
+enum { RFX_SET_UNION = 0, RFX_SET_DIFFERENCE = 1, RFX_SET_INTERSECTION = 2 };
+
+size_t rfx_set_op_workspace(uint32_t op, uint64_t na, uint64_t nb, uint32_t elem_bytes);
+
+/* Multiset set operations on sorted arrays of elem_bytes (1/2/4/8/16) containers, with
+ * thrust / STL semantics: union keeps max(m, n) copies of a value (redfox::set_union,
+ * Union.cu:47-148), difference max(m - n, 0) (redfox::difference, Difference.cu:35-143),
+ * intersection min(m, n) (no reference entry: RelationalAlgebraKernel.cpp:919-922).
+ * Output sorted; *d_count = its element count. */
+rfx_status rfx_set_op(uint32_t op, void* out, uint64_t* d_count, const void* a, uint64_t na,
+                      const void* b, uint64_t nb, uint32_t elem_bytes, void* workspace,
+                      size_t workspace_bytes, void* stream);
+
+/* redfox::unique (Unique.cu:36-114): keeps the first of each run of equal elements, in
+ * place; *d_count = elements kept. */
+size_t rfx_unique_workspace(uint64_t n, uint32_t elem_bytes);
+rfx_status rfx_unique(void* data, uint64_t n, uint64_t* d_count, uint32_t elem_bytes,
+                      void* workspace, size_t workspace_bytes, void* stream);
+
+/* The reference's set entries with its argument meaning: [lbegin, lend) and [rbegin,
+ * rend) device ranges, DataType `type` (I8..I128; I8..I64 for unique), *size = output
+ * bytes on the device (for unique: input bytes in, output bytes out).  Synchronous.
+ * An unknown type returns RFX_ERR_UNSUPPORTED and leaves the outputs untouched, where the
+ * reference falls through to its I8 case (Union.cu:59, Difference.cu:47). */
+rfx_status rfx_set_union_compat(void* result, uint64_t* size, void* lbegin, void* lend,
+                                void* rbegin, void* rend, uint32_t type);
+rfx_status rfx_difference_compat(void* result, uint64_t* size, void* lbegin, void* lend,
+                                 void* rbegin, void* rend, uint32_t type);
+rfx_status rfx_intersection_compat(void* result, uint64_t* size, void* lbegin, void* lend,
+                                   void* rbegin, void* rend, uint32_t type);
+rfx_status rfx_unique_compat(void* begin, uint64_t* size, uint64_t type);
+
 /* ---------------------------------------------------------------- synthetic data */
 /* Column j of row i = lo[j] + mulhi64(rand(seed, stream_j, i), hi[j] - lo[j]) with the
  * SplitMix64 stream below, packed as `type`.  The generator behind the benchmarks. */

@@ -1,0 +1,251 @@
+// join_abi.cu -- C ABI of the sort-merge join: find_bounds, index expansion, gather, the
+// fused tuple join, and the reference-compatible find_bounds_* / join entries.
+#include <cstring>
+
+#include "host_common.h"
+#include "join_kernels.cuh"
+
+namespace rfx {
+namespace {
+
+bool key_width(uint32_t e) { return e == 1 || e == 2 || e == 4 || e == 8 || e == 16; }
+
+struct FbLayout {
+  uint64_t* status;
+  uint32_t* counter;
+  size_t clear;
+  uint64_t* lb64;
+  uint64_t* off64;
+  size_t total;
+};
+
+FbLayout fb_layout(void* ws, uint64_t nl, bool with_offsets) {
+  FbLayout L;
+  Carver c(ws);
+  L.status = c.take<uint64_t>((nl + kFbTile - 1) / kFbTile + 1);
+  L.counter = c.take<uint32_t>(1);
+  L.clear = align_up(c.used, 256);
+  c.used = L.clear;
+  L.lb64 = with_offsets ? c.take<uint64_t>(nl + 1) : nullptr;
+  L.off64 = with_offsets ? c.take<uint64_t>(nl + 1) : nullptr;
+  L.total = align_up(c.used, 256);
+  return L;
+}
+
+template <int LE, int RE>
+rfx_status launch_fb(FindBoundsArgs& a, cudaStream_t s) {
+  auto k = find_bounds_kernel<LE, RE>;
+  const uint64_t tiles = (a.nl + kFbTile - 1) / kFbTile;
+  const int grid = persistent_grid((const void*)k, kJoinThreads, 0, tiles ? tiles : 1);
+  k<<<grid, kJoinThreads, 0, s>>>(a);
+  RFX_CUDA_TRY(cudaGetLastError());
+  return RFX_OK;
+}
+
+rfx_status dispatch_fb(uint32_t le, uint32_t re, FindBoundsArgs& a, cudaStream_t s) {
+#define RFX_FB(L, R) \
+  if (le == L && re == R) return launch_fb<L, R>(a, s);
+  RFX_FB(1, 1) RFX_FB(2, 2) RFX_FB(4, 4) RFX_FB(8, 8) RFX_FB(16, 16)
+  RFX_FB(4, 8) RFX_FB(4, 16) RFX_FB(8, 4) RFX_FB(8, 16) RFX_FB(16, 4) RFX_FB(16, 8)
+#undef RFX_FB
+  return RFX_ERR_UNSUPPORTED;
+}
+
+template <int LE, int RE, int OE>
+rfx_status launch_tj(TupleJoinArgs& a, cudaStream_t s) {
+  auto k = tuple_join_kernel<LE, RE, OE>;
+  const uint64_t tiles = (a.cap + kExpTile - 1) / kExpTile;
+  const int grid = persistent_grid((const void*)k, kJoinThreads, 0, tiles ? tiles : 1);
+  k<<<grid, kJoinThreads, 0, s>>>(a);
+  RFX_CUDA_TRY(cudaGetLastError());
+  return RFX_OK;
+}
+
+template <int LE, int RE>
+rfx_status dispatch_tj_o(uint32_t oe, TupleJoinArgs& a, cudaStream_t s) {
+  switch (oe) {
+    case 4: return launch_tj<LE, RE, 4>(a, s);
+    case 8: return launch_tj<LE, RE, 8>(a, s);
+    case 16: return launch_tj<LE, RE, 16>(a, s);
+    default: return RFX_ERR_UNSUPPORTED;
+  }
+}
+
+rfx_status dispatch_tj(uint32_t le, uint32_t re, uint32_t oe, TupleJoinArgs& a, cudaStream_t s) {
+#define RFX_TJ(L, R) \
+  if (le == L && re == R) return dispatch_tj_o<L, R>(oe, a, s);
+  RFX_TJ(4, 4) RFX_TJ(4, 8) RFX_TJ(4, 16) RFX_TJ(8, 4) RFX_TJ(8, 8) RFX_TJ(8, 16) RFX_TJ(16, 4) RFX_TJ(16, 8)
+  RFX_TJ(16, 16)
+#undef RFX_TJ
+  return RFX_ERR_UNSUPPORTED;
+}
+
+bool aligned_to(const void* p, uint32_t b) { return (reinterpret_cast<uintptr_t>(p) % (b < 16 ? b : 16)) == 0; }
+
+}  // namespace
+
+size_t find_bounds_workspace_impl(uint64_t nl) { return fb_layout(nullptr, nl, false).total; }
+
+rfx_status find_bounds_impl(int32_t* lb, int32_t* scan, uint64_t* d_total, const void* left, uint64_t nl,
+                            const void* right, uint64_t nr, uint32_t kb, void* ws, size_t wsb, cudaStream_t s) {
+  if (!key_width(kb)) return RFX_ERR_UNSUPPORTED;
+  if (!d_total || (nl && (!left || !lb || !scan)) || (nr && !right)) return RFX_ERR_INVALID;
+  if (nl >= (1ull << 31) || nr >= (1ull << 31)) return RFX_ERR_UNSUPPORTED;  // int32 outputs
+  if ((nl && !aligned_to(left, kb)) || (nr && !aligned_to(right, kb))) return RFX_ERR_INVALID;
+  FbLayout L = fb_layout(ws, nl, false);
+  if (!ws || wsb < L.total) return RFX_ERR_WORKSPACE;
+  uint32_t* err = device_error_word();
+  if (!err) return RFX_ERR_CUDA;
+  RFX_CUDA_TRY(cudaMemsetAsync(ws, 0, L.clear, s));
+  FindBoundsArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.left = static_cast<const uint8_t*>(left);
+  a.nl = nl;
+  a.right = static_cast<const uint8_t*>(right);
+  a.nr = nr;
+  a.lb32 = lb;
+  a.scan32 = scan;
+  a.d_total = d_total;
+  a.status = L.status;
+  a.tile_counter = L.counter;
+  a.err = err;
+  return dispatch_fb(kb, kb, a, s);
+}
+
+rfx_status join_expand_impl(int32_t* li, int32_t* ri, uint64_t nout, const uint64_t* d_nout, const int32_t* lb,
+                            const int32_t* scan, uint64_t nl, cudaStream_t s) {
+  if (nout == 0) return RFX_OK;
+  if (!li || !ri || !lb || !scan || nl == 0) return RFX_ERR_INVALID;
+  const uint64_t tiles = (nout + kExpTile - 1) / kExpTile;
+  const int grid = persistent_grid((const void*)join_expand_kernel, kJoinThreads, 0, tiles);
+  join_expand_kernel<<<grid, kJoinThreads, 0, s>>>(li, ri, nout, d_nout, lb, scan, nl);
+  RFX_CUDA_TRY(cudaGetLastError());
+  return RFX_OK;
+}
+
+}  // namespace rfx
+
+using namespace rfx;
+
+extern "C" size_t rfx_join_find_bounds_workspace(uint64_t nl) { return find_bounds_workspace_impl(nl); }
+
+extern "C" rfx_status rfx_join_find_bounds(int32_t* lower_bound, int32_t* left_count, uint64_t* d_total,
+                                           const void* left_keys, uint64_t nl, const void* right_keys, uint64_t nr,
+                                           uint32_t key_bytes, void* workspace, size_t workspace_bytes, void* stream) {
+  return find_bounds_impl(lower_bound, left_count, d_total, left_keys, nl, right_keys, nr, key_bytes, workspace,
+                          workspace_bytes, as_stream(stream));
+}
+
+extern "C" rfx_status rfx_join_expand(int32_t* left_idx, int32_t* right_idx, uint64_t nout, const uint64_t* d_nout,
+                                      const int32_t* lower_bound, const int32_t* left_count_scan, uint64_t nl,
+                                      void* stream) {
+  return join_expand_impl(left_idx, right_idx, nout, d_nout, lower_bound, left_count_scan, nl, as_stream(stream));
+}
+
+extern "C" rfx_status rfx_join_gather(void* out, uint32_t out_bytes, uint64_t nout, const uint64_t* d_nout,
+                                      const int32_t* left_idx, const int32_t* right_idx, const void* lkey,
+                                      uint32_t lkey_bytes, const void* lval, uint32_t lval_bytes, uint32_t lval_bits,
+                                      const void* rval, uint32_t rval_bytes, uint32_t rval_bits, void* stream) {
+  auto ok_w = [](uint32_t b) { return b == 1 || b == 2 || b == 4 || b == 8 || b == 16 || b == 32 || b == 64; };
+  if (!ok_w(out_bytes) || !ok_w(lkey_bytes) || (lval && !ok_w(lval_bytes)) || (rval && !ok_w(rval_bytes)))
+    return RFX_ERR_UNSUPPORTED;
+  if (nout == 0) return RFX_OK;
+  if (!out || !left_idx || !lkey || (rval && !right_idx)) return RFX_ERR_INVALID;
+  GatherArgs a;
+  a.out = static_cast<uint8_t*>(out);
+  a.ob = out_bytes;
+  a.nout_max = nout;
+  a.d_nout = d_nout;
+  a.li = left_idx;
+  a.ri = right_idx;
+  a.lkey = static_cast<const uint8_t*>(lkey);
+  a.lkb = lkey_bytes;
+  a.lval = static_cast<const uint8_t*>(lval);
+  a.lvb = lval_bytes;
+  a.lv_bits = lval ? lval_bits : 0;
+  a.rval = static_cast<const uint8_t*>(rval);
+  a.rvb = rval_bytes;
+  a.rv_bits = rval ? rval_bits : 0;
+  const uint64_t blocks = (nout + kJoinThreads - 1) / kJoinThreads;
+  const int grid = persistent_grid((const void*)join_gather_kernel, kJoinThreads, 0, blocks);
+  join_gather_kernel<<<grid, kJoinThreads, 0, as_stream(stream)>>>(a);
+  RFX_CUDA_TRY(cudaGetLastError());
+  return RFX_OK;
+}
+
+extern "C" size_t rfx_join_tuples_workspace(uint64_t nl) { return fb_layout(nullptr, nl, true).total; }
+
+extern "C" rfx_status rfx_join_tuples(void* out, uint32_t out_bytes, uint64_t capacity, uint64_t* d_count,
+                                      const void* left, uint64_t nl, uint32_t left_bytes, uint32_t left_value_bits,
+                                      const void* right, uint64_t nr, uint32_t right_bytes, uint32_t right_value_bits,
+                                      void* workspace, size_t workspace_bytes, void* stream) {
+  const bool w_ok = (left_bytes == 4 || left_bytes == 8 || left_bytes == 16) &&
+                    (right_bytes == 4 || right_bytes == 8 || right_bytes == 16) &&
+                    (out_bytes == 4 || out_bytes == 8 || out_bytes == 16);
+  if (!w_ok || left_value_bits >= left_bytes * 8u || right_value_bits >= right_bytes * 8u) return RFX_ERR_UNSUPPORTED;
+  if (!d_count || (nl && !left) || (nr && !right) || (capacity && !out)) return RFX_ERR_INVALID;
+  if ((nl && !aligned_to(left, left_bytes)) || (nr && !aligned_to(right, right_bytes)) ||
+      (capacity && !aligned_to(out, out_bytes)))
+    return RFX_ERR_INVALID;
+  cudaStream_t s = as_stream(stream);
+  FbLayout L = fb_layout(workspace, nl, true);
+  if (!workspace || workspace_bytes < L.total) return RFX_ERR_WORKSPACE;
+  uint32_t* err = device_error_word();
+  if (!err) return RFX_ERR_CUDA;
+  RFX_CUDA_TRY(cudaMemsetAsync(workspace, 0, L.clear, s));
+  FindBoundsArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.left = static_cast<const uint8_t*>(left);
+  a.nl = nl;
+  a.right = static_cast<const uint8_t*>(right);
+  a.nr = nr;
+  a.lshift = left_value_bits;
+  a.rshift = right_value_bits;
+  a.lb64 = L.lb64;
+  a.off64 = L.off64;
+  a.d_total = d_count;
+  a.status = L.status;
+  a.tile_counter = L.counter;
+  a.err = err;
+  rfx_status st = dispatch_fb(left_bytes, right_bytes, a, s);
+  if (st != RFX_OK || capacity == 0 || nl == 0) return st;
+  TupleJoinArgs j;
+  j.left = static_cast<const uint8_t*>(left);
+  j.nl = nl;
+  j.right = static_cast<const uint8_t*>(right);
+  j.rv_bits = right_value_bits;
+  j.lb64 = L.lb64;
+  j.off64 = L.off64;
+  j.out = static_cast<uint8_t*>(out);
+  j.cap = capacity;
+  return dispatch_tj(left_bytes, right_bytes, out_bytes, j, s);
+}
+
+// ---- reference-compatible entries (synchronous, own their scratch) ----
+
+// redfox::find_bounds_{8,16,32,64,128} (ModernGPUJoin.cu:109-663): sizes in elements,
+// *result_size (device) = number of matches.
+extern "C" rfx_status rfx_find_bounds_compat(int32_t* lower_bound, int32_t* left_count, uint64_t* result_size,
+                                             const void* left_key, uint64_t left_size, const void* right_key,
+                                             uint64_t right_size, uint32_t key_bytes) {
+  cudaStream_t s = 0;
+  const size_t need = find_bounds_workspace_impl(left_size);
+  void* ws = nullptr;
+  RFX_CUDA_TRY(cudaMallocAsync(&ws, need, s));
+  rfx_status st = find_bounds_impl(lower_bound, left_count, result_size, left_key, left_size, right_key, right_size,
+                                   key_bytes, ws, need, s);
+  cudaFreeAsync(ws, s);
+  if (st != RFX_OK) return st;
+  RFX_CUDA_TRY(cudaStreamSynchronize(s));
+  return RFX_OK;
+}
+
+// redfox::join (ModernGPUJoin.cu:665-733): result_size and input_size in elements.
+extern "C" rfx_status rfx_join_compat(int32_t* left_indices, int32_t* right_indices, uint64_t result_size,
+                                      const int32_t* lower_bound, const int32_t* left_count, uint64_t input_size) {
+  rfx_status st = join_expand_impl(left_indices, right_indices, result_size, nullptr, lower_bound, left_count,
+                                   input_size, 0);
+  if (st != RFX_OK) return st;
+  RFX_CUDA_TRY(cudaStreamSynchronize(0));
+  return RFX_OK;
+}

@@ -1,0 +1,294 @@
+// join_kernels.cuh -- sort-merge join: find_bounds (lower bound + equality count + scan
+// in one pass), load-balanced expansion into (left, right) index pairs, the gather that
+// assembles output tuples, and the fused tuple join that expands and assembles without
+// materialising indices.
+//
+// Output order is the reference's: left row ascending, then right row ascending
+// (KernelLeftJoin<Tuning, false>, ModernGPUJoin.cu:665-733; CPUJoin,
+// moderngpu/tests/benchmarkjoin.cu:40-128).  Expansion is balanced over output rows, so a
+// skewed key (one left row with millions of matches) spreads over all blocks.
+#pragma once
+
+#include "search.cuh"
+#include "sort_kernels.cuh"
+
+namespace rfx {
+
+constexpr int kJoinThreads = 256;
+constexpr int kFbIPT = 4;                        // left rows per thread in find_bounds
+constexpr int kFbTile = kJoinThreads * kFbIPT;
+constexpr int kExpVT = 8;                        // outputs per thread in the expansion
+constexpr int kExpTile = kJoinThreads * kExpVT;
+
+struct FindBoundsArgs {
+  const uint8_t* left;
+  uint64_t nl;
+  const uint8_t* right;
+  uint64_t nr;
+  uint32_t lshift, rshift;   // key = container >> shift
+  int32_t* lb32;             // reference outputs (may be null)
+  int32_t* scan32;
+  uint64_t* lb64;            // workspace outputs for the fused join (may be null)
+  uint64_t* off64;           // exclusive offsets, off64[nl] = total
+  uint64_t* d_total;
+  uint64_t* status;
+  uint32_t* tile_counter;
+  uint32_t* err;
+};
+
+// Block-wide exclusive sum of one 64-bit value per thread.
+__device__ __forceinline__ uint64_t block_exclusive_u64(uint64_t x, uint64_t* s_warp, uint64_t* total) {
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint64_t incl = x;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint64_t y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= (uint32_t)o) incl += y;
+  }
+  if (lane == 31) s_warp[warp] = incl;
+  __syncthreads();
+  uint64_t wpre = 0, tot = 0;
+  for (uint32_t w = 0; w < blockDim.x / 32; ++w) {
+    if (w < warp) wpre += s_warp[w];
+    tot += s_warp[w];
+  }
+  *total = tot;
+  return wpre + incl - x;
+}
+
+template <int LE, int RE>
+__global__ void __launch_bounds__(kJoinThreads) find_bounds_kernel(const FindBoundsArgs a) {
+  __shared__ uint64_t s_warp[kJoinThreads / 32];
+  __shared__ uint64_t s_prefix;
+  __shared__ uint32_t s_tile;
+  const uint32_t t = threadIdx.x;
+  const uint64_t num_tiles = (a.nl + kFbTile - 1) / kFbTile;
+  const KeyView<LE> L{a.left, a.nl, a.lshift};
+  const KeyView<RE> R{a.right, a.nr, a.rshift};
+  while (true) {
+    if (t == 0) s_tile = atomicAdd(a.tile_counter, 1u);
+    __syncthreads();
+    const uint64_t tile = s_tile;
+    if (tile >= num_tiles) break;
+    const uint64_t first = tile * kFbTile + (uint64_t)t * kFbIPT;
+    uint64_t lo[kFbIPT], cnt[kFbIPT];
+    uint64_t tsum = 0;
+    u128 prevk = 0;
+    uint64_t plo = 0, phi = 0;
+#pragma unroll
+    for (int j = 0; j < kFbIPT; ++j) {
+      const uint64_t i = first + j;
+      lo[j] = 0;
+      cnt[j] = 0;
+      if (i >= a.nl) continue;
+      const u128 k = L.key(i);
+      if (j > 0 && k == prevk) {
+        lo[j] = plo;
+        cnt[j] = phi - plo;
+      } else {
+        const uint64_t l = j == 0 ? bsearch<RE>(R, k, 0, a.nr, false) : gallop<RE>(R, k, phi, false);
+        const uint64_t h = gallop<RE>(R, k, l, true);
+        lo[j] = l;
+        cnt[j] = h - l;
+        plo = l;
+        phi = h;
+        prevk = k;
+      }
+      tsum += cnt[j];
+    }
+    uint64_t btot;
+    const uint64_t ex = block_exclusive_u64(tsum, s_warp, &btot);
+    if ((t >> 5) == 0) {
+      const uint64_t pre = lookback_exclusive(a.status, (uint32_t)tile, btot, a.err);
+      if (t == 0) {
+        s_prefix = pre;
+        if (tile == num_tiles - 1) {
+          *a.d_total = pre + btot;
+          if (a.off64) a.off64[a.nl] = pre + btot;
+        }
+      }
+    }
+    __syncthreads();
+    uint64_t run = s_prefix + ex;
+#pragma unroll
+    for (int j = 0; j < kFbIPT; ++j) {
+      const uint64_t i = first + j;
+      if (i >= a.nl) continue;
+      if (a.lb32) a.lb32[i] = (int32_t)lo[j];
+      if (a.scan32) a.scan32[i] = (int32_t)(uint32_t)run;
+      if (a.lb64) a.lb64[i] = lo[j];
+      if (a.off64) a.off64[i] = run;
+      run += cnt[j];
+    }
+    __syncthreads();
+  }
+  if (a.nl == 0 && blockIdx.x == 0 && t == 0) {
+    *a.d_total = 0;
+    if (a.off64) a.off64[0] = 0;
+  }
+}
+
+// ------------------------------------------------------------------ index expansion
+// Output k belongs to the last left row i with scan[i] <= k; right row lb[i] + k - scan[i].
+__global__ void __launch_bounds__(kJoinThreads)
+join_expand_kernel(int32_t* __restrict__ li, int32_t* __restrict__ ri, uint64_t nout_max, const uint64_t* d_nout,
+                   const int32_t* __restrict__ lb, const int32_t* __restrict__ scan, uint64_t nl) {
+  uint64_t nout = nout_max;
+  if (d_nout) nout = min(nout, *d_nout);
+  const uint64_t stride = (uint64_t)gridDim.x * kExpTile;
+  for (uint64_t base = (uint64_t)blockIdx.x * kExpTile + (uint64_t)threadIdx.x * kExpVT; base < nout; base += stride) {
+    // last i with (u32)scan[i] <= base
+    uint64_t lo = 0, hi = nl;
+    while (lo < hi) {
+      const uint64_t mid = lo + ((hi - lo) >> 1);
+      if ((uint64_t)(uint32_t)__ldg(scan + mid) <= base) lo = mid + 1;
+      else hi = mid;
+    }
+    uint64_t i = lo - 1;
+    uint64_t nxt = i + 1 < nl ? (uint64_t)(uint32_t)__ldg(scan + i + 1) : ~0ull;
+#pragma unroll
+    for (int v = 0; v < kExpVT; ++v) {
+      const uint64_t k = base + v;
+      if (k >= nout) break;
+      while (k >= nxt) {
+        ++i;
+        nxt = i + 1 < nl ? (uint64_t)(uint32_t)__ldg(scan + i + 1) : ~0ull;
+      }
+      li[k] = (int32_t)i;
+      ri[k] = __ldg(lb + i) + (int32_t)(k - (uint64_t)(uint32_t)__ldg(scan + i));
+    }
+  }
+}
+
+// ------------------------------------------------------------------ gather
+// out = lkey << (lv_bits + rv_bits) | lval << rv_bits | rval over containers of up to
+// 64 bytes (gather_{key_key,key_value,value_key,value_value}, ModernGPUJoin.h:43-200).
+struct GatherArgs {
+  uint8_t* out;
+  uint32_t ob;
+  uint64_t nout_max;
+  const uint64_t* d_nout;
+  const int32_t* li;
+  const int32_t* ri;
+  const uint8_t* lkey;
+  uint32_t lkb;
+  const uint8_t* lval;
+  uint32_t lvb;
+  uint32_t lv_bits;
+  const uint8_t* rval;
+  uint32_t rvb;
+  uint32_t rv_bits;
+};
+
+__device__ __forceinline__ void limb_load(uint64_t (&L)[8], const uint8_t* p, uint32_t bytes) {
+#pragma unroll
+  for (int k = 0; k < 8; ++k) L[k] = 0;
+  if (bytes >= 8) {
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+      if ((uint32_t)k * 8 < bytes) L[k] = reinterpret_cast<const unsigned long long*>(p)[k];
+  } else if (bytes == 4) {
+    L[0] = *reinterpret_cast<const uint32_t*>(p);
+  } else if (bytes == 2) {
+    L[0] = *reinterpret_cast<const uint16_t*>(p);
+  } else {
+    L[0] = *p;
+  }
+}
+
+__device__ __forceinline__ void limb_shl_or(uint64_t (&acc)[8], const uint64_t (&v)[8], uint32_t s) {
+  const uint32_t q = s >> 6, r = s & 63;
+#pragma unroll
+  for (int k = 7; k >= 0; --k) {
+    const int src = k - (int)q;
+    if (src < 0) continue;
+    uint64_t x = v[src] << r;
+    if (r && src > 0) x |= v[src - 1] >> (64 - r);
+    acc[k] |= x;
+  }
+}
+
+__global__ void __launch_bounds__(kJoinThreads) join_gather_kernel(const GatherArgs a) {
+  uint64_t nout = a.nout_max;
+  if (a.d_nout) nout = min(nout, *a.d_nout);
+  for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < nout; k += (uint64_t)gridDim.x * blockDim.x) {
+    const uint64_t i = (uint32_t)a.li[k];
+    uint64_t acc[8] = {0, 0, 0, 0, 0, 0, 0, 0}, v[8];
+    limb_load(v, a.lkey + i * a.lkb, a.lkb);
+    limb_shl_or(acc, v, a.lv_bits + a.rv_bits);
+    if (a.lval) {
+      limb_load(v, a.lval + i * a.lvb, a.lvb);
+      limb_shl_or(acc, v, a.rv_bits);
+    }
+    if (a.rval) {
+      const uint64_t j = (uint32_t)a.ri[k];
+      limb_load(v, a.rval + j * a.rvb, a.rvb);
+      limb_shl_or(acc, v, 0);
+    }
+    uint8_t* o = a.out + k * a.ob;
+    if (a.ob >= 8) {
+#pragma unroll
+      for (int q = 0; q < 8; ++q)
+        if ((uint32_t)q * 8 < a.ob) reinterpret_cast<unsigned long long*>(o)[q] = acc[q];
+    } else if (a.ob == 4) {
+      *reinterpret_cast<uint32_t*>(o) = (uint32_t)acc[0];
+    } else if (a.ob == 2) {
+      *reinterpret_cast<uint16_t*>(o) = (uint16_t)acc[0];
+    } else {
+      *o = (uint8_t)acc[0];
+    }
+  }
+}
+
+// ------------------------------------------------------------------ fused tuple join
+// out[k] = (L[i] << rv_bits) | (R[j] & mask(rv_bits)) -- combine<> of Tuple.h:942-955, the
+// same bytes as gather_value_value on the split key/value arrays -- for the k < cap
+// output rows, i and j found from the find_bounds offsets.
+struct TupleJoinArgs {
+  const uint8_t* left;
+  uint64_t nl;
+  const uint8_t* right;
+  uint32_t rv_bits;
+  const uint64_t* lb64;
+  const uint64_t* off64;   // nl + 1 entries
+  uint8_t* out;
+  uint64_t cap;
+};
+
+template <int LE, int RE, int OE>
+__global__ void __launch_bounds__(kJoinThreads) tuple_join_kernel(const TupleJoinArgs a) {
+  const uint64_t total = a.off64[a.nl];
+  const uint64_t nout = total < a.cap ? total : a.cap;
+  const u128 rmask = a.rv_bits >= 128 ? ~(u128)0 : (((u128)1 << a.rv_bits) - 1);
+  const uint64_t stride = (uint64_t)gridDim.x * kExpTile;
+  for (uint64_t base = (uint64_t)blockIdx.x * kExpTile + (uint64_t)threadIdx.x * kExpVT; base < nout; base += stride) {
+    uint64_t lo = 0, hi = a.nl;
+    while (lo < hi) {
+      const uint64_t mid = lo + ((hi - lo) >> 1);
+      if (__ldg(a.off64 + mid) <= base) lo = mid + 1;
+      else hi = mid;
+    }
+    uint64_t i = lo - 1;
+    uint64_t nxt = __ldg(a.off64 + i + 1);
+    u128 lrow = load_u128<LE>(a.left, i) << a.rv_bits;
+    uint64_t lbi = __ldg(a.lb64 + i), offi = __ldg(a.off64 + i);
+#pragma unroll
+    for (int v = 0; v < kExpVT; ++v) {
+      const uint64_t k = base + v;
+      if (k >= nout) break;
+      if (k >= nxt) {
+        while (k >= nxt) {
+          ++i;
+          nxt = __ldg(a.off64 + i + 1);
+        }
+        lrow = load_u128<LE>(a.left, i) << a.rv_bits;
+        lbi = __ldg(a.lb64 + i);
+        offi = __ldg(a.off64 + i);
+      }
+      const uint64_t j = lbi + (k - offi);
+      store_u128<OE>(a.out, k, lrow | (load_u128<RE>(a.right, j) & rmask));
+    }
+  }
+}
+
+}  // namespace rfx

@@ -1,0 +1,85 @@
+// search.cuh -- sorted-search primitives over packed keys.
+//
+// A key view reads element i of a sorted array of E-byte containers (E <= 16) as an
+// unsigned 128-bit integer and shifts it right by `shift` bits: shift = 0 compares whole
+// keys (the find_bounds_{8..128} entries compare the whole container, limb a[1] before
+// a[0], ModernGPUJoin.cu:27-39), shift = value bits compares packed tuples on their key
+// fields, which Tuple.h places in the high bits.
+#pragma once
+
+#include "rfx_device.cuh"
+
+namespace rfx {
+
+typedef unsigned __int128 u128;
+
+template <int E>
+__device__ __forceinline__ u128 load_u128(const uint8_t* base, uint64_t i) {
+  if constexpr (E == 1) {
+    return (u128)__ldg(base + i);
+  } else if constexpr (E == 2) {
+    return (u128)__ldg(reinterpret_cast<const uint16_t*>(base) + i);
+  } else if constexpr (E == 4) {
+    return (u128)__ldg(reinterpret_cast<const uint32_t*>(base) + i);
+  } else if constexpr (E == 8) {
+    return (u128)__ldg(reinterpret_cast<const unsigned long long*>(base) + i);
+  } else {
+    const ulonglong2 v = __ldg(reinterpret_cast<const ulonglong2*>(base) + i);
+    return ((u128)v.y << 64) | (u128)v.x;
+  }
+}
+
+template <int E>
+__device__ __forceinline__ void store_u128(uint8_t* base, uint64_t i, u128 v) {
+  if constexpr (E == 1) {
+    base[i] = (uint8_t)v;
+  } else if constexpr (E == 2) {
+    reinterpret_cast<uint16_t*>(base)[i] = (uint16_t)v;
+  } else if constexpr (E == 4) {
+    reinterpret_cast<uint32_t*>(base)[i] = (uint32_t)v;
+  } else if constexpr (E == 8) {
+    reinterpret_cast<unsigned long long*>(base)[i] = (unsigned long long)v;
+  } else {
+    reinterpret_cast<ulonglong2*>(base)[i] = make_ulonglong2((unsigned long long)v, (unsigned long long)(v >> 64));
+  }
+}
+
+template <int E>
+struct KeyView {
+  const uint8_t* base;
+  uint64_t n;
+  uint32_t shift;
+  __device__ __forceinline__ u128 key(uint64_t i) const { return load_u128<E>(base, i) >> shift; }
+};
+
+// First index in [lo, hi) whose key is >= k (strict = false) or > k (strict = true).
+template <int E>
+__device__ __forceinline__ uint64_t bsearch(const KeyView<E>& v, u128 k, uint64_t lo, uint64_t hi, bool strict) {
+  while (lo < hi) {
+    const uint64_t mid = lo + ((hi - lo) >> 1);
+    const u128 m = v.key(mid);
+    const bool before = strict ? (m <= k) : (m < k);
+    if (before) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Same result as bsearch(v, k, from, n, strict) when the answer is >= from, found by
+// galloping forward from `from` (cheap when consecutive searches land close together).
+template <int E>
+__device__ __forceinline__ uint64_t gallop(const KeyView<E>& v, u128 k, uint64_t from, bool strict) {
+  uint64_t lo = from, step = 1, hi = from;
+  while (hi < v.n) {
+    const u128 m = v.key(hi);
+    const bool before = strict ? (m <= k) : (m < k);
+    if (!before) break;
+    lo = hi + 1;
+    hi = from + step;
+    step <<= 1;
+  }
+  if (hi > v.n) hi = v.n;
+  return bsearch<E>(v, k, lo, hi, strict);
+}
+
+}  // namespace rfx

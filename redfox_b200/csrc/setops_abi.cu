@@ -1,0 +1,284 @@
+// setops_abi.cu -- C ABI of union / difference / intersection / unique, and the
+// reference-compatible set_union / difference / unique entries.
+#include <cstring>
+
+#include "host_common.h"
+#include "setops_kernels.cuh"
+
+namespace rfx {
+namespace {
+
+bool elem_width(uint32_t e) { return e == 1 || e == 2 || e == 4 || e == 8 || e == 16; }
+
+struct FilterLayout {
+  uint64_t* status;
+  uint32_t* counter;
+  size_t clear;
+  size_t total;
+};
+
+FilterLayout filter_layout(void* ws, uint64_t n) {
+  FilterLayout L;
+  Carver c(ws);
+  L.status = c.take<uint64_t>((n + kSetTile - 1) / kSetTile + 1);
+  L.counter = c.take<uint32_t>(1);
+  L.clear = align_up(c.used, 256);
+  L.total = L.clear;
+  return L;
+}
+
+template <int E>
+rfx_status launch_filter(int mode, SetFilterArgs& a, cudaStream_t s) {
+  const uint64_t tiles = (a.na + kSetTile - 1) / kSetTile;
+  const void* k = mode == KEEP_MATCHED ? (const void*)set_filter_kernel<E, KEEP_MATCHED>
+                : mode == KEEP_UNMATCHED ? (const void*)set_filter_kernel<E, KEEP_UNMATCHED>
+                                         : (const void*)set_filter_kernel<E, KEEP_HEADS>;
+  const int grid = persistent_grid(k, kSetThreads, 0, tiles ? tiles : 1);
+  if (mode == KEEP_MATCHED) set_filter_kernel<E, KEEP_MATCHED><<<grid, kSetThreads, 0, s>>>(a);
+  else if (mode == KEEP_UNMATCHED) set_filter_kernel<E, KEEP_UNMATCHED><<<grid, kSetThreads, 0, s>>>(a);
+  else set_filter_kernel<E, KEEP_HEADS><<<grid, kSetThreads, 0, s>>>(a);
+  RFX_CUDA_TRY(cudaGetLastError());
+  return RFX_OK;
+}
+
+rfx_status dispatch_filter(uint32_t e, int mode, SetFilterArgs& a, cudaStream_t s) {
+  switch (e) {
+    case 1: return launch_filter<1>(mode, a, s);
+    case 2: return launch_filter<2>(mode, a, s);
+    case 4: return launch_filter<4>(mode, a, s);
+    case 8: return launch_filter<8>(mode, a, s);
+    case 16: return launch_filter<16>(mode, a, s);
+    default: return RFX_ERR_UNSUPPORTED;
+  }
+}
+
+template <int E>
+rfx_status launch_merge(const void* a, uint64_t na, const void* d, uint64_t nd_max, const uint64_t* d_nd, void* out,
+                        uint64_t* d_count, cudaStream_t s) {
+  const uint64_t tiles = (na + nd_max + kMergeTile - 1) / kMergeTile;
+  const int grid = persistent_grid((const void*)merge_kernel<E>, kSetThreads, 0, tiles ? tiles : 1);
+  merge_kernel<E><<<grid, kSetThreads, 0, s>>>(static_cast<const uint8_t*>(a), na, static_cast<const uint8_t*>(d),
+                                               nd_max, d_nd, static_cast<uint8_t*>(out), d_count);
+  RFX_CUDA_TRY(cudaGetLastError());
+  return RFX_OK;
+}
+
+rfx_status dispatch_merge(uint32_t e, const void* a, uint64_t na, const void* d, uint64_t nd_max, const uint64_t* d_nd,
+                          void* out, uint64_t* d_count, cudaStream_t s) {
+  switch (e) {
+    case 1: return launch_merge<1>(a, na, d, nd_max, d_nd, out, d_count, s);
+    case 2: return launch_merge<2>(a, na, d, nd_max, d_nd, out, d_count, s);
+    case 4: return launch_merge<4>(a, na, d, nd_max, d_nd, out, d_count, s);
+    case 8: return launch_merge<8>(a, na, d, nd_max, d_nd, out, d_count, s);
+    case 16: return launch_merge<16>(a, na, d, nd_max, d_nd, out, d_count, s);
+    default: return RFX_ERR_UNSUPPORTED;
+  }
+}
+
+template <int E>
+rfx_status launch_prev(const void* a, uint64_t n, void* prev, cudaStream_t s) {
+  const uint64_t tiles = (n + kSetTile - 1) / kSetTile;
+  const int grid = (int)((tiles + 255) / 256);
+  tile_prev_kernel<E><<<grid ? grid : 1, 256, 0, s>>>(static_cast<const uint8_t*>(a), n, static_cast<uint8_t*>(prev),
+                                                      kSetTile);
+  RFX_CUDA_TRY(cudaGetLastError());
+  return RFX_OK;
+}
+
+bool aligned_to(const void* p, uint32_t b) { return (reinterpret_cast<uintptr_t>(p) % (b < 16 ? b : 16)) == 0; }
+
+struct SetLayout {
+  FilterLayout f;
+  uint8_t* diff;
+  uint64_t* d_nd;
+  size_t total;
+};
+
+SetLayout set_layout(void* ws, uint32_t op, uint64_t na, uint64_t nb, uint32_t e) {
+  SetLayout L;
+  // union filters B against A, the others filter A against B
+  const uint64_t nf = op == RFX_SET_UNION ? nb : na;
+  L.f = filter_layout(ws, nf);
+  Carver c(ws);
+  c.used = L.f.total;
+  L.diff = op == RFX_SET_UNION ? c.take<uint8_t>(nb * e) : nullptr;
+  L.d_nd = op == RFX_SET_UNION ? c.take<uint64_t>(1) : nullptr;
+  L.total = align_up(c.used, 256);
+  return L;
+}
+
+}  // namespace
+
+size_t set_op_workspace_impl(uint32_t op, uint64_t na, uint64_t nb, uint32_t e) {
+  return set_layout(nullptr, op, na, nb, e).total;
+}
+
+rfx_status set_op_impl(uint32_t op, void* out, uint64_t* d_count, const void* a, uint64_t na, const void* b, uint64_t nb,
+                       uint32_t e, void* ws, size_t wsb, cudaStream_t s) {
+  if (!elem_width(e) || op > RFX_SET_INTERSECTION) return RFX_ERR_UNSUPPORTED;
+  if (!d_count || (na && !a) || (nb && !b) || ((na || nb) && !out)) return RFX_ERR_INVALID;
+  if ((na && !aligned_to(a, e)) || (nb && !aligned_to(b, e)) || (out && !aligned_to(out, e))) return RFX_ERR_INVALID;
+  SetLayout L = set_layout(ws, op, na, nb, e);
+  if (!ws || wsb < L.total) return RFX_ERR_WORKSPACE;
+  uint32_t* err = device_error_word();
+  if (!err) return RFX_ERR_CUDA;
+  RFX_CUDA_TRY(cudaMemsetAsync(ws, 0, L.f.clear, s));
+  SetFilterArgs f;
+  std::memset(&f, 0, sizeof(f));
+  f.status = L.f.status;
+  f.tile_counter = L.f.counter;
+  f.err = err;
+  if (op == RFX_SET_UNION) {
+    f.a = static_cast<const uint8_t*>(b);  // B - A: the copies of B beyond A's
+    f.na = nb;
+    f.b = static_cast<const uint8_t*>(a);
+    f.nb = na;
+    f.out = L.diff;
+    f.d_count = L.d_nd;
+    rfx_status st = dispatch_filter(e, KEEP_UNMATCHED, f, s);
+    if (st != RFX_OK) return st;
+    return dispatch_merge(e, a, na, L.diff, nb, L.d_nd, out, d_count, s);
+  }
+  f.a = static_cast<const uint8_t*>(a);
+  f.na = na;
+  f.b = static_cast<const uint8_t*>(b);
+  f.nb = nb;
+  f.out = static_cast<uint8_t*>(out);
+  f.d_count = d_count;
+  return dispatch_filter(e, op == RFX_SET_INTERSECTION ? KEEP_MATCHED : KEEP_UNMATCHED, f, s);
+}
+
+size_t unique_workspace_impl(uint64_t n, uint32_t e) {
+  FilterLayout f = filter_layout(nullptr, n);
+  Carver c(nullptr);
+  c.used = f.total;
+  c.take<uint8_t>(((n + kSetTile - 1) / kSetTile + 1) * (e < 16 ? 16 : e));
+  return align_up(c.used, 256);
+}
+
+rfx_status unique_impl(void* data, uint64_t n, uint64_t* d_count, uint32_t e, void* ws, size_t wsb, cudaStream_t s) {
+  if (!elem_width(e)) return RFX_ERR_UNSUPPORTED;
+  if (!d_count || (n && !data)) return RFX_ERR_INVALID;
+  if (n && !aligned_to(data, e)) return RFX_ERR_INVALID;
+  FilterLayout f = filter_layout(ws, n);
+  Carver c(ws);
+  c.used = f.total;
+  uint8_t* prev = c.take<uint8_t>(((n + kSetTile - 1) / kSetTile + 1) * (e < 16 ? 16 : e));
+  if (!ws || wsb < align_up(c.used, 256)) return RFX_ERR_WORKSPACE;
+  uint32_t* err = device_error_word();
+  if (!err) return RFX_ERR_CUDA;
+  RFX_CUDA_TRY(cudaMemsetAsync(ws, 0, f.clear, s));
+  if (n) {
+    rfx_status st;
+    switch (e) {
+      case 1: st = launch_prev<1>(data, n, prev, s); break;
+      case 2: st = launch_prev<2>(data, n, prev, s); break;
+      case 4: st = launch_prev<4>(data, n, prev, s); break;
+      case 8: st = launch_prev<8>(data, n, prev, s); break;
+      default: st = launch_prev<16>(data, n, prev, s); break;
+    }
+    if (st != RFX_OK) return st;
+  }
+  SetFilterArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.a = static_cast<const uint8_t*>(data);
+  a.na = n;
+  a.prev = prev;
+  a.out = static_cast<uint8_t*>(data);
+  a.d_count = d_count;
+  a.status = f.status;
+  a.tile_counter = f.counter;
+  a.err = err;
+  return dispatch_filter(e, KEEP_HEADS, a, s);
+}
+
+namespace {
+uint32_t type_bytes(uint64_t type) {
+  switch (type) {
+    case RFX_I8: return 1;
+    case RFX_I16: return 2;
+    case RFX_I32: return 4;
+    case RFX_I64: return 8;
+    case RFX_I128: return 16;
+    default: return 0;
+  }
+}
+
+__global__ void scale_kernel(uint64_t* p, uint64_t factor) { *p *= factor; }
+
+// Reference byte-size convention: *size (device) = output bytes.
+rfx_status set_compat(uint32_t op, void* result, uint64_t* size, void* lb, void* le, void* rb, void* re, uint64_t type) {
+  const uint32_t e = type_bytes(type);
+  if (!e) return RFX_ERR_UNSUPPORTED;
+  if (!size) return RFX_ERR_INVALID;
+  const uint64_t na = (uint64_t)((uint8_t*)le - (uint8_t*)lb) / e, nb = (uint64_t)((uint8_t*)re - (uint8_t*)rb) / e;
+  cudaStream_t s = 0;
+  const size_t need = set_op_workspace_impl(op, na, nb, e);
+  void* ws = nullptr;
+  RFX_CUDA_TRY(cudaMallocAsync(&ws, need, s));
+  rfx_status st = set_op_impl(op, result, size, lb, na, rb, nb, e, ws, need, s);
+  if (st == RFX_OK) scale_kernel<<<1, 1, 0, s>>>(size, e);
+  cudaFreeAsync(ws, s);
+  if (st != RFX_OK) return st;
+  RFX_CUDA_TRY(cudaStreamSynchronize(s));
+  return RFX_OK;
+}
+}  // namespace
+
+}  // namespace rfx
+
+using namespace rfx;
+
+extern "C" size_t rfx_set_op_workspace(uint32_t op, uint64_t na, uint64_t nb, uint32_t elem_bytes) {
+  return set_op_workspace_impl(op, na, nb, elem_bytes);
+}
+
+extern "C" rfx_status rfx_set_op(uint32_t op, void* out, uint64_t* d_count, const void* a, uint64_t na, const void* b,
+                                 uint64_t nb, uint32_t elem_bytes, void* workspace, size_t workspace_bytes, void* stream) {
+  return set_op_impl(op, out, d_count, a, na, b, nb, elem_bytes, workspace, workspace_bytes, as_stream(stream));
+}
+
+extern "C" size_t rfx_unique_workspace(uint64_t n, uint32_t elem_bytes) { return unique_workspace_impl(n, elem_bytes); }
+
+extern "C" rfx_status rfx_unique(void* data, uint64_t n, uint64_t* d_count, uint32_t elem_bytes, void* workspace,
+                                 size_t workspace_bytes, void* stream) {
+  return unique_impl(data, n, d_count, elem_bytes, workspace, workspace_bytes, as_stream(stream));
+}
+
+extern "C" rfx_status rfx_set_union_compat(void* result, uint64_t* size, void* lbegin, void* lend, void* rbegin,
+                                           void* rend, uint32_t type) {
+  return set_compat(RFX_SET_UNION, result, size, lbegin, lend, rbegin, rend, type);
+}
+
+extern "C" rfx_status rfx_difference_compat(void* result, uint64_t* size, void* lbegin, void* lend, void* rbegin,
+                                            void* rend, uint32_t type) {
+  return set_compat(RFX_SET_DIFFERENCE, result, size, lbegin, lend, rbegin, rend, type);
+}
+
+extern "C" rfx_status rfx_intersection_compat(void* result, uint64_t* size, void* lbegin, void* lend, void* rbegin,
+                                              void* rend, uint32_t type) {
+  return set_compat(RFX_SET_INTERSECTION, result, size, lbegin, lend, rbegin, rend, type);
+}
+
+// redfox::unique (Unique.cu:36-114): *size (device) holds the input bytes and receives
+// the output bytes; types I8..I64.  A single element is left as it is, as in the
+// reference.
+extern "C" rfx_status rfx_unique_compat(void* begin, uint64_t* size, uint64_t type) {
+  const uint32_t e = type_bytes(type);
+  if (!e || e > 8) return RFX_ERR_UNSUPPORTED;
+  if (!size) return RFX_ERR_INVALID;
+  uint64_t bytes = 0;
+  RFX_CUDA_TRY(cudaMemcpy(&bytes, size, sizeof(bytes), cudaMemcpyDeviceToHost));
+  const uint64_t n = bytes / e;
+  if (n <= 1) return RFX_OK;
+  cudaStream_t s = 0;
+  const size_t need = unique_workspace_impl(n, e);
+  void* ws = nullptr;
+  RFX_CUDA_TRY(cudaMallocAsync(&ws, need, s));
+  rfx_status st = unique_impl(begin, n, size, e, ws, need, s);
+  if (st == RFX_OK) scale_kernel<<<1, 1, 0, s>>>(size, e);
+  cudaFreeAsync(ws, s);
+  if (st != RFX_OK) return st;
+  RFX_CUDA_TRY(cudaStreamSynchronize(s));
+  return RFX_OK;
+}

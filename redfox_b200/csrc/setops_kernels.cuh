@@ -1,0 +1,175 @@
+// setops_kernels.cuh -- multiset set operations on sorted arrays and unique.
+//
+// STL / thrust semantics (thrust::set_union / set_difference in Union.cu:47-148 and
+// Difference.cu:35-143; std::set_intersection as moderngpu's benchmarksets.cu:95-125
+// checks it): a value occurring m times in A and n times in B occurs min(m, n) times in
+// the intersection, max(m - n, 0) times in A - B and max(m, n) times in the union.
+//   * intersection / difference keep A[i] when its rank within its run of equal values
+//     is below / not below the number of equal values in B -- one filtering pass with
+//     stable compaction (decoupled look-back);
+//   * union = merge(A, B - A) with A first on ties, by merge path (no scan needed);
+//   * unique keeps the first of each run, in place.
+#pragma once
+
+#include "search.cuh"
+
+namespace rfx {
+
+constexpr int kSetThreads = 256;
+constexpr int kSetIPT = 4;
+constexpr int kSetTile = kSetThreads * kSetIPT;
+constexpr int kMergeVT = 8;
+constexpr int kMergeTile = kSetThreads * kMergeVT;
+
+enum SetFilter : int { KEEP_MATCHED = 0, KEEP_UNMATCHED = 1, KEEP_HEADS = 2 };
+
+struct SetFilterArgs {
+  const uint8_t* a;
+  uint64_t na;
+  const uint8_t* b;
+  uint64_t nb;
+  const uint8_t* prev;   // KEEP_HEADS: element before each tile (saved before in-place writes)
+  uint8_t* out;
+  uint64_t* d_count;
+  uint64_t* status;
+  uint32_t* tile_counter;
+  uint32_t* err;
+};
+
+__device__ __forceinline__ uint64_t block_exclusive_u32(uint32_t x, uint32_t* s_warp, uint32_t* total) {
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  uint32_t incl = x;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= (uint32_t)o) incl += y;
+  }
+  if (lane == 31) s_warp[warp] = incl;
+  __syncthreads();
+  uint32_t wpre = 0, tot = 0;
+  for (uint32_t w = 0; w < blockDim.x / 32; ++w) {
+    if (w < warp) wpre += s_warp[w];
+    tot += s_warp[w];
+  }
+  *total = tot;
+  return wpre + incl - x;
+}
+
+template <int E, int MODE>
+__global__ void __launch_bounds__(kSetThreads) set_filter_kernel(const SetFilterArgs p) {
+  __shared__ uint32_t s_warp[kSetThreads / 32];
+  __shared__ uint64_t s_prefix;
+  __shared__ uint32_t s_tile;
+  const uint32_t t = threadIdx.x;
+  const uint64_t num_tiles = (p.na + kSetTile - 1) / kSetTile;
+  const KeyView<E> A{p.a, p.na, 0};
+  const KeyView<E> B{p.b, p.nb, 0};
+  while (true) {
+    if (t == 0) s_tile = atomicAdd(p.tile_counter, 1u);
+    __syncthreads();
+    const uint64_t tile = s_tile;
+    if (tile >= num_tiles) break;
+    const uint64_t first = tile * kSetTile + (uint64_t)t * kSetIPT;
+    u128 v[kSetIPT];
+    bool keep[kSetIPT];
+    uint32_t kept = 0;
+    // every input of this tile is read before its aggregate is published, which keeps
+    // the in-place unique safe (writes land below the inputs of later tiles)
+#pragma unroll
+    for (int j = 0; j < kSetIPT; ++j) {
+      const uint64_t i = first + j;
+      keep[j] = false;
+      if (i < p.na) v[j] = A.key(i);
+    }
+    if constexpr (MODE == KEEP_HEADS) {
+      u128 before = 0;
+      if (first < p.na && first > 0) {
+        before = (t == 0) ? load_u128<E>(p.prev, tile) : A.key(first - 1);
+      }
+#pragma unroll
+      for (int j = 0; j < kSetIPT; ++j) {
+        const uint64_t i = first + j;
+        if (i >= p.na) continue;
+        keep[j] = i == 0 || v[j] != (j == 0 ? before : v[j - 1]);
+      }
+    } else {
+      uint64_t run_start = 0, blo = 0, bhi = 0;
+      u128 prevk = 0;
+#pragma unroll
+      for (int j = 0; j < kSetIPT; ++j) {
+        const uint64_t i = first + j;
+        if (i >= p.na) continue;
+        if (j == 0 || v[j] != prevk) {
+          run_start = (j > 0) ? i : bsearch<E>(A, v[j], 0, i, false);
+          blo = (j == 0) ? bsearch<E>(B, v[j], 0, p.nb, false) : gallop<E>(B, v[j], bhi, false);
+          bhi = gallop<E>(B, v[j], blo, true);
+          prevk = v[j];
+        }
+        const uint64_t rank = i - run_start, nbeq = bhi - blo;
+        keep[j] = MODE == KEEP_MATCHED ? rank < nbeq : rank >= nbeq;
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < kSetIPT; ++j) kept += keep[j] ? 1u : 0u;
+    uint32_t btot;
+    const uint64_t ex = block_exclusive_u32(kept, s_warp, &btot);
+    if ((t >> 5) == 0) {
+      const uint64_t pre = lookback_exclusive(p.status, (uint32_t)tile, btot, p.err);
+      if (t == 0) {
+        s_prefix = pre;
+        if (tile == num_tiles - 1) *p.d_count = pre + btot;
+      }
+    }
+    __syncthreads();
+    uint64_t pos = s_prefix + ex;
+#pragma unroll
+    for (int j = 0; j < kSetIPT; ++j) {
+      if (!keep[j]) continue;
+      if (pos < p.na) store_u128<E>(p.out, pos, v[j]);
+      ++pos;
+    }
+    __syncthreads();
+  }
+  if (p.na == 0 && blockIdx.x == 0 && t == 0) *p.d_count = 0;
+}
+
+// The element before each tile, saved before an in-place pass overwrites it.
+template <int E>
+__global__ void tile_prev_kernel(const uint8_t* a, uint64_t n, uint8_t* prev, uint64_t tile_items) {
+  const uint64_t tiles = (n + tile_items - 1) / tile_items;
+  for (uint64_t tl = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; tl < tiles; tl += (uint64_t)gridDim.x * blockDim.x)
+    store_u128<E>(prev, tl, tl == 0 ? (u128)0 : load_u128<E>(a, tl * tile_items - 1));
+}
+
+// Merge of A and D (A first on ties): the union.
+template <int E>
+__global__ void __launch_bounds__(kSetThreads)
+merge_kernel(const uint8_t* a, uint64_t na, const uint8_t* d, uint64_t nd_max, const uint64_t* d_nd, uint8_t* out,
+             uint64_t* d_count) {
+  const uint64_t nd = d_nd ? min(nd_max, *d_nd) : nd_max;
+  const uint64_t total = na + nd;
+  if (blockIdx.x == 0 && threadIdx.x == 0) *d_count = total;
+  const KeyView<E> A{a, na, 0};
+  const KeyView<E> D{d, nd, 0};
+  const uint64_t stride = (uint64_t)gridDim.x * kMergeTile;
+  for (uint64_t k0 = (uint64_t)blockIdx.x * kMergeTile + (uint64_t)threadIdx.x * kMergeVT; k0 < total; k0 += stride) {
+    // merge path: i = number of A elements among the first k0 outputs
+    uint64_t lo = k0 > nd ? k0 - nd : 0, hi = k0 < na ? k0 : na;
+    while (lo < hi) {
+      const uint64_t mid = lo + ((hi - lo) >> 1);
+      if (A.key(mid) <= D.key(k0 - mid - 1)) lo = mid + 1;
+      else hi = mid;
+    }
+    uint64_t i = lo, j = k0 - lo;
+#pragma unroll
+    for (int v = 0; v < kMergeVT; ++v) {
+      const uint64_t k = k0 + v;
+      if (k >= total) break;
+      const bool take_a = j >= nd || (i < na && A.key(i) <= D.key(j));
+      if (take_a) store_u128<E>(out, k, A.key(i++));
+      else store_u128<E>(out, k, D.key(j++));
+    }
+  }
+}
+
+}  // namespace rfx

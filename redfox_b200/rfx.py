@@ -308,3 +308,169 @@ def sort_pairs(keys, values=None, begin_bit=0, end_bit=None, flags=0, stream=Non
     s = Sorter(n, _width(keys), 0 if values is None else _width(values), begin_bit, end_bit, device=keys.device)
     s(keys, values, flags, stream)
     return keys, values
+
+
+# ---------------------------------------------------------------------------- reduce
+VAL_NONE, VAL_U32, VAL_I64 = 0, 1, 2
+
+
+def _declare_more():
+    P, u32, u64, sz, st = C.c_void_p, C.c_uint32, C.c_uint64, C.c_size_t, C.c_int
+    more = {
+        "rfx_reduce_by_key_workspace": (sz, [u64]),
+        "rfx_reduce_by_key": (st, [P, u64, P, u32, P, u32, P, P, P, P, P, sz, P]),
+        "rfx_count_compat": (st, [P, P, P, P, P, P, u32]),
+        "rfx_total_64_32_compat": (st, [P, P, P, P, P, P]),
+        "rfx_total_i64_compat": (st, [P, P, P, P, P, P, u32]),
+    }
+    for name, (res, args) in more.items():
+        f = getattr(LIB, name)
+        f.restype = res
+        f.argtypes = args
+
+
+_declare_more()
+
+
+def reduce_by_key(keys, values=None, value_kind=None, counts=True, d_n=None, stream=None):
+    """Runs of equal keys -> (out_keys, out_sums or None, out_counts or None, groups)."""
+    import torch
+    n = keys.shape[0]
+    kb = _width(keys)
+    if value_kind is None:
+        value_kind = VAL_NONE if values is None else (VAL_I64 if values.element_size() == 8 else VAL_U32)
+    out_k = torch.empty_like(keys)
+    out_v = None
+    if value_kind != VAL_NONE:
+        out_v = torch.empty(n, dtype=torch.int64 if value_kind == VAL_I64 else torch.int32, device=keys.device)
+    out_c = torch.empty(n, dtype=torch.int32, device=keys.device) if counts else None
+    g = torch.zeros(1, dtype=torch.int64, device=keys.device)
+    wsb = LIB.rfx_reduce_by_key_workspace(n)
+    ws = _empty_bytes(wsb, keys.device)
+    check("rfx_reduce_by_key", LIB.rfx_reduce_by_key(_ptr(keys), n, _ptr(d_n), kb, _ptr(values), value_kind,
+                                                     _ptr(out_k), _ptr(out_v), _ptr(out_c), _ptr(g), _ptr(ws), wsb,
+                                                     _stream(stream)))
+    k = int(g.item())
+    return out_k[:k], (out_v[:k] if out_v is not None else None), (out_c[:k] if out_c is not None else None), k
+
+
+# ---------------------------------------------------------------------------- join / set ops
+SET_UNION, SET_DIFFERENCE, SET_INTERSECTION = 0, 1, 2
+
+
+def _declare_join():
+    P, u32, u64, sz, st = C.c_void_p, C.c_uint32, C.c_uint64, C.c_size_t, C.c_int
+    more = {
+        "rfx_join_find_bounds_workspace": (sz, [u64]),
+        "rfx_join_find_bounds": (st, [P, P, P, P, u64, P, u64, u32, P, sz, P]),
+        "rfx_join_expand": (st, [P, P, u64, P, P, P, u64, P]),
+        "rfx_join_gather": (st, [P, u32, u64, P, P, P, P, u32, P, u32, u32, P, u32, u32, P]),
+        "rfx_join_tuples_workspace": (sz, [u64]),
+        "rfx_join_tuples": (st, [P, u32, u64, P, P, u64, u32, u32, P, u64, u32, u32, P, sz, P]),
+        "rfx_find_bounds_compat": (st, [P, P, P, P, u64, P, u64, u32]),
+        "rfx_join_compat": (st, [P, P, u64, P, P, u64]),
+        "rfx_set_op_workspace": (sz, [u32, u64, u64, u32]),
+        "rfx_set_op": (st, [u32, P, P, P, u64, P, u64, u32, P, sz, P]),
+        "rfx_unique_workspace": (sz, [u64, u32]),
+        "rfx_unique": (st, [P, u64, P, u32, P, sz, P]),
+        "rfx_set_union_compat": (st, [P, P, P, P, P, P, u32]),
+        "rfx_difference_compat": (st, [P, P, P, P, P, P, u32]),
+        "rfx_intersection_compat": (st, [P, P, P, P, P, P, u32]),
+        "rfx_unique_compat": (st, [P, P, u64]),
+    }
+    for name, (res, args) in more.items():
+        f = getattr(LIB, name)
+        f.restype = res
+        f.argtypes = args
+
+
+_declare_join()
+
+
+def find_bounds(left, right, stream=None):
+    import torch
+    nl, nr = left.shape[0], right.shape[0]
+    kb = _width(left)
+    lb = torch.empty(nl, dtype=torch.int32, device=left.device)
+    sc = torch.empty(nl, dtype=torch.int32, device=left.device)
+    tot = torch.zeros(1, dtype=torch.int64, device=left.device)
+    wsb = LIB.rfx_join_find_bounds_workspace(nl)
+    ws = _empty_bytes(wsb, left.device)
+    check("rfx_join_find_bounds", LIB.rfx_join_find_bounds(_ptr(lb), _ptr(sc), _ptr(tot), _ptr(left), nl, _ptr(right),
+                                                           nr, kb, _ptr(ws), wsb, _stream(stream)))
+    return lb, sc, int(tot.item())
+
+
+def join_expand(lb, scan, nout, stream=None):
+    import torch
+    li = torch.empty(max(1, nout), dtype=torch.int32, device=lb.device)
+    ri = torch.empty(max(1, nout), dtype=torch.int32, device=lb.device)
+    check("rfx_join_expand", LIB.rfx_join_expand(_ptr(li), _ptr(ri), nout, None, _ptr(lb), _ptr(scan), lb.shape[0],
+                                                 _stream(stream)))
+    return li[:nout], ri[:nout]
+
+
+def join_gather(out_bytes, li, ri, lkey, lval, lval_bits, rval, rval_bits, stream=None):
+    import torch
+    n = li.shape[0]
+    out = torch.empty((max(1, n), out_bytes), dtype=torch.uint8, device=li.device)
+    check("rfx_join_gather", LIB.rfx_join_gather(
+        _ptr(out), out_bytes, n, None, _ptr(li), _ptr(ri), _ptr(lkey), _width(lkey), _ptr(lval),
+        _width(lval) if lval is not None else 0, lval_bits, _ptr(rval), _width(rval) if rval is not None else 0,
+        rval_bits, _stream(stream)))
+    return out[:n]
+
+
+class TupleJoin:
+    """A prepared fused tuple join (workspace allocated once)."""
+
+    def __init__(self, nl, device="cuda"):
+        self.wsb = LIB.rfx_join_tuples_workspace(nl)
+        self.ws = _empty_bytes(self.wsb, device)
+        import torch
+        self.count = torch.zeros(1, dtype=torch.int64, device=device)
+
+    def __call__(self, out, capacity, left, lvbits, right, rvbits, stream=None):
+        check("rfx_join_tuples", LIB.rfx_join_tuples(_ptr(out), _width(out), capacity, _ptr(self.count), _ptr(left),
+                                                     left.shape[0], _width(left), lvbits, _ptr(right), right.shape[0],
+                                                     _width(right), rvbits, _ptr(self.ws), self.wsb, _stream(stream)))
+
+
+def join_tuples(left, lvbits, right, rvbits, out_bytes, capacity=None, stream=None):
+    """Returns (rows, total).  With capacity None the count is taken first (two calls)."""
+    import torch
+    tj = TupleJoin(left.shape[0], device=left.device)
+    if capacity is None:
+        dummy = torch.empty((1, out_bytes), dtype=torch.uint8, device=left.device)
+        tj(dummy, 0, left, lvbits, right, rvbits, stream)
+        capacity = int(tj.count.item())
+    out = torch.empty((max(1, capacity), out_bytes), dtype=torch.uint8, device=left.device)
+    tj(out, capacity, left, lvbits, right, rvbits, stream)
+    total = int(tj.count.item())
+    return out[:min(total, capacity)], total
+
+
+def set_op(op, a, b, stream=None):
+    import torch
+    na, nb = a.shape[0], b.shape[0]
+    e = _width(a)
+    out = torch.empty((max(1, na + nb),) + tuple(a.shape[1:]), dtype=a.dtype, device=a.device)
+    cnt = torch.zeros(1, dtype=torch.int64, device=a.device)
+    wsb = LIB.rfx_set_op_workspace(op, na, nb, e)
+    ws = _empty_bytes(wsb, a.device)
+    check("rfx_set_op", LIB.rfx_set_op(op, _ptr(out), _ptr(cnt), _ptr(a), na, _ptr(b), nb, e, _ptr(ws), wsb,
+                                       _stream(stream)))
+    k = int(cnt.item())
+    return out[:k]
+
+
+def unique(data, stream=None):
+    """In place; returns the kept prefix."""
+    import torch
+    n = data.shape[0]
+    e = _width(data)
+    cnt = torch.zeros(1, dtype=torch.int64, device=data.device)
+    wsb = LIB.rfx_unique_workspace(n, e)
+    ws = _empty_bytes(wsb, data.device)
+    check("rfx_unique", LIB.rfx_unique(_ptr(data), n, _ptr(cnt), e, _ptr(ws), wsb, _stream(stream)))
+    return data[:int(cnt.item())]

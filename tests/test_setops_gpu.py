@@ -1,0 +1,107 @@
+"""Set operations and unique against the oracle and the reference's golden vectors."""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+from redfox_b200 import rfx as R
+
+from helpers import to_np
+
+pytestmark = pytest.mark.gpu
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def _dev(a, cuda):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a)).to(cuda)
+
+
+def _cases():
+    g = np.load(os.path.join(GOLD, "setops.npz"))
+    return g, sorted({k.rsplit("_", 1)[0] for k in g.files if k.endswith("_a")})
+
+
+def test_set_ops_match_reference_golden(cuda):
+    g, keys = _cases()
+    for key in keys:
+        a, b = g[key + "_a"], g[key + "_b"]
+        da, db = _dev(a, cuda), _dev(b, cuda)
+        assert np.array_equal(to_np(R.set_op(R.SET_UNION, da, db)), g[key + "_union"]), key
+        assert np.array_equal(to_np(R.set_op(R.SET_DIFFERENCE, da, db)), g[key + "_difference"]), key
+        if key + "_intersection" in g.files:
+            assert np.array_equal(to_np(R.set_op(R.SET_INTERSECTION, da, db)), g[key + "_intersection"]), key
+        if key + "_unique" in g.files:
+            assert np.array_equal(to_np(R.unique(_dev(a, cuda))), g[key + "_unique"]), key
+
+
+@pytest.mark.parametrize("dtype", [np.uint8, np.uint16, np.uint32, np.uint64])
+@pytest.mark.parametrize("na,nb,hi", [(0, 0, 10), (0, 100, 10), (100, 0, 10), (1, 1, 2), (1023, 1025, 50),
+                                      (100003, 70001, 3000), (200000, 200000, 2**31)])
+def test_set_ops_random(cuda, dtype, na, nb, hi):
+    rng = np.random.default_rng(na + nb)
+    hi = min(hi, np.iinfo(dtype).max)
+    a = np.sort(rng.integers(0, hi, na)).astype(dtype)
+    b = np.sort(rng.integers(0, hi, nb)).astype(dtype)
+    da, db = _dev(a, cuda), _dev(b, cuda)
+    for op, ref in ((R.SET_UNION, O.set_union), (R.SET_DIFFERENCE, O.set_difference),
+                    (R.SET_INTERSECTION, O.set_intersection)):
+        assert np.array_equal(to_np(R.set_op(op, da, db)), ref(a, b)), op
+    assert np.array_equal(to_np(R.unique(_dev(a, cuda))), O.unique(a))
+    assert R.device_status() == R.OK
+
+
+def test_set_ops_128bit(cuda):
+    rng = np.random.default_rng(8)
+    def mk(n):
+        k = np.sort(rng.integers(0, 2000, n)).astype(np.uint64)
+        a = np.zeros((n, 16), np.uint8)
+        a.view(np.uint64)[:, 1] = k // 5
+        a.view(np.uint64)[:, 0] = k % 5
+        return a
+    a, b = mk(40000), mk(30000)
+    da, db = _dev(a, cuda), _dev(b, cuda)
+    assert np.array_equal(to_np(R.set_op(R.SET_UNION, da, db)), O.set_union(a, b))
+    assert np.array_equal(to_np(R.set_op(R.SET_DIFFERENCE, da, db)), O.set_difference(a, b))
+    assert np.array_equal(to_np(R.set_op(R.SET_INTERSECTION, da, db)), O.set_intersection(a, b))
+    assert np.array_equal(to_np(R.unique(_dev(a, cuda))), O.unique(a))
+
+
+def test_unique_all_equal_and_all_distinct(cuda):
+    import torch
+    n = 1_000_003
+    x = torch.full((n,), 5, dtype=torch.int32, device=cuda)
+    assert R.unique(x).shape[0] == 1
+    y = torch.arange(n, dtype=torch.int64, device=cuda)
+    assert torch.equal(R.unique(y), torch.arange(n, dtype=torch.int64, device=cuda))
+
+
+def test_reference_compatible_set_entries(cuda):
+    import torch
+    g, keys = _cases()
+    a, b = g["e4_c1_a"], g["e4_c1_b"]
+    da, db = _dev(a, cuda), _dev(b, cuda)
+    out = torch.zeros(len(a) + len(b), dtype=torch.int32, device=cuda)
+    size = torch.zeros(1, dtype=torch.int64, device=cuda)
+    P = C.c_void_p
+    torch.cuda.synchronize()
+    assert R.LIB.rfx_set_union_compat(P(out.data_ptr()), P(size.data_ptr()), P(da.data_ptr()),
+                                      P(da.data_ptr() + 4 * len(a)), P(db.data_ptr()), P(db.data_ptr() + 4 * len(b)),
+                                      R.I32) == R.OK
+    k = int(size.item()) // 4
+    assert np.array_equal(to_np(out)[:k].view(np.uint32), g["e4_c1_union"])
+    assert R.LIB.rfx_difference_compat(P(out.data_ptr()), P(size.data_ptr()), P(da.data_ptr()),
+                                       P(da.data_ptr() + 4 * len(a)), P(db.data_ptr()), P(db.data_ptr() + 4 * len(b)),
+                                       R.I32) == R.OK
+    k = int(size.item()) // 4
+    assert np.array_equal(to_np(out)[:k].view(np.uint32), g["e4_c1_difference"])
+    u = _dev(a, cuda)
+    size = torch.tensor([4 * len(a)], dtype=torch.int64, device=cuda)
+    torch.cuda.synchronize()
+    assert R.LIB.rfx_unique_compat(P(u.data_ptr()), P(size.data_ptr()), R.I32) == R.OK
+    k = int(size.item()) // 4
+    assert np.array_equal(to_np(u)[:k], g["e4_c1_unique"])
+    assert R.LIB.rfx_set_union_compat(P(out.data_ptr()), P(size.data_ptr()), P(da.data_ptr()), P(da.data_ptr()),
+                                      P(db.data_ptr()), P(db.data_ptr()), 99) == R.ERR_UNSUPPORTED

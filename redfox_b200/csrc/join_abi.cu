@@ -213,6 +213,7 @@ extern "C" rfx_status rfx_join_tuples(void* out, uint32_t out_bytes, uint64_t ca
   j.left = static_cast<const uint8_t*>(left);
   j.nl = nl;
   j.right = static_cast<const uint8_t*>(right);
+  j.nr = nr;
   j.rv_bits = right_value_bits;
   j.lb64 = L.lb64;
   j.off64 = L.off64;

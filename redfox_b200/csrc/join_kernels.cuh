@@ -248,6 +248,7 @@ struct TupleJoinArgs {
   const uint8_t* left;
   uint64_t nl;
   const uint8_t* right;
+  uint64_t nr;
   uint32_t rv_bits;
   const uint64_t* lb64;
   const uint64_t* off64;   // nl + 1 entries
@@ -286,7 +287,7 @@ __global__ void __launch_bounds__(kJoinThreads) tuple_join_kernel(const TupleJoi
         offi = __ldg(a.off64 + i);
       }
       const uint64_t j = lbi + (k - offi);
-      store_u128<OE>(a.out, k, lrow | (load_u128<RE>(a.right, j) & rmask));
+      if (j < a.nr) store_u128<OE>(a.out, k, lrow | (load_u128<RE>(a.right, j) & rmask));  // guards a timed-out scan
     }
   }
 }

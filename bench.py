@@ -266,6 +266,7 @@ def main_ours(args):
 
     from redfox_b200 import rfx as R
     from redfox_b200 import workloads as WL
+    from redfox_b200.partition import merge_group_tables, partition_seed
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -279,7 +280,7 @@ def main_ours(args):
     stream = torch.cuda.current_stream()
 
     # each rank's partition: rows [rank*n, (rank+1)*n) of the seeded table, made on device
-    rows = R.gen_uniform_rows(n, WL.FACT_WIDTHS, WL.FACT_SEED + rank, WL.FACT_LO, WL.FACT_HI, device=dev)
+    rows = R.gen_uniform_rows(n, WL.FACT_WIDTHS, partition_seed(WL.FACT_SEED, rank), WL.FACT_LO, WL.FACT_HI, device=dev)
     plan = WL.fact_plan(n, device=dev)
     nacc = plan.G * (plan.nsum + 1)
     gacc = plan.ws[: nacc * 8].view(torch.int64)
@@ -288,7 +289,7 @@ def main_ours(args):
     def step():
         plan.launch(rows)
         if world > 1:
-            dist.all_reduce(gacc)
+            merge_group_tables(gacc)
 
     for _ in range(args.warmup):
         step()
@@ -315,7 +316,7 @@ def main_ours(args):
         plan.launch(rows)
         k_ev[i][1].record(stream)
         if world > 1:
-            dist.all_reduce(gacc)
+            merge_group_tables(gacc)
     ev1.record(stream)
     torch.cuda.synchronize()
     if world > 1:
@@ -343,7 +344,7 @@ def main_ours(args):
         dev_in.copy_(host, non_blocking=True)
         plan.launch(dev_in)
         if world > 1:
-            dist.all_reduce(gacc)
+            merge_group_tables(gacc)
         out_k.copy_(plan.keys, non_blocking=True)
         out_s.copy_(plan.sums[:, :plan.nsum], non_blocking=True)
         out_c.copy_(plan.counts, non_blocking=True)

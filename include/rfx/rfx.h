@@ -307,6 +307,26 @@ rfx_status rfx_intersection_compat(void* result, uint64_t* size, void* lbegin, v
                                    void* rbegin, void* rend, uint32_t type);
 rfx_status rfx_unique_compat(void* begin, uint64_t* size, uint64_t type);
 
+/* rfx_filter_aggregate for callers that cannot allocate device memory when they call it:
+ * a runtime that has already handed all device memory out by liveness, code recording a
+ * stream capture, or a request path that must not touch the allocator.  It has no
+ * counterpart in the reference.  The arguments and outputs are rfx_filter_aggregate's
+ * minus the workspace; its scratch is a fixed array inside the library (about 160 KiB,
+ * held by every GPU that loads the library until exit), so it allocates nothing.
+ * Limits: at most 4096 groups x (nsum + 1) <= 20480 accumulators -- a larger plan gets
+ * RFX_ERR_CAPACITY.  The first call on a device looks the array's address up; make it
+ * before any stream capture.  All calls share the array: calls whose kernels overlap on
+ * the GPU race (order them on one stream).  A row outside the declared group domains is
+ * recorded as RFX_ERR_CAPACITY in *d_error (a device word the caller zeroes; may be
+ * NULL), not in the library's error word. */
+rfx_status rfx_filter_aggregate_noalloc(const void* in, uint64_t n, const rfx_tuple* in_type,
+                                        const rfx_cmp* cmps, uint32_t ncmp,
+                                        const rfx_arith_expr* ariths, uint32_t narith,
+                                        const uint32_t* group_fields, const uint32_t* group_domain,
+                                        uint32_t ngroup, const uint32_t* sum_fields, uint32_t nsum,
+                                        uint64_t* out_keys, int64_t* out_sums, uint64_t* out_counts,
+                                        uint64_t* d_groups, uint32_t* d_error, void* stream);
+
 /* ---------------------------------------------------------------- synthetic data */
 /* Column j of row i = lo[j] + mulhi64(rand(seed, stream_j, i), hi[j] - lo[j]) with the
  * SplitMix64 stream below, packed as `type`.  The generator behind the benchmarks. */

@@ -202,6 +202,19 @@ rfx_status rfx_reduce_by_key(const void* keys, uint64_t n, const uint64_t* d_n, 
                              void* out_values, uint32_t* out_counts, uint64_t* d_groups,
                              void* workspace, size_t workspace_bytes, void* stream);
 
+/* Reduce-by-key over packed tuples of row_bytes (4/8/16) sorted on their key fields: the
+ * key is the row shifted right by key_shift, the value the value_bits-wide field at
+ * value_shift (summed as exact int64).  Per run, in order: the key in out_key_bytes
+ * (4/8/16), its sum (out_sums, may be NULL) and length (out_counts, may be NULL);
+ * *d_groups = runs.  This is addAgg's split + reduce + count (RelationalAlgebraCompiler.cpp
+ * :7852-8643, Reduce.cu) on a join output without the split pass.  Workspace:
+ * rfx_reduce_by_key_workspace(n). */
+rfx_status rfx_reduce_tuples(const void* rows, uint64_t n, const uint64_t* d_n, uint32_t row_bytes,
+                             uint32_t key_shift, uint32_t value_shift, uint32_t value_bits,
+                             void* out_keys, uint32_t out_key_bytes, int64_t* out_sums,
+                             uint32_t* out_counts, uint64_t* d_groups, void* workspace,
+                             size_t workspace_bytes, void* stream);
+
 /* redfox::count_{8,16,32,128,256} (Reduce.cu:175-660, Reduce.h:43-83) with the reference's
  * argument meaning: *key_size / *value_size are device-resident byte counts, read on
  * entry and replaced by the output byte counts; the u32 value column is summed per run.
@@ -262,6 +275,15 @@ rfx_status rfx_join_tuples(void* out, uint32_t out_bytes, uint64_t capacity, uin
                            uint32_t left_value_bits, const void* right, uint64_t nr,
                            uint32_t right_bytes, uint32_t right_value_bits, void* workspace,
                            size_t workspace_bytes, void* stream);
+
+/* The expansion half of rfx_join_tuples, reusing the bounds a preceding rfx_join_tuples
+ * call (capacity 0 counts only) left in `workspace`: the caller reads *d_count, sizes
+ * `out`, then emits -- the reference's find_bounds -> join_get_result_size -> Resize ->
+ * join_main + gather sequence (RelationalAlgebraCompiler.cpp:4466-5227). */
+rfx_status rfx_join_tuples_emit(void* out, uint32_t out_bytes, uint64_t capacity, const void* left,
+                                uint64_t nl, uint32_t left_bytes, const void* right, uint64_t nr,
+                                uint32_t right_bytes, uint32_t right_value_bits, void* workspace,
+                                size_t workspace_bytes, void* stream);
 
 /* redfox::find_bounds_* and redfox::join with the reference's argument meaning (element
  * counts; *result_size on the device).  Own their scratch, synchronous (default

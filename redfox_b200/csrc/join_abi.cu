@@ -250,3 +250,32 @@ extern "C" rfx_status rfx_join_compat(int32_t* left_indices, int32_t* right_indi
   RFX_CUDA_TRY(cudaStreamSynchronize(0));
   return RFX_OK;
 }
+
+// Second half of rfx_join_tuples: expands and assembles from the bounds and offsets that a
+// preceding rfx_join_tuples call (any capacity, 0 to count only) left in the same
+// workspace, so the caller can size the output from *d_count in between -- the shape of
+// the reference's find_bounds -> join_get_result_size -> Resize -> join_main + gather.
+extern "C" rfx_status rfx_join_tuples_emit(void* out, uint32_t out_bytes, uint64_t capacity, const void* left,
+                                           uint64_t nl, uint32_t left_bytes, const void* right, uint64_t nr,
+                                           uint32_t right_bytes, uint32_t right_value_bits, void* workspace,
+                                           size_t workspace_bytes, void* stream) {
+  const bool w_ok = (left_bytes == 4 || left_bytes == 8 || left_bytes == 16) &&
+                    (right_bytes == 4 || right_bytes == 8 || right_bytes == 16) &&
+                    (out_bytes == 4 || out_bytes == 8 || out_bytes == 16);
+  if (!w_ok || right_value_bits >= right_bytes * 8u) return RFX_ERR_UNSUPPORTED;
+  if (capacity == 0 || nl == 0) return RFX_OK;
+  if (!out || !left || (nr && !right) || !aligned_to(out, out_bytes)) return RFX_ERR_INVALID;
+  FbLayout L = fb_layout(workspace, nl, true);
+  if (!workspace || workspace_bytes < L.total) return RFX_ERR_WORKSPACE;
+  TupleJoinArgs j;
+  j.left = static_cast<const uint8_t*>(left);
+  j.nl = nl;
+  j.right = static_cast<const uint8_t*>(right);
+  j.nr = nr;
+  j.rv_bits = right_value_bits;
+  j.lb64 = L.lb64;
+  j.off64 = L.off64;
+  j.out = static_cast<uint8_t*>(out);
+  j.cap = capacity;
+  return dispatch_tj(left_bytes, right_bytes, out_bytes, j, as_stream(stream));
+}

@@ -179,3 +179,69 @@ extern "C" rfx_status rfx_total_i64_compat(const void* key_begin, const void* va
   return count_like(key_begin, value_begin, result_key_begin, result_value_begin, key_size, value_size, key_bytes,
                     VAL_I64);
 }
+
+namespace rfx {
+namespace {
+template <int RB, int OKB>
+rfx_status launch_tuples(TupleReduceArgs& a, cudaStream_t s) {
+  auto k = reduce_tuples_kernel<RB, OKB>;
+  const uint64_t tiles = (a.r.n_max + kRedTile - 1) / kRedTile;
+  const int grid = persistent_grid((const void*)k, kRedThreads, 0, tiles ? tiles : 1);
+  k<<<grid, kRedThreads, 0, s>>>(a);
+  RFX_CUDA_TRY(cudaGetLastError());
+  return RFX_OK;
+}
+template <int RB>
+rfx_status launch_tuples_o(uint32_t okb, TupleReduceArgs& a, cudaStream_t s) {
+  switch (okb) {
+    case 4: return launch_tuples<RB, 4>(a, s);
+    case 8: return launch_tuples<RB, 8>(a, s);
+    case 16: return launch_tuples<RB, 16>(a, s);
+    default: return RFX_ERR_UNSUPPORTED;
+  }
+}
+}  // namespace
+}  // namespace rfx
+
+extern "C" rfx_status rfx_reduce_tuples(const void* rows, uint64_t n, const uint64_t* d_n, uint32_t row_bytes,
+                                        uint32_t key_shift, uint32_t value_shift, uint32_t value_bits,
+                                        void* out_keys, uint32_t out_key_bytes, int64_t* out_sums,
+                                        uint32_t* out_counts, uint64_t* d_groups, void* workspace,
+                                        size_t workspace_bytes, void* stream) {
+  if (!(row_bytes == 4 || row_bytes == 8 || row_bytes == 16) || key_shift >= row_bytes * 8u || value_bits == 0 ||
+      value_bits > 64 || value_shift + value_bits > row_bytes * 8u)
+    return RFX_ERR_UNSUPPORTED;
+  if (!d_groups || (n && (!rows || !out_keys))) return RFX_ERR_INVALID;
+  if (n && (reinterpret_cast<uintptr_t>(rows) % row_bytes) != 0) return RFX_ERR_INVALID;
+  cudaStream_t s = as_stream(stream);
+  RedLayout L = red_layout(workspace, n);
+  if (!workspace || workspace_bytes < L.total) return RFX_ERR_WORKSPACE;
+  uint32_t* err = device_error_word();
+  if (!err) return RFX_ERR_CUDA;
+  RFX_CUDA_TRY(cudaMemsetAsync(workspace, 0, L.clear_bytes, s));
+  TupleReduceArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.r.keys = static_cast<const uint8_t*>(rows);
+  a.r.n_max = n;
+  a.r.d_n = d_n;
+  a.r.n_div = 1;
+  a.r.out_keys = static_cast<uint8_t*>(out_keys);
+  a.r.out_vals = out_sums;
+  a.r.out_counts = out_counts;
+  a.r.d_groups = d_groups;
+  a.r.flags = L.flags;
+  a.r.tile_counter = L.counter;
+  a.r.agg = L.agg;
+  a.r.inc = L.inc;
+  a.r.cagg = L.cagg;
+  a.r.cinc = L.cinc;
+  a.r.err = err;
+  a.key_shift = key_shift;
+  a.val_shift = value_shift;
+  a.val_mask = value_bits >= 64 ? ~0ull : ((1ull << value_bits) - 1);
+  switch (row_bytes) {
+    case 4: return launch_tuples_o<4>(out_key_bytes, a, s);
+    case 8: return launch_tuples_o<8>(out_key_bytes, a, s);
+    default: return launch_tuples_o<16>(out_key_bytes, a, s);
+  }
+}

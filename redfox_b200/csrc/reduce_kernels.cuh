@@ -10,6 +10,7 @@
 #pragma once
 
 #include "rfx_device.cuh"
+#include "search.cuh"
 #include "sort_kernels.cuh"
 
 namespace rfx {
@@ -269,6 +270,109 @@ reduce_by_key_kernel(const ReduceArgs a) {
     if (a.d_groups_bytes_k) *a.d_groups_bytes_k = 0;
     if (a.d_groups_bytes_v) *a.d_groups_bytes_v = 0;
   }
+}
+
+// ------------------------------------------------------------------ packed-tuple reduce
+// The same segmented reduction over packed tuples of RB <= 16 bytes: the key is the row
+// shifted right by key_shift (the high key fields), the value a field of the row
+// (int64 sum), and the run key is written in OKB bytes.  Reduces a sorted join output
+// without splitting it into key and value arrays (the split / set_split step of addAgg,
+// RelationalAlgebraCompiler.cpp:7852-8643, fused away).
+
+struct TupleReduceArgs {
+  ReduceArgs r;
+  uint32_t key_shift;
+  uint32_t val_shift;
+  uint64_t val_mask;
+};
+
+template <int RB, int OKB>
+__global__ void __launch_bounds__(kRedThreads)
+reduce_tuples_kernel(const TupleReduceArgs ta) {
+  const ReduceArgs& a = ta.r;
+  __shared__ SegPair s_warp[kRedThreads / 32], s_cwarp[kRedThreads / 32];
+  __shared__ SegPair s_pre, s_cpre;
+  __shared__ uint32_t s_tile;
+  const uint32_t t = threadIdx.x, warp = t >> 5;
+  uint64_t n = a.n_max;
+  if (a.d_n) n = min(n, *a.d_n / a.n_div);
+  const uint64_t num_tiles = (n + kRedTile - 1) / kRedTile;
+  while (true) {
+    if (t == 0) s_tile = atomicAdd(a.tile_counter, 1u);
+    __syncthreads();
+    const uint64_t tile = s_tile;
+    if (tile >= num_tiles) break;
+    const uint64_t first = tile * kRedTile + (uint64_t)t * kRedIPT;
+    u128 key[kRedIPT];
+    uint64_t val[kRedIPT];
+    bool head[kRedIPT], tail[kRedIPT], valid[kRedIPT];
+    u128 prev = 0;
+    if (first > 0 && first < n) prev = load_u128<RB>(a.keys, first - 1) >> ta.key_shift;
+#pragma unroll
+    for (int j = 0; j < kRedIPT; ++j) {
+      const uint64_t i = first + j;
+      valid[j] = i < n;
+      if (valid[j]) {
+        const u128 row = load_u128<RB>(a.keys, i);
+        key[j] = row >> ta.key_shift;
+        val[j] = (uint64_t)(row >> ta.val_shift) & ta.val_mask;
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < kRedIPT; ++j) {
+      const uint64_t i = first + j;
+      if (!valid[j]) {
+        head[j] = false;
+        continue;
+      }
+      head[j] = i == 0 || (j == 0 ? prev != key[0] : key[j - 1] != key[j]);
+    }
+#pragma unroll
+    for (int j = 0; j < kRedIPT; ++j) {
+      const uint64_t i = first + j;
+      if (!valid[j]) tail[j] = false;
+      else if (i + 1 >= n) tail[j] = true;
+      else if (j + 1 < kRedIPT) tail[j] = head[j + 1];
+      else tail[j] = key[j] != (load_u128<RB>(a.keys, i + 1) >> ta.key_shift);
+    }
+    SegPair tp{0, 0}, tc{0, 0};
+#pragma unroll
+    for (int j = 0; j < kRedIPT; ++j) {
+      if (!valid[j]) continue;
+      tp = seg_op(tp, SegPair{head[j] ? 1ull : 0ull, val[j]});
+      tc = seg_op(tc, SegPair{head[j] ? 1ull : 0ull, 1ull});
+    }
+    SegPair btot, bctot;
+    SegPair ex = block_seg_exclusive<kRedThreads>(tp, s_warp, &btot);
+    SegPair cex = block_seg_exclusive<kRedThreads>(tc, s_cwarp, &bctot);
+    if (warp == 0) {
+      SegPair pre, cpre;
+      seg_lookback(a, (uint32_t)tile, btot, bctot, &pre, &cpre);
+      if (t == 0) {
+        s_pre = pre;
+        s_cpre = cpre;
+        if (tile == num_tiles - 1) *a.d_groups = pre.f + btot.f;
+      }
+    }
+    __syncthreads();
+    SegPair run = seg_op(s_pre, ex), crun = seg_op(s_cpre, cex);
+#pragma unroll
+    for (int j = 0; j < kRedIPT; ++j) {
+      if (!valid[j]) continue;
+      run = seg_op(run, SegPair{head[j] ? 1ull : 0ull, val[j]});
+      crun = seg_op(crun, SegPair{head[j] ? 1ull : 0ull, 1ull});
+      if (tail[j]) {
+        const uint64_t g = run.f - 1;
+        if (g < n) {
+          store_u128<OKB>(a.out_keys, g, key[j]);
+          if (a.out_vals) reinterpret_cast<int64_t*>(a.out_vals)[g] = (int64_t)run.v;
+          if (a.out_counts) a.out_counts[g] = (uint32_t)crun.v;
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (n == 0 && blockIdx.x == 0 && t == 0) *a.d_groups = 0;
 }
 
 }  // namespace rfx

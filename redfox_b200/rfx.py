@@ -474,3 +474,51 @@ def unique(data, stream=None):
     ws = _empty_bytes(wsb, data.device)
     check("rfx_unique", LIB.rfx_unique(_ptr(data), n, _ptr(cnt), e, _ptr(ws), wsb, _stream(stream)))
     return data[:int(cnt.item())]
+
+
+def _declare_tuple_ops():
+    P, u32, u64, sz, st = C.c_void_p, C.c_uint32, C.c_uint64, C.c_size_t, C.c_int
+    more = {
+        "rfx_reduce_tuples": (st, [P, u64, P, u32, u32, u32, u32, P, u32, P, P, P, P, sz, P]),
+        "rfx_join_tuples_emit": (st, [P, u32, u64, P, u64, u32, P, u64, u32, u32, P, sz, P]),
+    }
+    for name, (res, args) in more.items():
+        f = getattr(LIB, name)
+        f.restype = res
+        f.argtypes = args
+
+
+_declare_tuple_ops()
+
+
+def reduce_tuples(rows, key_shift, value_shift, value_bits, out_key_bytes, n=None, d_n=None, stream=None):
+    """Runs of equal keys (row >> key_shift) of packed rows -> (keys, sums, counts, groups)."""
+    import torch
+    n = rows.shape[0] if n is None else n
+    kdt = {4: torch.int32, 8: torch.int64}.get(out_key_bytes)
+    keys = (torch.empty(max(1, n), dtype=kdt, device=rows.device) if kdt is not None
+            else torch.empty((max(1, n), 16), dtype=torch.uint8, device=rows.device))
+    sums = torch.empty(max(1, n), dtype=torch.int64, device=rows.device)
+    counts = torch.empty(max(1, n), dtype=torch.int32, device=rows.device)
+    g = torch.zeros(1, dtype=torch.int64, device=rows.device)
+    wsb = LIB.rfx_reduce_by_key_workspace(n)
+    ws = _empty_bytes(wsb, rows.device)
+    check("rfx_reduce_tuples", LIB.rfx_reduce_tuples(_ptr(rows), n, _ptr(d_n), _width(rows), key_shift, value_shift,
+                                                     value_bits, _ptr(keys), out_key_bytes, _ptr(sums), _ptr(counts),
+                                                     _ptr(g), _ptr(ws), wsb, _stream(stream)))
+    k = int(g.item())
+    return keys[:k], sums[:k], counts[:k], k
+
+
+def join_tuples_two_step(left, lvbits, right, rvbits, out_bytes, stream=None):
+    """Count, read the size back, allocate exactly, emit (the reference's shape)."""
+    import torch
+    tj = TupleJoin(left.shape[0], device=left.device)
+    dummy = torch.empty((1, out_bytes), dtype=torch.uint8, device=left.device)
+    tj(dummy, 0, left, lvbits, right, rvbits, stream)
+    total = int(tj.count.item())
+    out = torch.empty((max(1, total), out_bytes), dtype=torch.uint8, device=left.device)
+    check("rfx_join_tuples_emit", LIB.rfx_join_tuples_emit(
+        _ptr(out), out_bytes, total, _ptr(left), left.shape[0], _width(left), _ptr(right), right.shape[0],
+        _width(right), rvbits, _ptr(tj.ws), tj.wsb, _stream(stream)))
+    return out[:total], total

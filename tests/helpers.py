@@ -29,3 +29,62 @@ def fact_oracle(rows):
 
 def to_np(t):
     return t.detach().cpu().numpy()
+
+
+# ---------------------------------------------------------------- plan restatements (oracle)
+def join_aggregate_oracle_data(nr, ns, key_domain):
+    from redfox_b200 import plans as PL
+    key = O.uniform(nr, PL.C0_SEED, 0, 0, key_domain)
+    pay = O.uniform(nr, PL.C0_SEED, 1, 0, 1 << 32)
+    idx = O.uniform(ns, PL.C0_S_SEED, 0, 0, nr)
+    amt = O.uniform(ns, PL.C0_S_SEED, 1, 100, 10_000_000)
+    return O.pack([32, 32], [key, pay]), O.pack([32, 64], [key[idx.astype(np.int64)], amt])
+
+
+def join_aggregate_oracle(r, s):
+    rs = O.sort_pairs(r, begin_bit=32, end_bit=64)
+    ss = O.sort_pairs(s, begin_bit=64, end_bit=96)
+    out = O.join_tuples(rs, 32, ss, 64, 16)
+    limbs = out.view(np.uint64)
+    key = (limbs[:, 1] >> np.uint64(32)).astype(np.uint32)
+    amt = limbs[:, 0].astype(np.int64)
+    k, sums = O.reduce_sum_i64(key, amt)
+    _, counts = O.reduce_count(key)
+    return k, sums, counts, len(out)
+
+
+def three_relation_oracle_data(n1, n2, n3, l5, l2):
+    from redfox_b200 import plans as PL
+    seg = O.uniform(n1, PL.C2_SEED, 0, 0, 5)
+    d1 = O.pack([32, 8], [np.arange(n1, dtype=np.uint64), seg])
+    fk = O.zipf(n2, PL.C2_SEED + 1, 0, n1)
+    date = O.uniform(n2, PL.C2_SEED + 5, 0, 0, 2526)
+    d2 = O.pack([32, 32, 32], [np.arange(n2, dtype=np.uint64), fk, date])
+    fcols = [O.uniform(n3, PL.C2_SEED + 2, 0, 0, n2), O.uniform(n3, PL.C2_SEED + 2, 1, 100, 10_000_000)]
+    f = O.pack([32, 64], fcols)
+    lists = []
+    for cnt, seed in ((l5, PL.C2_SEED + 3), (l2, PL.C2_SEED + 4)):
+        raw = O.uniform(cnt, seed, 0, 0, n2).astype(np.uint32)
+        lists.append(O.unique(O.sort_pairs(raw)))
+    return d1, d2, f, lists[0], lists[1]
+
+
+def three_relation_oracle(d1, d2, f, list_in, list_out):
+    from redfox_b200 import plans as PL
+    d1s = O.select(d1, [32, 8], oracle_cmps([(O.EQ, (O.OPND_VAR, 1), (O.OPND_CONST, PL.C2_SEGMENT), O.I8)]))
+    d2f = O.select(d2, [32, 32, 32], oracle_cmps([(O.GE, (O.OPND_VAR, 2), (O.OPND_CONST, PL.C2_DATE_LO), O.I32),
+                                                  (O.LT, (O.OPND_VAR, 2), (O.OPND_CONST, PL.C2_DATE_HI), O.I32)]))
+    d2s = O.project(d2f, [32, 32, 32], [32, 32], [1, 0])
+    d2s = O.sort_pairs(d2s, begin_bit=32, end_bit=64)
+    j1 = O.join_tuples(d1s, 8, d2s, 32, 16)
+    keys = O.project(j1, [32, 8, 32], [32], [2]).view(np.uint32).ravel()
+    keys = O.sort_pairs(keys)
+    keys = O.set_difference(O.set_intersection(keys, list_in), list_out)
+    fs = O.sort_pairs(f, begin_bit=64, end_bit=96)
+    j2 = O.join_tuples(keys.view(np.uint8).reshape(-1, 4), 0, fs, 64, 16)
+    limbs = j2.view(np.uint64)
+    key = limbs[:, 1].astype(np.uint32)
+    amt = limbs[:, 0].astype(np.int64)
+    k, sums = O.reduce_sum_i64(key, amt)
+    _, counts = O.reduce_count(key)
+    return k, sums, counts

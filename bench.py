@@ -45,6 +45,7 @@ def parse():
     ap.add_argument("--rows", type=int, default=ROWS)
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-operators", action="store_true")
     return ap.parse_args()
 
 
@@ -259,6 +260,151 @@ def main_reference(args):
     return 0
 
 
+# ------------------------------------------------------------------------------ per operator
+def _time_ms(fn, reps, setup=None):
+    """Mean device time of fn() over `reps` calls (CUDA events on the current stream);
+    setup() runs before each call outside the timed interval."""
+    import torch
+    stream = torch.cuda.current_stream()
+    total = 0.0
+    for _ in range(reps):
+        if setup is not None:
+            setup()
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        b.synchronize()
+        total += a.elapsed_time(b)
+    return total / reps
+
+
+def _op_line(n, nbytes, ms, peak, **extra):
+    gbs = nbytes / (ms / 1e3) / 1e9
+    d = {"tuples": n, "ms": ms, "tuples_per_s": n / (ms / 1e3), "algorithmic_bytes": nbytes, "gb_s": gbs,
+         "frac_of_measured_hbm": gbs / peak}
+    d.update(extra)
+    return d
+
+
+def operator_benchmarks(dev, fact_rows, peak, reps=5):
+    """tuples/s and fraction of the measured HBM bandwidth per operator, on the workload
+    shapes (data resident in HBM; inputs larger than L2 except where noted)."""
+    import torch
+
+    from redfox_b200 import plans as PL
+    from redfox_b200 import rfx as R
+    from redfox_b200 import workloads as WL
+
+    ops = {}
+    # select on the 60M-row fact table (64 B rows, ~98% kept)
+    n = fact_rows.shape[0]
+    out = torch.empty_like(fact_rows)
+    cnt = torch.zeros(1, dtype=torch.int64, device=dev)
+    t = R.Tuple.of(WL.FACT_WIDTHS)
+    cm = R.make_cmps(WL.fact_predicate())
+    wsb = R.LIB.rfx_select_workspace(n, R.C.byref(t))
+    ws = R._empty_bytes(wsb, dev)
+
+    def sel():
+        R.check("rfx_select", R.LIB.rfx_select(R._ptr(out), R._ptr(cnt), R._ptr(fact_rows), n, R.C.byref(t), cm, 1,
+                                               R._ptr(ws), wsb, R._stream()))
+    sel()
+    ms = _time_ms(sel, reps)
+    k = int(cnt.item())
+    ops["select_fact_60M"] = _op_line(n, n * 64 + k * 64, ms, peak, kept=k)
+    del out
+
+    # join + aggregate inputs (1M x 4M)
+    r, s = PL.gen_join_aggregate(device=dev)
+    # sort pairs: S rows (16 B) on the 32-bit key field (= b40c sort_pair of u32 key / u64 value)
+    ss = torch.empty_like(s)
+    srt = R.Sorter(s.shape[0], 16, 0, 64, 96, device=dev)
+    ms = _time_ms(lambda: srt(ss), reps, setup=lambda: ss.copy_(s))
+    ns = s.shape[0]
+    ops["sort_pairs_4M_u32key_u64val"] = _op_line(ns, ns * 16 + 4 * 2 * ns * 16, ms, peak, passes=4,
+                                                  note="input 64 MB (fits L2)")
+    rs = r.clone()
+    R.sort_pairs(rs, begin_bit=32, end_bit=64)
+    srt(ss)
+    # fused tuple join (count + emit), 19.3M output rows
+    tj = R.TupleJoin(rs.shape[0], device=dev)
+    dummy = torch.empty((1, 16), dtype=torch.uint8, device=dev)
+    tj(dummy, 0, rs, 32, ss, 64)
+    total = int(tj.count.item())
+    jout = torch.empty((total, 16), dtype=torch.uint8, device=dev)
+    ms = _time_ms(lambda: tj(jout, total, rs, 32, ss, 64), reps)
+    nl, nr = rs.shape[0], ss.shape[0]
+    ops["join_fused_1Mx4M"] = _op_line(total, total * 16 + nl * 8 + nr * 16 + nl * 16, ms, peak,
+                                       inputs=nl + nr)
+    # find_bounds alone on the split u32 keys
+    lk = ((rs.view(torch.int64).view(-1) >> 32) & 0xFFFFFFFF).to(torch.int32)
+    rk = (ss.view(torch.int64).view(-1, 2)[:, 1] & 0xFFFFFFFF).to(torch.int32)
+    lb = torch.empty(nl, dtype=torch.int32, device=dev)
+    sc = torch.empty(nl, dtype=torch.int32, device=dev)
+    tot = torch.zeros(1, dtype=torch.int64, device=dev)
+    fwsb = R.LIB.rfx_join_find_bounds_workspace(nl)
+    fws = R._empty_bytes(fwsb, dev)
+    ms = _time_ms(lambda: R.check("fb", R.LIB.rfx_join_find_bounds(R._ptr(lb), R._ptr(sc), R._ptr(tot), R._ptr(lk), nl,
+                                                                   R._ptr(rk), nr, 4, R._ptr(fws), fwsb, R._stream())),
+                  reps)
+    ops["find_bounds_1Mx4M_u32"] = _op_line(nl, (nl + nr) * 4 + 8 * nl, ms, peak, note="inputs fit L2")
+    # reduce-by-key over the 19.3M-row join output (16 B rows, key = high 32 bits)
+    g = torch.zeros(1, dtype=torch.int64, device=dev)
+    okeys = torch.empty(total, dtype=torch.int32, device=dev)
+    osum = torch.empty(total, dtype=torch.int64, device=dev)
+    ocnt = torch.empty(total, dtype=torch.int32, device=dev)
+    rwsb = R.LIB.rfx_reduce_by_key_workspace(total)
+    rws = R._empty_bytes(rwsb, dev)
+    ms = _time_ms(lambda: R.check("rt", R.LIB.rfx_reduce_tuples(R._ptr(jout), total, None, 16, 96, 0, 64, R._ptr(okeys),
+                                                                4, R._ptr(osum), R._ptr(ocnt), R._ptr(g), R._ptr(rws),
+                                                                rwsb, R._stream())), reps)
+    groups = int(g.item())
+    ops["reduce_by_key_19M_rows"] = _op_line(total, total * 16 + groups * 16, ms, peak, groups=groups)
+    del jout, okeys, osum, ocnt
+
+    # three-relation inputs: sort of F (60M x 16 B) on fk, set ops on the key lists
+    d1, d2, f, l5, l2 = PL.gen_three_relation(device=dev)
+    fs = torch.empty_like(f)
+    fsort = R.Sorter(f.shape[0], 16, 0, 64, 96, device=dev)
+    ms = _time_ms(lambda: fsort(fs, flags=R.SORT_SKIP_TRIVIAL), 3, setup=lambda: fs.copy_(f))
+    nf = f.shape[0]
+    ops["sort_tuples_60M_16B_on_fk"] = _op_line(nf, nf * 16 + 3 * 2 * nf * 16, ms, peak, passes=3,
+                                               note="fk < 2^24: the top digit is constant and skipped")
+    for name, op, a, b in (("intersect_5M_2M_u32", R.SET_INTERSECTION, l5, l2),
+                           ("difference_5M_2M_u32", R.SET_DIFFERENCE, l5, l2),
+                           ("union_5M_2M_u32", R.SET_UNION, l5, l2)):
+        outp = torch.empty(a.shape[0] + b.shape[0], dtype=torch.int32, device=dev)
+        c = torch.zeros(1, dtype=torch.int64, device=dev)
+        swsb = R.LIB.rfx_set_op_workspace(op, a.shape[0], b.shape[0], 4)
+        sws = R._empty_bytes(swsb, dev)
+
+        def run(op=op, a=a, b=b, outp=outp, c=c, sws=sws, swsb=swsb):
+            R.check("set", R.LIB.rfx_set_op(op, R._ptr(outp), R._ptr(c), R._ptr(a), a.shape[0], R._ptr(b), b.shape[0],
+                                            4, R._ptr(sws), swsb, R._stream()))
+        ms = _time_ms(run, reps)
+        no = int(c.item())
+        ops[name] = _op_line(a.shape[0] + b.shape[0], (a.shape[0] + b.shape[0] + no) * 4, ms, peak, out=no,
+                             note="inputs fit L2")
+    # the two pipelines end to end (host reads sizes back between steps, as the reference)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    PL.join_aggregate(r, s)
+    torch.cuda.synchronize()
+    ms = (time.perf_counter() - t0) * 1e3
+    ops["pipeline_join_aggregate_1Mx4M"] = {"tuples": nl + nr, "ms": ms, "tuples_per_s": (nl + nr) / (ms / 1e3),
+                                            "note": "sort R, sort S, join, reduce; wall clock incl. size reads"}
+    t0 = time.perf_counter()
+    PL.three_relation(d1, d2, f, l5, l2)
+    torch.cuda.synchronize()
+    ms = (time.perf_counter() - t0) * 1e3
+    nin = d1.shape[0] + d2.shape[0] + f.shape[0]
+    ops["pipeline_three_relation_76M"] = {"tuples": nin, "ms": ms, "tuples_per_s": nin / (ms / 1e3),
+                                          "note": "selects, sort, 2 joins, set ops, sort of F, reduce; wall clock"}
+    return ops
+
+
 # ------------------------------------------------------------------------------ our arm
 def main_ours(args):
     import torch
@@ -366,7 +512,8 @@ def main_ours(args):
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
     e2e_ms = float(te[0]) / args.e2e_steps
     d2h = (plan.G * (2 + plan.nsum) + 1) * 8
-    del host, dev_in
+    del host
+    dev_in_keep = dev_in
 
     ok = R.device_status() == R.OK
     result = None
@@ -407,6 +554,9 @@ def main_ours(args):
             "clocks": clocks,
             "parity": "ok" if ok else "MISMATCH",
         }
+        if world == 1 and not args.no_operators:
+            del dev_in_keep
+            result["operators"] = operator_benchmarks(dev, rows, peak)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

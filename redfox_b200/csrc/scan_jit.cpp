@@ -340,44 +340,73 @@ std::string gen_compact(const ScanProgram& p, int mode, uint32_t wout, int rows_
     s << "}\n";
   }
   s << "return keep;\n}\n";
+  if (mode == 2) {
+    s << R"RFX(
+extern "C" __global__ void __launch_bounds__(NT) rfx_plan_compact(
+    const u8* __restrict__ in, u64 n, u8* __restrict__ out, u64* __restrict__ d_count,
+    u64* __restrict__ status, u32* __restrict__ tile_counter, u32* err) {
+  const u32 t = threadIdx.x;
+  const u64 num_tiles = (n + TILE - 1) / TILE;
+  for (u64 tile = blockIdx.x; tile < num_tiles; tile += gridDim.x) {
+    u64 L[IPT][NL];
+    u64 O[IPT][NO];
+#pragma unroll
+    for (int j = 0; j < IPT; ++j) {
+      const u64 i = tile * TILE + (u64)j * NT + t;
+      if (i < n) { )RFX" << load_code(p.in_bytes, "L[j]", "i") << R"RFX( }
+    }
+#pragma unroll
+    for (int j = 0; j < IPT; ++j) {
+      const u64 i = tile * TILE + (u64)j * NT + t;
+      if (i < n) { process(L[j], O[j]); )RFX" << store_code(wout, "O[j]", "i") << R"RFX( }
+    }
+  }
+}
+)RFX";
+    return s.str();
+  }
+  // Compaction.  The next tile is claimed and its rows are requested before this tile's
+  // barriers and look-back, so HBM reads stay in flight while warp 0 walks predecessors.
+  // Claiming ahead cannot deadlock: a tile's look-back waits only on lower tiles.
   s << R"RFX(
 extern "C" __global__ void __launch_bounds__(NT) rfx_plan_compact(
     const u8* __restrict__ in, u64 n, u8* __restrict__ out, u64* __restrict__ d_count,
     u64* __restrict__ status, u32* __restrict__ tile_counter, u32* err) {
   __shared__ u32 s_cnt[IPT][NT / 32];
   __shared__ u64 s_prefix;
-  __shared__ u32 s_tile;
+  __shared__ u32 s_tile[2];
   const u32 t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const u64 num_tiles = (n + TILE - 1) / TILE;
-  for (u64 iter = 0;; ++iter) {
-)RFX";
-  if (mode == 2) {
-    s << "    const u64 tile = iter * gridDim.x + blockIdx.x;\n    if (tile >= num_tiles) break;\n";
-  } else {
-    s << "    if (t == 0) s_tile = atomicAdd(tile_counter, 1u);\n    __syncthreads();\n    const u64 tile = s_tile;\n"
-         "    if (tile >= num_tiles) break;\n";
+  if (t == 0) s_tile[0] = atomicAdd(tile_counter, 1u);
+  __syncthreads();
+  u64 tile = s_tile[0];
+  u64 L[IPT][NL];
+#pragma unroll
+  for (int j = 0; j < IPT; ++j) {
+    const u64 i = tile * TILE + (u64)j * NT + t;
+    if (tile < num_tiles && i < n) { )RFX" << load_code(p.in_bytes, "L[j]", "i") << R"RFX( }
   }
-  s << "    u64 L[IPT][NL];\n    u64 O[IPT][NO];\n    bool sel[IPT];\n";
-  s << "#pragma unroll\n    for (int j = 0; j < IPT; ++j) {\n      const u64 i = tile * TILE + (u64)j * NT + t;\n"
-       "      if (i < n) { "
-    << load_code(p.in_bytes, "L[j]", "i") << " }\n    }\n";
-  s << "#pragma unroll\n    for (int j = 0; j < IPT; ++j) {\n      const u64 i = tile * TILE + (u64)j * NT + t;\n"
-       "      sel[j] = i < n ? process(L[j], O[j]) : false;\n    }\n";
-  if (mode == 2) {
-    s << "#pragma unroll\n    for (int j = 0; j < IPT; ++j) {\n      const u64 i = tile * TILE + (u64)j * NT + t;\n"
-         "      if (i < n) { "
-      << store_code(wout, "O[j]", "i") << " }\n    }\n  }\n}\n";
-    return s.str();
-  }
-  s << R"RFX(
+  for (u32 it = 0; tile < num_tiles; ++it) {
+    if (t == 0) s_tile[(it + 1) & 1] = atomicAdd(tile_counter, 1u);
+    u64 O[IPT][NO];
+    bool sel[IPT];
     u32 rank[IPT];
 #pragma unroll
     for (int j = 0; j < IPT; ++j) {
+      const u64 i = tile * TILE + (u64)j * NT + t;
+      sel[j] = i < n ? process(L[j], O[j]) : false;
       const unsigned b = __ballot_sync(0xffffffffu, sel[j]);
       rank[j] = __popc(b & ((1u << lane) - 1u));
       if (lane == 0) s_cnt[j][warp] = __popc(b);
     }
     __syncthreads();
+    const u64 next = s_tile[(it + 1) & 1];
+    u64 Ln[IPT][NL];
+#pragma unroll
+    for (int j = 0; j < IPT; ++j) {
+      const u64 i = next * TILE + (u64)j * NT + t;
+      if (next < num_tiles && i < n) { )RFX" << load_code(p.in_bytes, "Ln[j]", "i") << R"RFX( }
+    }
     if (warp == 0) {
       const u32 NC = IPT * (NT / 32);
       u32 c = lane < NC ? s_cnt[lane / (NT / 32)][lane % (NT / 32)] : 0u;
@@ -400,13 +429,14 @@ extern "C" __global__ void __launch_bounds__(NT) rfx_plan_compact(
     for (int j = 0; j < IPT; ++j) {
       if (sel[j]) {
         const u64 pos = base + s_cnt[j][warp] + rank[j];
-        if (pos < n) {
-)RFX";
-  s << "          " << store_code(wout, "O[j]", "pos") << "\n";
-  s << R"RFX(
-        }
+        if (pos < n) { )RFX" << store_code(wout, "O[j]", "pos") << R"RFX( }
       }
     }
+#pragma unroll
+    for (int j = 0; j < IPT; ++j)
+#pragma unroll
+      for (int l = 0; l < NL; ++l) L[j][l] = Ln[j][l];
+    tile = next;
     __syncthreads();
   }
 }
@@ -439,7 +469,12 @@ rfx_status jit_aggregate(const ScanProgram& p, const void* in, uint64_t n, unsig
 rfx_status jit_compact(const ScanProgram& p, int mode, const void* in, uint64_t n, void* out, uint64_t* d_count,
                        uint64_t* status, uint32_t* counter, uint32_t* err, cudaStream_t stream, uint64_t tile_rows) {
   const uint32_t wout = mode == 0 ? p.in_bytes : p.out_bytes;
-  const int ipt = (int)(tile_rows / kJitThreads);
+  // rows per thread by row width (registers hold the current and the prefetched tile);
+  // tiles are never smaller than the workspace's tile_rows, so its status array suffices
+  const uint32_t wmax = p.in_bytes > wout ? p.in_bytes : wout;
+  int ipt = wmax >= 32 ? 2 : wmax >= 16 ? 4 : 8;
+  if ((uint64_t)ipt * kJitThreads < tile_rows) ipt = (int)(tile_rows / kJitThreads);
+  tile_rows = (uint64_t)ipt * kJitThreads;
   cudaKernel_t k;
   rfx_status st = jit_kernel(gen_compact(p, mode, wout, ipt), "rfx_plan_compact", &k);
   if (st != RFX_OK) return st;

@@ -143,12 +143,19 @@ sort_histogram_kernel(const uint8_t* __restrict__ keys, uint64_t n, uint32_t beg
     const bool valid = i < n;
     Elem<K> e;
     if (valid) e = load_elem<K>(keys, i);
+    const unsigned vmask = __ballot_sync(0xffffffffu, valid);
     for (uint32_t p = 0; p < passes; ++p) {
       const uint32_t shift = begin_bit + 8 * p;
       const uint32_t w = end_bit - shift < 8 ? end_bit - shift : 8;
       const uint32_t d = valid ? (elem_bits<K>(e, shift) & ((1u << w) - 1)) : kRadix;
-      const unsigned peers = __match_any_sync(0xffffffffu, d);
-      if (valid && (peers & ((1u << lane) - 1)) == 0) atomicAdd(&h[p][d], (uint32_t)__popc(peers));
+      // a digit shared by the whole warp (constant high digits) is one add, not 32
+      // conflicting atomics; otherwise plain shared atomics
+      const uint32_t d0 = __shfl_sync(0xffffffffu, d, 0);
+      if (__all_sync(0xffffffffu, d == d0 || !valid) && vmask == 0xffffffffu) {
+        if (lane == 0) atomicAdd(&h[p][d0], 32u);
+      } else if (valid) {
+        atomicAdd(&h[p][d], 1u);
+      }
     }
   }
   __syncthreads();
@@ -185,8 +192,10 @@ sort_histogram_kernel(const uint8_t* __restrict__ keys, uint64_t n, uint32_t beg
 }
 
 // ------------------------------------------------------------------ onesweep pass
+// Two blocks per SM: the per-item keys and ranks must fit 128 registers, so digits and
+// tile positions are recomputed where needed instead of being kept live.
 template <int K, int V>
-__global__ void __launch_bounds__(kSortThreads)
+__global__ void __launch_bounds__(kSortThreads, 2)
 sort_pass_kernel(const SortPassArgs a) {
   using T = SortTuning<K, V>;
   constexpr int IPT = T::IPT;
@@ -212,7 +221,7 @@ sort_pass_kernel(const SortPassArgs a) {
     // warp w owns items [w*32*IPT, (w+1)*32*IPT) of the tile, item j of lane l at j*32+l
     const uint32_t wbase = warp * 32 * IPT;
     Elem<K> key[IPT];
-    uint32_t dig[IPT], rank[IPT];
+    uint32_t rank[IPT];
 #pragma unroll
     for (int j = 0; j < IPT; ++j) {
       const uint32_t li = wbase + j * 32 + lane;
@@ -223,7 +232,6 @@ sort_pass_kernel(const SortPassArgs a) {
       const uint32_t li = wbase + j * 32 + lane;
       const bool valid = li < tcount;
       const uint32_t d = valid ? (elem_bits<K>(key[j], a.shift) & a.mask) : kRadix + 1;
-      dig[j] = d;
       const unsigned peers = __match_any_sync(0xffffffffu, d);
       const unsigned lower = peers & ((1u << lane) - 1);
       uint32_t base = 0;
@@ -287,14 +295,12 @@ sort_pass_kernel(const SortPassArgs a) {
     __syncthreads();
     // keys: scatter into tile order in shared memory, then out in digit runs
     Elem<K>* skeys = reinterpret_cast<Elem<K>*>(sbuf);
-    uint32_t lpos[IPT];
 #pragma unroll
     for (int j = 0; j < IPT; ++j) {
       const uint32_t li = wbase + j * 32 + lane;
       if (li < tcount) {
-        const uint32_t d = dig[j];
-        lpos[j] = s_local[d] + whist[warp][d] + rank[j];
-        skeys[lpos[j]] = key[j];
+        const uint32_t d = elem_bits<K>(key[j], a.shift) & a.mask;
+        skeys[s_local[d] + whist[warp][d] + rank[j]] = key[j];
       }
     }
     __syncthreads();
@@ -311,7 +317,10 @@ sort_pass_kernel(const SortPassArgs a) {
 #pragma unroll
       for (int j = 0; j < IPT; ++j) {
         const uint32_t li = wbase + j * 32 + lane;
-        if (li < tcount) svals[lpos[j]] = load_elem<V>(a.vals_in, tbase + li);
+        if (li < tcount) {
+          const uint32_t d = elem_bits<K>(key[j], a.shift) & a.mask;
+          svals[s_local[d] + whist[warp][d] + rank[j]] = load_elem<V>(a.vals_in, tbase + li);
+        }
       }
       __syncthreads();
       for (uint32_t i = t; i < tcount; i += kSortThreads) {

@@ -9,6 +9,8 @@
 // skewed key (one left row with millions of matches) spreads over all blocks.
 #pragma once
 
+#include <type_traits>
+
 #include "search.cuh"
 #include "sort_kernels.cuh"
 
@@ -56,11 +58,35 @@ __device__ __forceinline__ uint64_t block_exclusive_u64(uint64_t x, uint64_t* s_
   return wpre + incl - x;
 }
 
+// Right-side keys a block's left keys can match, staged in shared memory: u64 keys for
+// containers up to 8 bytes, u128 above.
+template <int RE>
+struct Window {
+  typedef typename std::conditional<(RE <= 8), uint64_t, u128>::type T;
+  static constexpr int CAP = RE <= 8 ? 4096 : 2048;
+};
+
+template <typename T>
+__device__ __forceinline__ uint32_t smem_bound(const T* w, uint32_t n, u128 k, bool strict) {
+  uint32_t lo = 0, hi = n;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    const u128 m = (u128)w[mid];
+    if (strict ? (m <= k) : (m < k)) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
 template <int LE, int RE>
 __global__ void __launch_bounds__(kJoinThreads) find_bounds_kernel(const FindBoundsArgs a) {
+  typedef typename Window<RE>::T WT;
+  constexpr int CAP = Window<RE>::CAP;
   __shared__ uint64_t s_warp[kJoinThreads / 32];
   __shared__ uint64_t s_prefix;
   __shared__ uint32_t s_tile;
+  __shared__ uint64_t s_lo, s_hi;
+  __shared__ WT s_win[CAP];
   const uint32_t t = threadIdx.x;
   const uint64_t num_tiles = (a.nl + kFbTile - 1) / kFbTile;
   const KeyView<LE> L{a.left, a.nl, a.lshift};
@@ -70,7 +96,18 @@ __global__ void __launch_bounds__(kJoinThreads) find_bounds_kernel(const FindBou
     __syncthreads();
     const uint64_t tile = s_tile;
     if (tile >= num_tiles) break;
-    const uint64_t first = tile * kFbTile + (uint64_t)t * kFbIPT;
+    const uint64_t tfirst = tile * kFbTile;
+    const uint64_t tlast = min(tfirst + kFbTile, a.nl) - 1;
+    // the window of right keys between the tile's smallest and largest left key
+    if (t == 0) s_lo = bsearch<RE>(R, L.key(tfirst), 0, a.nr, false);
+    if (t == 32) s_hi = bsearch<RE>(R, L.key(tlast), 0, a.nr, true);
+    __syncthreads();
+    const uint64_t wlo = s_lo, wn = s_hi > s_lo ? s_hi - s_lo : 0;
+    const bool staged = wn <= (uint64_t)CAP;
+    if (staged)
+      for (uint64_t x = t; x < wn; x += kJoinThreads) s_win[x] = (WT)R.key(wlo + x);
+    __syncthreads();
+    const uint64_t first = tfirst + (uint64_t)t * kFbIPT;
     uint64_t lo[kFbIPT], cnt[kFbIPT];
     uint64_t tsum = 0;
     u128 prevk = 0;
@@ -86,8 +123,14 @@ __global__ void __launch_bounds__(kJoinThreads) find_bounds_kernel(const FindBou
         lo[j] = plo;
         cnt[j] = phi - plo;
       } else {
-        const uint64_t l = j == 0 ? bsearch<RE>(R, k, 0, a.nr, false) : gallop<RE>(R, k, phi, false);
-        const uint64_t h = gallop<RE>(R, k, l, true);
+        uint64_t l, h;
+        if (staged) {
+          l = wlo + smem_bound<WT>(s_win, (uint32_t)wn, k, false);
+          h = wlo + smem_bound<WT>(s_win, (uint32_t)wn, k, true);
+        } else {
+          l = j == 0 ? bsearch<RE>(R, k, 0, a.nr, false) : gallop<RE>(R, k, phi, false);
+          h = gallop<RE>(R, k, l, true);
+        }
         lo[j] = l;
         cnt[j] = h - l;
         plo = l;
@@ -130,33 +173,67 @@ __global__ void __launch_bounds__(kJoinThreads) find_bounds_kernel(const FindBou
 
 // ------------------------------------------------------------------ index expansion
 // Output k belongs to the last left row i with scan[i] <= k; right row lb[i] + k - scan[i].
+// A block stages the scan entries covering its outputs in shared memory.
+constexpr int kExpCap = 2048 + 1;
+
+__device__ __forceinline__ uint64_t owner_scan(const int32_t* scan, uint64_t n, uint64_t k) {
+  uint64_t lo = 0, hi = n;
+  while (lo < hi) {
+    const uint64_t mid = lo + ((hi - lo) >> 1);
+    if ((uint64_t)(uint32_t)__ldg(scan + mid) <= k) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo - 1;
+}
+
 __global__ void __launch_bounds__(kJoinThreads)
 join_expand_kernel(int32_t* __restrict__ li, int32_t* __restrict__ ri, uint64_t nout_max, const uint64_t* d_nout,
                    const int32_t* __restrict__ lb, const int32_t* __restrict__ scan, uint64_t nl) {
+  __shared__ uint32_t s_scan[kExpCap];
+  __shared__ int32_t s_lb[kExpCap];
+  __shared__ uint64_t s_i0, s_i1;
+  const uint32_t t = threadIdx.x;
   uint64_t nout = nout_max;
   if (d_nout) nout = min(nout, *d_nout);
-  const uint64_t stride = (uint64_t)gridDim.x * kExpTile;
-  for (uint64_t base = (uint64_t)blockIdx.x * kExpTile + (uint64_t)threadIdx.x * kExpVT; base < nout; base += stride) {
-    // last i with (u32)scan[i] <= base
-    uint64_t lo = 0, hi = nl;
-    while (lo < hi) {
-      const uint64_t mid = lo + ((hi - lo) >> 1);
-      if ((uint64_t)(uint32_t)__ldg(scan + mid) <= base) lo = mid + 1;
-      else hi = mid;
+  for (uint64_t k0 = (uint64_t)blockIdx.x * kExpTile; k0 < nout; k0 += (uint64_t)gridDim.x * kExpTile) {
+    const uint64_t k1 = min(k0 + (uint64_t)kExpTile, nout);
+    if (t == 0) s_i0 = owner_scan(scan, nl, k0);
+    if (t == 32) s_i1 = owner_scan(scan, nl, k1 - 1);
+    __syncthreads();
+    const uint64_t i0 = s_i0, span = s_i1 - i0 + 1;
+    const bool staged = span <= (uint64_t)kExpCap;
+    if (staged) {
+      for (uint64_t x = t; x < span; x += kJoinThreads) {
+        s_scan[x] = (uint32_t)__ldg(scan + i0 + x);
+        s_lb[x] = __ldg(lb + i0 + x);
+      }
     }
-    uint64_t i = lo - 1;
-    uint64_t nxt = i + 1 < nl ? (uint64_t)(uint32_t)__ldg(scan + i + 1) : ~0ull;
-#pragma unroll
+    __syncthreads();
     for (int v = 0; v < kExpVT; ++v) {
-      const uint64_t k = base + v;
-      if (k >= nout) break;
-      while (k >= nxt) {
-        ++i;
-        nxt = i + 1 < nl ? (uint64_t)(uint32_t)__ldg(scan + i + 1) : ~0ull;
+      const uint64_t k = k0 + (uint64_t)v * kJoinThreads + t;
+      if (k >= k1) break;
+      uint64_t i;
+      uint32_t sc;
+      int32_t l;
+      if (staged) {
+        uint32_t lo = 0, hi = (uint32_t)span;
+        while (lo < hi) {
+          const uint32_t mid = (lo + hi) >> 1;
+          if (s_scan[mid] <= k) lo = mid + 1;
+          else hi = mid;
+        }
+        i = i0 + lo - 1;
+        sc = s_scan[lo - 1];
+        l = s_lb[lo - 1];
+      } else {
+        i = owner_scan(scan, nl, k);
+        sc = (uint32_t)__ldg(scan + i);
+        l = __ldg(lb + i);
       }
       li[k] = (int32_t)i;
-      ri[k] = __ldg(lb + i) + (int32_t)(k - (uint64_t)(uint32_t)__ldg(scan + i));
+      ri[k] = l + (int32_t)(k - (uint64_t)sc);
     }
+    __syncthreads();
   }
 }
 
@@ -256,39 +333,67 @@ struct TupleJoinArgs {
   uint64_t cap;
 };
 
+// Offsets of the left rows that cover a block's outputs, staged in shared memory.
+constexpr int kStageCap = kExpTile + 1;
+
+// Last index i in [0, n) with off[i] <= k (off non-decreasing, off[0] = 0).
+__device__ __forceinline__ uint64_t owner_global(const uint64_t* off, uint64_t n, uint64_t k) {
+  uint64_t lo = 0, hi = n;
+  while (lo < hi) {
+    const uint64_t mid = lo + ((hi - lo) >> 1);
+    if (__ldg(off + mid) <= k) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo - 1;
+}
+
 template <int LE, int RE, int OE>
 __global__ void __launch_bounds__(kJoinThreads) tuple_join_kernel(const TupleJoinArgs a) {
+  __shared__ uint64_t s_off[kStageCap + 1];
+  __shared__ uint64_t s_lb[kStageCap];
+  __shared__ uint64_t s_i0, s_i1;
+  const uint32_t t = threadIdx.x;
   const uint64_t total = a.off64[a.nl];
   const uint64_t nout = total < a.cap ? total : a.cap;
   const u128 rmask = a.rv_bits >= 128 ? ~(u128)0 : (((u128)1 << a.rv_bits) - 1);
-  const uint64_t stride = (uint64_t)gridDim.x * kExpTile;
-  for (uint64_t base = (uint64_t)blockIdx.x * kExpTile + (uint64_t)threadIdx.x * kExpVT; base < nout; base += stride) {
-    uint64_t lo = 0, hi = a.nl;
-    while (lo < hi) {
-      const uint64_t mid = lo + ((hi - lo) >> 1);
-      if (__ldg(a.off64 + mid) <= base) lo = mid + 1;
-      else hi = mid;
+  for (uint64_t k0 = (uint64_t)blockIdx.x * kExpTile; k0 < nout; k0 += (uint64_t)gridDim.x * kExpTile) {
+    const uint64_t k1 = min(k0 + (uint64_t)kExpTile, nout);
+    if (t == 0) s_i0 = owner_global(a.off64, a.nl, k0);
+    if (t == 32) s_i1 = owner_global(a.off64, a.nl, k1 - 1);
+    __syncthreads();
+    const uint64_t i0 = s_i0, span = s_i1 - i0 + 1;
+    const bool staged = span <= (uint64_t)kStageCap;
+    if (staged) {
+      for (uint64_t x = t; x <= span; x += kJoinThreads) s_off[x] = __ldg(a.off64 + i0 + x);
+      for (uint64_t x = t; x < span; x += kJoinThreads) s_lb[x] = __ldg(a.lb64 + i0 + x);
     }
-    uint64_t i = lo - 1;
-    uint64_t nxt = __ldg(a.off64 + i + 1);
-    u128 lrow = load_u128<LE>(a.left, i) << a.rv_bits;
-    uint64_t lbi = __ldg(a.lb64 + i), offi = __ldg(a.off64 + i);
-#pragma unroll
+    __syncthreads();
+    // outputs striped over the block: consecutive threads write consecutive rows
+#pragma unroll 2
     for (int v = 0; v < kExpVT; ++v) {
-      const uint64_t k = base + v;
-      if (k >= nout) break;
-      if (k >= nxt) {
-        while (k >= nxt) {
-          ++i;
-          nxt = __ldg(a.off64 + i + 1);
+      const uint64_t k = k0 + (uint64_t)v * kJoinThreads + t;
+      if (k >= k1) break;
+      uint64_t i, offi, lbi;
+      if (staged) {
+        uint32_t lo = 0, hi = (uint32_t)span;
+        while (lo < hi) {
+          const uint32_t mid = (lo + hi) >> 1;
+          if (s_off[mid] <= k) lo = mid + 1;
+          else hi = mid;
         }
-        lrow = load_u128<LE>(a.left, i) << a.rv_bits;
-        lbi = __ldg(a.lb64 + i);
+        i = i0 + lo - 1;
+        offi = s_off[lo - 1];
+        lbi = s_lb[lo - 1];
+      } else {
+        i = owner_global(a.off64, a.nl, k);
         offi = __ldg(a.off64 + i);
+        lbi = __ldg(a.lb64 + i);
       }
       const uint64_t j = lbi + (k - offi);
-      if (j < a.nr) store_u128<OE>(a.out, k, lrow | (load_u128<RE>(a.right, j) & rmask));  // guards a timed-out scan
+      if (j < a.nr)  // guards a timed-out scan
+        store_u128<OE>(a.out, k, (load_u128<LE>(a.left, i) << a.rv_bits) | (load_u128<RE>(a.right, j) & rmask));
     }
+    __syncthreads();
   }
 }
 

@@ -13,8 +13,6 @@ struct RedLayout {
   uint32_t* counter;
   SegPair* agg;
   SegPair* inc;
-  SegPair* cagg;
-  SegPair* cinc;
   size_t clear_bytes;
   size_t total;
 };
@@ -29,8 +27,6 @@ RedLayout red_layout(void* ws, uint64_t n) {
   c.used = L.clear_bytes;
   L.agg = c.take<SegPair>(tiles);
   L.inc = c.take<SegPair>(tiles);
-  L.cagg = c.take<SegPair>(tiles);
-  L.cinc = c.take<SegPair>(tiles);
   L.total = align_up(c.used, 256);
   return L;
 }
@@ -62,8 +58,6 @@ rfx_status run_reduce(ReduceArgs& a, uint32_t kb, int vk, void* ws, size_t ws_by
   a.tile_counter = L.counter;
   a.agg = L.agg;
   a.inc = L.inc;
-  a.cagg = L.cagg;
-  a.cinc = L.cinc;
   a.err = device_error_word();
   if (!a.err) return RFX_ERR_CUDA;
   RFX_CUDA_TRY(cudaMemsetAsync(ws, 0, L.clear_bytes, s));
@@ -233,8 +227,6 @@ extern "C" rfx_status rfx_reduce_tuples(const void* rows, uint64_t n, const uint
   a.r.tile_counter = L.counter;
   a.r.agg = L.agg;
   a.r.inc = L.inc;
-  a.r.cagg = L.cagg;
-  a.r.cinc = L.cinc;
   a.r.err = err;
   a.key_shift = key_shift;
   a.val_shift = value_shift;

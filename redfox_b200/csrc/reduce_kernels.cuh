@@ -24,10 +24,11 @@ enum ValKind : int { VAL_NONE = 0, VAL_U32 = 1, VAL_I64 = 2 };
 struct SegPair {
   uint64_t f;  // heads
   uint64_t v;  // running total since the last head (u64 arithmetic, wraps)
+  uint64_t h;  // position of the last head (max); a run's length at its last item i is i - h + 1
 };
 
 __device__ __forceinline__ SegPair seg_op(const SegPair& a, const SegPair& b) {
-  return SegPair{a.f + b.f, b.f ? b.v : a.v + b.v};
+  return SegPair{a.f + b.f, b.f ? b.v : a.v + b.v, a.h > b.h ? a.h : b.h};
 }
 
 template <int K>
@@ -53,47 +54,36 @@ struct ReduceArgs {
   uint32_t* flags;       // [tiles] look-back flags
   SegPair* agg;          // [tiles]
   SegPair* inc;          // [tiles]
-  SegPair* cagg;         // [tiles] counts (when out_counts)
-  SegPair* cinc;
   uint32_t* tile_counter;
   uint32_t* err;
 };
 
-// Warp 0: exclusive prefix of this tile (values and run counts) by look-back.
-__device__ __forceinline__ void seg_lookback(const ReduceArgs& a, uint32_t tile, SegPair agg, SegPair cagg,
-                                             SegPair* pre, SegPair* cpre) {
+// Warp 0: exclusive prefix of this tile by look-back (flags released after payloads).
+__device__ __forceinline__ void seg_lookback(const ReduceArgs& a, uint32_t tile, SegPair agg, SegPair* pre) {
   const uint32_t lane = threadIdx.x & 31;
   if (tile == 0) {
     if (lane == 0) {
       a.inc[0] = agg;
-      a.cinc[0] = cagg;
       st_release_u32(&a.flags[0], 2u);
     }
-    *pre = SegPair{0, 0};
-    *cpre = SegPair{0, 0};
+    *pre = SegPair{0, 0, 0};
     return;
   }
   if (lane == 0) {
     a.agg[tile] = agg;
-    a.cagg[tile] = cagg;
     st_release_u32(&a.flags[tile], 1u);
   }
-  SegPair run{0, 0}, crun{0, 0};
+  SegPair run{0, 0, 0};
   int64_t base = (int64_t)tile - 1;
   uint32_t spins = 0;
   while (true) {
     const int64_t idx = base - (int64_t)lane;
     uint32_t fl = 2u;
-    SegPair e{0, 0}, ce{0, 0};
+    SegPair e{0, 0, 0};
     if (idx >= 0) {
       fl = ld_acquire_u32(&a.flags[idx]);
-      if (fl == 1u) {
-        e = a.agg[idx];
-        ce = a.cagg[idx];
-      } else if (fl == 2u) {
-        e = a.inc[idx];
-        ce = a.cinc[idx];
-      }
+      if (fl == 1u) e = a.agg[idx];
+      else if (fl == 2u) e = a.inc[idx];
     }
     const unsigned not_ready = __ballot_sync(0xffffffffu, fl == 0u);
     const unsigned inc = __ballot_sync(0xffffffffu, fl == 2u);
@@ -110,29 +100,23 @@ __device__ __forceinline__ void seg_lookback(const ReduceArgs& a, uint32_t tile,
     // fold lanes 0 (nearest) .. last usable (farthest) in sequence order
     const unsigned heads = __ballot_sync(0xffffffffu, in && e.f > 0);
     const unsigned vcut = heads ? ((heads & (0u - heads)) << 1) - 1 : upto;
-    uint64_t f = in ? e.f : 0, v = ((vcut & upto) >> lane) & 1u ? e.v : 0;
-    const unsigned cheads = __ballot_sync(0xffffffffu, in && ce.f > 0);
-    const unsigned ccut = cheads ? ((cheads & (0u - cheads)) << 1) - 1 : upto;
-    uint64_t cf = in ? ce.f : 0, cv = ((ccut & upto) >> lane) & 1u ? ce.v : 0;
+    uint64_t f = in ? e.f : 0, v = ((vcut & upto) >> lane) & 1u ? e.v : 0, h = in ? e.h : 0;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       f += __shfl_xor_sync(0xffffffffu, f, o);
       v += __shfl_xor_sync(0xffffffffu, v, o);
-      cf += __shfl_xor_sync(0xffffffffu, cf, o);
-      cv += __shfl_xor_sync(0xffffffffu, cv, o);
+      const uint64_t ho = __shfl_xor_sync(0xffffffffu, h, o);
+      h = h > ho ? h : ho;
     }
-    run = seg_op(SegPair{f, v}, run);  // the window is older than what is folded so far
-    crun = seg_op(SegPair{cf, cv}, crun);
+    run = seg_op(SegPair{f, v, h}, run);  // the window is older than what is folded so far
     if (inc) break;
     base -= 32;
   }
   if (lane == 0) {
     a.inc[tile] = seg_op(run, agg);
-    a.cinc[tile] = seg_op(crun, cagg);
     st_release_u32(&a.flags[tile], 2u);
   }
   *pre = run;
-  *cpre = crun;
 }
 
 // Block-wide exclusive scan with the segmented operator.
@@ -145,27 +129,29 @@ __device__ __forceinline__ SegPair block_seg_exclusive(SegPair x, SegPair* s_war
     SegPair y;
     y.f = __shfl_up_sync(0xffffffffu, incl.f, o);
     y.v = __shfl_up_sync(0xffffffffu, incl.v, o);
+    y.h = __shfl_up_sync(0xffffffffu, incl.h, o);
     if (lane >= (uint32_t)o) incl = seg_op(y, incl);
   }
   if (lane == 31) s_warp[warp] = incl;
   __syncthreads();
-  SegPair wpre{0, 0};
+  SegPair wpre{0, 0, 0};
   for (uint32_t w = 0; w < warp; ++w) wpre = seg_op(wpre, s_warp[w]);
-  SegPair tot{0, 0};
+  SegPair tot{0, 0, 0};
   for (uint32_t w = 0; w < NT / 32; ++w) tot = seg_op(tot, s_warp[w]);
   *total = tot;
   SegPair ex;
   ex.f = __shfl_up_sync(0xffffffffu, incl.f, 1);
   ex.v = __shfl_up_sync(0xffffffffu, incl.v, 1);
-  if (lane == 0) ex = SegPair{0, 0};
+  ex.h = __shfl_up_sync(0xffffffffu, incl.h, 1);
+  if (lane == 0) ex = SegPair{0, 0, 0};
   return seg_op(wpre, ex);
 }
 
 template <int K, int VK>
-__global__ void __launch_bounds__(kRedThreads)
+__global__ void __launch_bounds__(kRedThreads, 3)
 reduce_by_key_kernel(const ReduceArgs a) {
-  __shared__ SegPair s_warp[kRedThreads / 32], s_cwarp[kRedThreads / 32];
-  __shared__ SegPair s_pre, s_cpre;
+  __shared__ SegPair s_warp[kRedThreads / 32];
+  __shared__ SegPair s_pre;
   __shared__ uint32_t s_tile;
   const uint32_t t = threadIdx.x, warp = t >> 5;
   uint64_t n = a.n_max;
@@ -220,22 +206,19 @@ reduce_by_key_kernel(const ReduceArgs a) {
       }
     }
     // thread aggregates
-    SegPair tp{0, 0}, tc{0, 0};
+    SegPair tp{0, 0, 0};
 #pragma unroll
     for (int j = 0; j < kRedIPT; ++j) {
       if (!valid[j]) continue;
-      tp = seg_op(tp, SegPair{head[j] ? 1ull : 0ull, val[j]});
-      tc = seg_op(tc, SegPair{head[j] ? 1ull : 0ull, 1ull});
+      tp = seg_op(tp, SegPair{head[j] ? 1ull : 0ull, val[j], head[j] ? first + j : 0ull});
     }
-    SegPair btot, bctot;
+    SegPair btot;
     SegPair ex = block_seg_exclusive<kRedThreads>(tp, s_warp, &btot);
-    SegPair cex = block_seg_exclusive<kRedThreads>(tc, s_cwarp, &bctot);
     if (warp == 0) {
-      SegPair pre, cpre;
-      seg_lookback(a, (uint32_t)tile, btot, bctot, &pre, &cpre);
+      SegPair pre;
+      seg_lookback(a, (uint32_t)tile, btot, &pre);
       if (t == 0) {
         s_pre = pre;
-        s_cpre = cpre;
         if (tile == num_tiles - 1) {
           const uint64_t groups = pre.f + btot.f;
           *a.d_groups = groups;
@@ -245,12 +228,11 @@ reduce_by_key_kernel(const ReduceArgs a) {
       }
     }
     __syncthreads();
-    SegPair run = seg_op(s_pre, ex), crun = seg_op(s_cpre, cex);
+    SegPair run = seg_op(s_pre, ex);
 #pragma unroll
     for (int j = 0; j < kRedIPT; ++j) {
       if (!valid[j]) continue;
-      run = seg_op(run, SegPair{head[j] ? 1ull : 0ull, val[j]});
-      crun = seg_op(crun, SegPair{head[j] ? 1ull : 0ull, 1ull});
+      run = seg_op(run, SegPair{head[j] ? 1ull : 0ull, val[j], head[j] ? first + j : 0ull});
       if (tail[j]) {
         const uint64_t g = run.f - 1;
         if (g < n) {
@@ -259,7 +241,7 @@ reduce_by_key_kernel(const ReduceArgs a) {
             if constexpr (VK == VAL_I64) reinterpret_cast<int64_t*>(a.out_vals)[g] = (int64_t)run.v;
             else reinterpret_cast<uint32_t*>(a.out_vals)[g] = (uint32_t)run.v;
           }
-          if (a.out_counts) a.out_counts[g] = (uint32_t)crun.v;
+          if (a.out_counts) a.out_counts[g] = (uint32_t)(first + j - run.h + 1);
         }
       }
     }
@@ -287,11 +269,11 @@ struct TupleReduceArgs {
 };
 
 template <int RB, int OKB>
-__global__ void __launch_bounds__(kRedThreads)
+__global__ void __launch_bounds__(kRedThreads, 3)
 reduce_tuples_kernel(const TupleReduceArgs ta) {
   const ReduceArgs& a = ta.r;
-  __shared__ SegPair s_warp[kRedThreads / 32], s_cwarp[kRedThreads / 32];
-  __shared__ SegPair s_pre, s_cpre;
+  __shared__ SegPair s_warp[kRedThreads / 32];
+  __shared__ SegPair s_pre;
   __shared__ uint32_t s_tile;
   const uint32_t t = threadIdx.x, warp = t >> 5;
   uint64_t n = a.n_max;
@@ -335,38 +317,34 @@ reduce_tuples_kernel(const TupleReduceArgs ta) {
       else if (j + 1 < kRedIPT) tail[j] = head[j + 1];
       else tail[j] = key[j] != (load_u128<RB>(a.keys, i + 1) >> ta.key_shift);
     }
-    SegPair tp{0, 0}, tc{0, 0};
+    SegPair tp{0, 0, 0};
 #pragma unroll
     for (int j = 0; j < kRedIPT; ++j) {
       if (!valid[j]) continue;
-      tp = seg_op(tp, SegPair{head[j] ? 1ull : 0ull, val[j]});
-      tc = seg_op(tc, SegPair{head[j] ? 1ull : 0ull, 1ull});
+      tp = seg_op(tp, SegPair{head[j] ? 1ull : 0ull, val[j], head[j] ? first + j : 0ull});
     }
-    SegPair btot, bctot;
+    SegPair btot;
     SegPair ex = block_seg_exclusive<kRedThreads>(tp, s_warp, &btot);
-    SegPair cex = block_seg_exclusive<kRedThreads>(tc, s_cwarp, &bctot);
     if (warp == 0) {
-      SegPair pre, cpre;
-      seg_lookback(a, (uint32_t)tile, btot, bctot, &pre, &cpre);
+      SegPair pre;
+      seg_lookback(a, (uint32_t)tile, btot, &pre);
       if (t == 0) {
         s_pre = pre;
-        s_cpre = cpre;
         if (tile == num_tiles - 1) *a.d_groups = pre.f + btot.f;
       }
     }
     __syncthreads();
-    SegPair run = seg_op(s_pre, ex), crun = seg_op(s_cpre, cex);
+    SegPair run = seg_op(s_pre, ex);
 #pragma unroll
     for (int j = 0; j < kRedIPT; ++j) {
       if (!valid[j]) continue;
-      run = seg_op(run, SegPair{head[j] ? 1ull : 0ull, val[j]});
-      crun = seg_op(crun, SegPair{head[j] ? 1ull : 0ull, 1ull});
+      run = seg_op(run, SegPair{head[j] ? 1ull : 0ull, val[j], head[j] ? first + j : 0ull});
       if (tail[j]) {
         const uint64_t g = run.f - 1;
         if (g < n) {
           store_u128<OKB>(a.out_keys, g, key[j]);
           if (a.out_vals) reinterpret_cast<int64_t*>(a.out_vals)[g] = (int64_t)run.v;
-          if (a.out_counts) a.out_counts[g] = (uint32_t)crun.v;
+          if (a.out_counts) a.out_counts[g] = (uint32_t)(first + j - run.h + 1);
         }
       }
     }

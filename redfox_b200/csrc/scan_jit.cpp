@@ -408,15 +408,20 @@ extern "C" __global__ void __launch_bounds__(NT) rfx_plan_compact(
       if (next < num_tiles && i < n) { )RFX" << load_code(p.in_bytes, "Ln[j]", "i") << R"RFX( }
     }
     if (warp == 0) {
+      // exclusive scan of the IPT x warps counts, 32 at a time
       const u32 NC = IPT * (NT / 32);
-      u32 c = lane < NC ? s_cnt[lane / (NT / 32)][lane % (NT / 32)] : 0u;
-      u32 incl = c;
-      for (int o = 1; o < 32; o <<= 1) {
-        const u32 v = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= (u32)o) incl += v;
+      u32 total = 0;
+      for (u32 c0 = 0; c0 < NC; c0 += 32) {
+        const u32 idx = c0 + lane;
+        const u32 c = idx < NC ? s_cnt[idx / (NT / 32)][idx % (NT / 32)] : 0u;
+        u32 incl = c;
+        for (int o = 1; o < 32; o <<= 1) {
+          const u32 v = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= (u32)o) incl += v;
+        }
+        if (idx < NC) s_cnt[idx / (NT / 32)][idx % (NT / 32)] = total + incl - c;
+        total += __shfl_sync(0xffffffffu, incl, 31);
       }
-      const u32 total = __shfl_sync(0xffffffffu, incl, 31);
-      if (lane < NC) s_cnt[lane / (NT / 32)][lane % (NT / 32)] = incl - c;
       const u64 prefix = lookback(status, (u32)tile, total, err);
       if (lane == 0) {
         s_prefix = prefix;

@@ -11,6 +11,8 @@
 //   * unique keeps the first of each run, in place.
 #pragma once
 
+#include <type_traits>
+
 #include "search.cuh"
 
 namespace rfx {
@@ -55,8 +57,34 @@ __device__ __forceinline__ uint64_t block_exclusive_u32(uint32_t x, uint32_t* s_
   return wpre + incl - x;
 }
 
+template <typename T>
+__device__ __forceinline__ uint32_t smem_lower(const T* w, uint32_t n, u128 k) {
+  uint32_t lo = 0, hi = n;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if ((u128)w[mid] < k) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+template <typename T>
+__device__ __forceinline__ uint32_t smem_lower_strict(const T* w, uint32_t n, u128 k) {
+  uint32_t lo = 0, hi = n;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if ((u128)w[mid] <= k) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
 template <int E, int MODE>
 __global__ void __launch_bounds__(kSetThreads) set_filter_kernel(const SetFilterArgs p) {
+  typedef typename std::conditional<(E <= 8), uint64_t, u128>::type WT;
+  constexpr int WCAP = E <= 8 ? 2048 : 1024;
+  __shared__ WT s_a[MODE == KEEP_HEADS ? 1 : kSetTile];
+  __shared__ WT s_b[MODE == KEEP_HEADS ? 1 : WCAP];
+  __shared__ uint64_t s_rs0, s_blo, s_bhi;
   __shared__ uint32_t s_warp[kSetThreads / 32];
   __shared__ uint64_t s_prefix;
   __shared__ uint32_t s_tile;
@@ -93,19 +121,35 @@ __global__ void __launch_bounds__(kSetThreads) set_filter_kernel(const SetFilter
         keep[j] = i == 0 || v[j] != (j == 0 ? before : v[j - 1]);
       }
     } else {
-      uint64_t run_start = 0, blo = 0, bhi = 0;
-      u128 prevk = 0;
+      // the tile's own elements and the window of B values they can equal, in shared
+      // memory; the run containing the tile's first element may start in an earlier tile
+      const uint64_t tfirst = tile * kSetTile;
+      const uint64_t tn = min((uint64_t)kSetTile, p.na - tfirst);
+      if (t == 0) s_rs0 = bsearch<E>(A, A.key(tfirst), 0, tfirst, false);
+      if (t == 32) s_blo = bsearch<E>(B, A.key(tfirst), 0, p.nb, false);
+      if (t == 64) s_bhi = bsearch<E>(B, A.key(tfirst + tn - 1), 0, p.nb, true);
+      for (uint32_t x = t; x < tn; x += kSetThreads) s_a[x] = (WT)A.key(tfirst + x);
+      __syncthreads();
+      const uint64_t blo0 = s_blo, bn = s_bhi > s_blo ? s_bhi - s_blo : 0;
+      const bool staged = bn <= (uint64_t)WCAP;
+      if (staged)
+        for (uint64_t x = t; x < bn; x += kSetThreads) s_b[x] = (WT)B.key(blo0 + x);
+      __syncthreads();
+      const u128 v0 = (u128)s_a[0];
 #pragma unroll
       for (int j = 0; j < kSetIPT; ++j) {
         const uint64_t i = first + j;
         if (i >= p.na) continue;
-        if (j == 0 || v[j] != prevk) {
-          run_start = (j > 0) ? i : bsearch<E>(A, v[j], 0, i, false);
-          blo = (j == 0) ? bsearch<E>(B, v[j], 0, p.nb, false) : gallop<E>(B, v[j], bhi, false);
-          bhi = gallop<E>(B, v[j], blo, true);
-          prevk = v[j];
+        const uint32_t li = (uint32_t)(i - tfirst);
+        const uint64_t run_start = v[j] == v0 ? s_rs0 : tfirst + smem_lower(s_a, li, v[j]);
+        uint64_t nbeq;
+        if (staged) {
+          nbeq = smem_lower_strict(s_b, (uint32_t)bn, v[j]) - smem_lower(s_b, (uint32_t)bn, v[j]);
+        } else {
+          const uint64_t l = bsearch<E>(B, v[j], 0, p.nb, false);
+          nbeq = gallop<E>(B, v[j], l, true) - l;
         }
-        const uint64_t rank = i - run_start, nbeq = bhi - blo;
+        const uint64_t rank = i - run_start;
         keep[j] = MODE == KEEP_MATCHED ? rank < nbeq : rank >= nbeq;
       }
     }

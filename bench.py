@@ -46,6 +46,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=5)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-operators", action="store_true")
+    ap.add_argument("--batched-queries", type=int, default=512,
+                    help="queries of the batched join+aggregate comparison (0: skip it)")
     return ap.parse_args()
 
 
@@ -408,6 +410,78 @@ def operator_benchmarks(dev, fact_rows, peak, reps=5):
     return ops
 
 
+def batched_benchmark(dev, nq, reps=3):
+    """512 (nq) independent sort + join + aggregate queries, |R|, |S| log-uniform in
+    [1e4, 8e6]: one plain launch sequence per query, back to back, against the batched plan
+    (all queries folded into one relation by query id, each operator one persistent launch)
+    replayed as one CUDA graph.  All queries are submitted at once, so a query's latency is
+    the time from the start of the batch to its own completion."""
+    import torch
+
+    from redfox_b200 import batch as B
+
+    sizes = B.query_sizes(nq)
+    r_all, s_all, r_off, s_off = B.gen_batch(sizes, device=dev)
+    rows = int(r_all.shape[0] + s_all.shape[0])
+    for q in range(min(nq, 4)):                         # warm-up (allocator, kernels)
+        B.plain_query(r_all, s_all, r_off, s_off, q)
+    torch.cuda.synchronize()
+    done = [torch.cuda.Event(enable_timing=True) for _ in range(nq)]
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev0.record()
+    plain = []
+    for q in range(nq):
+        res = B.plain_query(r_all, s_all, r_off, s_off, q)
+        done[q].record()
+        if q < 8:
+            plain.append(tuple(x.clone() if torch.is_tensor(x) else x for x in res))
+    torch.cuda.synchronize()
+    plain_done = [ev0.elapsed_time(e) for e in done]
+    plain_ms = plain_done[-1]
+    service = [plain_done[0]] + [b - a for a, b in zip(plain_done, plain_done[1:])]
+    torch.cuda.empty_cache()
+
+    plan = B.BatchedPlan(r_all, s_all)
+    plan.capture()
+    plan.replay()
+    torch.cuda.synchronize()
+    ms = []
+    for _ in range(reps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        plan.replay()
+        e1.record()
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    batch_ms = statistics.median(ms)
+    keys, sums, counts, total = plan.result()
+    per = B.split_by_query(keys, sums, counts, min(nq, 8))
+    ok = all(torch.equal(per[q][0], plain[q][0] & B.QUERY_KEY_MASK) and torch.equal(per[q][1], plain[q][1])
+             and torch.equal(per[q][2], plain[q][2]) for q in range(len(plain)))
+    nbytes = sum(t.numel() * t.element_size() for t in (plan.r, plan.s, plan.out, plan.keys, plan.sums, plan.counts))
+    del plan
+    torch.cuda.empty_cache()
+
+    def pct(v, p):
+        v = sorted(v)
+        return v[min(len(v) - 1, int(round(p / 100 * (len(v) - 1))))]
+
+    return {
+        "queries": nq, "rows": rows, "join_rows": total,
+        "plain": {"ms": plain_ms, "queries_per_s": nq / (plain_ms / 1e3),
+                  "latency_ms_p50": pct(plain_done, 50), "latency_ms_p99": pct(plain_done, 99),
+                  "service_ms_p50": pct(service, 50), "service_ms_p99": pct(service, 99)},
+        "batched_graph": {"ms": batch_ms, "queries_per_s": nq / (batch_ms / 1e3),
+                          "latency_ms_p50": batch_ms, "latency_ms_p99": batch_ms, "replays": ms,
+                          "plan_buffers_gb": nbytes / 1e9},
+        "speedup_queries_per_s": plain_ms / batch_ms,
+        "parity_first_8_queries": "ok" if ok else "MISMATCH",
+        "note": "same kernels both ways; plain reads each query's join and group counts back to size its "
+                "outputs, batched sizes them once and replays the captured plan",
+    }
+
+
 # ------------------------------------------------------------------------------ our arm
 def main_ours(args):
     import torch
@@ -560,6 +634,10 @@ def main_ours(args):
         if world == 1 and not args.no_operators:
             del dev_in_keep
             result["operators"] = operator_benchmarks(dev, rows, peak)
+        if world == 1 and args.batched_queries > 0:
+            del rows
+            torch.cuda.empty_cache()
+            result["batched"] = batched_benchmark(dev, args.batched_queries)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

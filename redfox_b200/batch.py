@@ -1,0 +1,155 @@
+"""Batched execution: many independent sort + join + aggregate queries in one launch per
+operator, and the whole batched plan captured as a CUDA graph.
+
+The queries are folded into one relation by putting the query id above each query's key
+(key' = q << 21 | key, the per-query key domains |R|/4 being below 2^21): sorting on the
+composite key sorts every query, the sort-merge join on it joins every query with itself
+only, and the reduce-by-key groups per (query, key).  Tiles of all queries then share the
+persistent kernels' dynamic tile queues (the device work queue), so a 10^4-row query and an
+8 * 10^6-row query occupy the GPU alike, and per-query launch and read-back costs vanish.
+
+Per query (the batched-form workload): |R|, |S| log-uniform in [1e4, 8e6]; R keys uniform
+over [0, |R|/4); S.fk drawn uniformly from R's keys; amounts uniform in [100, 10^7).
+"""
+import math
+
+from . import plans as PL
+from . import rfx as R
+from .workloads import SEED_BASE
+
+C3_QUERIES = 512
+C3_MIN, C3_MAX = 10_000, 8_000_000
+C3_SEED = SEED_BASE + 3
+QUERY_SHIFT = 21               # query id bits start here in the 32-bit key field
+QUERY_KEY_MASK = (1 << QUERY_SHIFT) - 1
+
+
+def _mix64(x):
+    m = (1 << 64) - 1
+    x = ((x ^ (x >> 30)) * 0xBF58476D1CE4E5B9) & m
+    x = ((x ^ (x >> 27)) * 0x94D049BB133111EB) & m
+    return x ^ (x >> 31)
+
+
+def _rand(seed, stream, idx):
+    """The SplitMix64 stream every generator here uses (same as the device generator)."""
+    m = (1 << 64) - 1
+    base = _mix64(seed ^ ((stream * 0xD1B54A32D192ED03) & m))
+    return _mix64((base + (idx + 1) * 0x9E3779B97F4A7C15) & m)
+
+
+def query_sizes(nq=C3_QUERIES, lo=C3_MIN, hi=C3_MAX, seed=C3_SEED):
+    """(|R|, |S|) per query, log-uniform in [lo, hi]."""
+    out = []
+    for q in range(nq):
+        u = [(_rand(seed, s, q) >> 11) * 2.0 ** -53 for s in (0, 1)]
+        out.append(tuple(int(round(math.exp(math.log(lo) + x * (math.log(hi) - math.log(lo))))) for x in u))
+    return out
+
+
+def gen_batch(sizes, device="cuda"):
+    """Concatenated R (8-byte rows) and S (16-byte rows) of all queries with the query id in
+    the key's high bits, plus per-query row offsets."""
+    import torch
+    nr_tot = sum(s[0] for s in sizes)
+    ns_tot = sum(s[1] for s in sizes)
+    r_all = torch.empty((nr_tot, 8), dtype=torch.uint8, device=device)
+    s_all = torch.empty((ns_tot, 16), dtype=torch.uint8, device=device)
+    r_off, s_off = [0], [0]
+    for q, (nr, ns) in enumerate(sizes):
+        dom = max(1, nr // 4)
+        rq = R.gen_uniform_rows(nr, [32, 32], C3_SEED + 16 + 2 * q, [0, 0], [dom, 1 << 32], device=device)
+        sq = R.gen_uniform_rows(ns, [32, 64], C3_SEED + 17 + 2 * q, [0, 100], [nr, 10_000_000], device=device)
+        r64 = rq.view(torch.int64).view(nr)
+        keys = (r64 >> 32) & 0xFFFFFFFF
+        s64 = sq.view(torch.int64).view(ns, 2)
+        s64[:, 1] = keys[s64[:, 1]] | (q << QUERY_SHIFT)
+        r64 |= (q << QUERY_SHIFT) << 32
+        r_all[r_off[-1]:r_off[-1] + nr] = rq
+        s_all[s_off[-1]:s_off[-1] + ns] = sq
+        r_off.append(r_off[-1] + nr)
+        s_off.append(s_off[-1] + ns)
+    return r_all, s_all, r_off, s_off
+
+
+class BatchedPlan:
+    """The join + aggregate plan over the folded relations, with every buffer allocated up
+    front so that the plan can be captured in a CUDA graph and replayed.  The join output
+    capacity comes from one eager count of the same inputs."""
+
+    def __init__(self, r_all, s_all):
+        import torch
+        dev = r_all.device
+        self.r_in, self.s_in = r_all, s_all
+        self.nr, self.ns = r_all.shape[0], s_all.shape[0]
+        self.r = torch.empty_like(r_all)
+        self.s = torch.empty_like(s_all)
+        self.rsort = R.Sorter(self.nr, 8, 0, 32, 64, device=dev)
+        self.ssort = R.Sorter(self.ns, 16, 0, 64, 96, device=dev)
+        self.tj = R.TupleJoin(self.nr, device=dev)
+        # size the join output with one eager pass
+        self.r.copy_(r_all)
+        self.s.copy_(s_all)
+        self.rsort(self.r)
+        self.ssort(self.s)
+        dummy = torch.empty((1, 16), dtype=torch.uint8, device=dev)
+        self.tj(dummy, 0, self.r, 32, self.s, 64)
+        self.cap = int(self.tj.count.item())
+        self.out = torch.empty((max(1, self.cap), 16), dtype=torch.uint8, device=dev)
+        # one group per distinct (query, key) of R at most
+        g = max(1, self.nr)
+        self.keys = torch.empty(g, dtype=torch.int32, device=dev)
+        self.sums = torch.empty(g, dtype=torch.int64, device=dev)
+        self.counts = torch.empty(g, dtype=torch.int32, device=dev)
+        self.groups = torch.zeros(1, dtype=torch.int64, device=dev)
+        self.rwsb = R.LIB.rfx_reduce_by_key_workspace(self.cap)
+        self.rws = R._empty_bytes(self.rwsb, dev)
+        self.graph = None
+
+    def run(self, stream=None):
+        """Enqueue the whole plan (no host synchronisation)."""
+        self.r.copy_(self.r_in)
+        self.s.copy_(self.s_in)
+        self.rsort(self.r, stream=stream)
+        self.ssort(self.s, stream=stream)
+        self.tj(self.out, self.cap, self.r, 32, self.s, 64, stream=stream)
+        R.check("rfx_reduce_tuples", R.LIB.rfx_reduce_tuples(
+            R._ptr(self.out), self.cap, R._ptr(self.tj.count), 16, 96, 0, 64, R._ptr(self.keys), 4,
+            R._ptr(self.sums), R._ptr(self.counts), R._ptr(self.groups), R._ptr(self.rws), self.rwsb,
+            R._stream(stream)))
+
+    def capture(self):
+        """Capture run() in a CUDA graph (after one eager run has warmed every kernel up)."""
+        import torch
+        self.run()
+        torch.cuda.synchronize()
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph, stream=s):
+            self.run(stream=s)
+        torch.cuda.synchronize()
+
+    def replay(self):
+        self.graph.replay()
+
+    def result(self):
+        g = int(self.groups.item())
+        return self.keys[:g], self.sums[:g], self.counts[:g], int(self.tj.count.item())
+
+
+def split_by_query(keys, sums, counts, nq):
+    """Batched groups -> per-query (keys, sums, counts) with the query bits removed."""
+    import torch
+    q = (keys.to(torch.int64) >> QUERY_SHIFT)
+    bounds = torch.searchsorted(q, torch.arange(nq + 1, device=keys.device))
+    out = []
+    for i in range(nq):
+        a, b = int(bounds[i]), int(bounds[i + 1])
+        out.append((keys[a:b] & QUERY_KEY_MASK, sums[a:b], counts[a:b]))
+    return out
+
+
+def plain_query(r_all, s_all, r_off, s_off, q, stream=None):
+    """Query q alone through the plain plan (one launch sequence, sizes read back)."""
+    return PL.join_aggregate(r_all[r_off[q]:r_off[q + 1]], s_all[s_off[q]:s_off[q + 1]], stream=stream)

@@ -365,29 +365,28 @@ extern "C" __global__ void __launch_bounds__(NT) rfx_plan_compact(
 )RFX";
     return s.str();
   }
-  // Compaction.  The next tile is claimed and its rows are requested before this tile's
-  // barriers and look-back, so HBM reads stay in flight while warp 0 walks predecessors.
-  // Claiming ahead cannot deadlock: a tile's look-back waits only on lower tiles.
+  // Compaction: tiles claimed in order from a counter, kept rows ranked by warp ballots
+  // and a block scan, tile offsets by decoupled look-back.
   s << R"RFX(
 extern "C" __global__ void __launch_bounds__(NT) rfx_plan_compact(
     const u8* __restrict__ in, u64 n, u8* __restrict__ out, u64* __restrict__ d_count,
     u64* __restrict__ status, u32* __restrict__ tile_counter, u32* err) {
   __shared__ u32 s_cnt[IPT][NT / 32];
   __shared__ u64 s_prefix;
-  __shared__ u32 s_tile[2];
+  __shared__ u32 s_tile;
   const u32 t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const u64 num_tiles = (n + TILE - 1) / TILE;
-  if (t == 0) s_tile[0] = atomicAdd(tile_counter, 1u);
-  __syncthreads();
-  u64 tile = s_tile[0];
-  u64 L[IPT][NL];
+  while (true) {
+    if (t == 0) s_tile = atomicAdd(tile_counter, 1u);
+    __syncthreads();
+    const u64 tile = s_tile;
+    if (tile >= num_tiles) break;
+    u64 L[IPT][NL];
 #pragma unroll
-  for (int j = 0; j < IPT; ++j) {
-    const u64 i = tile * TILE + (u64)j * NT + t;
-    if (tile < num_tiles && i < n) { )RFX" << load_code(p.in_bytes, "L[j]", "i") << R"RFX( }
-  }
-  for (u32 it = 0; tile < num_tiles; ++it) {
-    if (t == 0) s_tile[(it + 1) & 1] = atomicAdd(tile_counter, 1u);
+    for (int j = 0; j < IPT; ++j) {
+      const u64 i = tile * TILE + (u64)j * NT + t;
+      if (i < n) { )RFX" << load_code(p.in_bytes, "L[j]", "i") << R"RFX( }
+    }
     u64 O[IPT][NO];
     bool sel[IPT];
     u32 rank[IPT];
@@ -400,13 +399,6 @@ extern "C" __global__ void __launch_bounds__(NT) rfx_plan_compact(
       if (lane == 0) s_cnt[j][warp] = __popc(b);
     }
     __syncthreads();
-    const u64 next = s_tile[(it + 1) & 1];
-    u64 Ln[IPT][NL];
-#pragma unroll
-    for (int j = 0; j < IPT; ++j) {
-      const u64 i = next * TILE + (u64)j * NT + t;
-      if (next < num_tiles && i < n) { )RFX" << load_code(p.in_bytes, "Ln[j]", "i") << R"RFX( }
-    }
     if (warp == 0) {
       // exclusive scan of the IPT x warps counts, 32 at a time
       const u32 NC = IPT * (NT / 32);
@@ -437,11 +429,6 @@ extern "C" __global__ void __launch_bounds__(NT) rfx_plan_compact(
         if (pos < n) { )RFX" << store_code(wout, "O[j]", "pos") << R"RFX( }
       }
     }
-#pragma unroll
-    for (int j = 0; j < IPT; ++j)
-#pragma unroll
-      for (int l = 0; l < NL; ++l) L[j][l] = Ln[j][l];
-    tile = next;
     __syncthreads();
   }
 }
@@ -474,7 +461,7 @@ rfx_status jit_aggregate(const ScanProgram& p, const void* in, uint64_t n, unsig
 rfx_status jit_compact(const ScanProgram& p, int mode, const void* in, uint64_t n, void* out, uint64_t* d_count,
                        uint64_t* status, uint32_t* counter, uint32_t* err, cudaStream_t stream, uint64_t tile_rows) {
   const uint32_t wout = mode == 0 ? p.in_bytes : p.out_bytes;
-  // rows per thread by row width (registers hold the current and the prefetched tile);
+  // rows per thread by row width (registers hold one tile's rows);
   // tiles are never smaller than the workspace's tile_rows, so its status array suffices
   const uint32_t wmax = p.in_bytes > wout ? p.in_bytes : wout;
   int ipt = wmax >= 32 ? 2 : wmax >= 16 ? 4 : 8;

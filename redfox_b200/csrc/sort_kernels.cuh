@@ -273,58 +273,31 @@ sort_pass_kernel(const SortPassArgs a) {
       uint32_t wpre = 0;
       for (uint32_t w = 0; w < warp; ++w) wpre += s_scan[w];
       s_local[t] = wpre + incl - count;
-      st_relaxed_u32(a.status + tile * kRadix + t, (tile == 0 ? kSFlagInc : kSFlagAgg) | count);
-      // Warp-parallel decoupled look-back: warp w resolves digits 32w..32w+31, eight at a
-      // time; lane l reads predecessor tile (base - l) for all eight digits at once, so a
-      // window of 32 predecessors costs one round trip instead of 32 dependent loads.
-      uint32_t prefix = 0;  // lane k: the prefix of digit 32 * warp + k
-      if (tile > 0) {
+      // decoupled look-back for this digit: predecessors usually hold an inclusive
+      // prefix within one or two steps, so each thread walks its own digit
+      uint32_t* st = a.status + tile * kRadix + t;
+      uint32_t prefix = 0;
+      if (tile == 0) {
+        st_relaxed_u32(st, kSFlagInc | count);
+      } else {
+        st_relaxed_u32(st, kSFlagAgg | count);
+        int64_t p = (int64_t)tile - 1;
         uint32_t spins = 0;
-        bool gave_up = false;
-        for (uint32_t g = 0; g < 4 && !gave_up; ++g) {
-          const uint32_t d0 = 32 * warp + 8 * g;  // first digit of this group
-          uint32_t unresolved = 0xffu;
-          int64_t base = (int64_t)tile - 1;
-          while (unresolved && !gave_up) {
-            uint32_t pending = unresolved;  // digits not yet folded from this window
-            while (pending) {
-              const int64_t pt = base - (int64_t)lane;
-              uint32_t w[8];
-              if (pt >= 0) {
-                const uint32_t* src = a.status + (uint64_t)pt * kRadix + d0;
-                const uint4 x = ld_volatile_v4(src), y = ld_volatile_v4(src + 4);
-                w[0] = x.x; w[1] = x.y; w[2] = x.z; w[3] = x.w;
-                w[4] = y.x; w[5] = y.y; w[6] = y.z; w[7] = y.w;
-              } else {
-#pragma unroll
-                for (int k = 0; k < 8; ++k) w[k] = kSFlagInc;  // before tile 0: prefix 0
-              }
-#pragma unroll
-              for (int k = 0; k < 8; ++k) {
-                if (!((pending >> k) & 1u)) continue;
-                const uint32_t flag = w[k] & ~kSValMask;
-                const unsigned not_ready = __ballot_sync(0xffffffffu, flag == 0);
-                const unsigned inc = __ballot_sync(0xffffffffu, flag == kSFlagInc);
-                const unsigned upto = inc ? ((inc & (0u - inc)) << 1) - 1 : 0xffffffffu;
-                if (not_ready & upto) continue;  // a predecessor is still ranking: re-read
-                const uint32_t v = __reduce_add_sync(0xffffffffu, ((upto >> lane) & 1u) ? (w[k] & kSValMask) : 0u);
-                if (lane == 8 * g + k) prefix += v;
-                pending &= ~(1u << k);
-                if (inc) unresolved &= ~(1u << k);
-              }
-              if (pending) {
-                if (++spins > kSpinLimit) {
-                  raise_error(a.err, kErrTimeout);
-                  gave_up = true;
-                  break;
-                }
-                __nanosleep(spins < 64 ? 20 : 100);
-              }
+        while (p >= 0) {
+          const uint32_t s = ld_relaxed_u32(a.status + (uint64_t)p * kRadix + t);
+          if ((s & ~kSValMask) == 0) {
+            if (++spins > kSpinLimit) {
+              raise_error(a.err, kErrTimeout);
+              break;
             }
-            base -= 32;
+            __nanosleep(spins < 64 ? 20 : 100);
+            continue;
           }
+          prefix += s & kSValMask;
+          if (s & kSFlagInc) break;
+          --p;
         }
-        st_relaxed_u32(a.status + tile * kRadix + t, kSFlagInc | ((prefix + count) & kSValMask));
+        st_relaxed_u32(st, kSFlagInc | ((prefix + count) & kSValMask));
       }
       s_global[t] = a.gexcl[t] + prefix;
     }

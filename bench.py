@@ -264,10 +264,15 @@ def main_reference(args):
 
 # ------------------------------------------------------------------------------ per operator
 def _time_ms(fn, reps, setup=None):
-    """Mean device time of fn() over `reps` calls (CUDA events on the current stream);
+    """Mean device time of fn() over `reps` calls (CUDA events on the current stream)
+    after one untimed call (first-call host set-up: tensor maps, launch attributes);
     setup() runs before each call outside the timed interval."""
     import torch
     stream = torch.cuda.current_stream()
+    if setup is not None:
+        setup()
+    fn()
+    torch.cuda.synchronize()
     total = 0.0
     for _ in range(reps):
         if setup is not None:

@@ -1,8 +1,11 @@
 // host_common.cpp -- see host_common.h.
 #include "host_common.h"
 
+#include <cstring>
 #include <mutex>
 #include <unordered_map>
+
+#include <cudaTypedefs.h>
 
 namespace rfx {
 
@@ -81,6 +84,43 @@ int persistent_grid(const void* kernel, int threads, size_t dyn_smem, uint64_t w
   uint64_t cap = (uint64_t)device_sms() * (uint64_t)per_sm;
   uint64_t g = work_blocks < cap ? work_blocks : cap;
   return (int)(g ? g : 1);
+}
+
+namespace {
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+}  // namespace
+
+bool encode_line_map(CUtensorMap* map, const void* base, uint64_t lines, uint32_t box_lines) {
+  std::memset(map, 0, sizeof(*map));
+  if (!base || lines == 0 || lines > (1ull << 31) || (reinterpret_cast<uintptr_t>(base) & 15u) || box_lines == 0 ||
+      box_lines > 256)
+    return false;
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc) return false;
+  cuuint64_t dims[2] = {128, lines};
+  cuuint64_t strides[1] = {128};
+  cuuint32_t box[2] = {128, box_lines};
+  cuuint32_t estr[2] = {1, 1};
+  const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void*>(base), dims, strides, box, estr,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    std::memset(map, 0, sizeof(*map));
+    return false;
+  }
+  return true;
 }
 
 }  // namespace rfx

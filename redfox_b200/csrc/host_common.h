@@ -4,6 +4,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "rfx/rfx.h"
@@ -45,5 +46,11 @@ inline cudaStream_t as_stream(void* s) { return static_cast<cudaStream_t>(s); }
 int persistent_grid(const void* kernel, int threads, size_t dyn_smem, uint64_t work_blocks);
 // Raise a kernel's dynamic shared memory limit once.
 cudaError_t allow_smem(const void* kernel, size_t bytes);
+
+// Tensor map of `lines` 128-byte lines at `base` (a [lines][128] u8 tensor, boxes of
+// `box_lines` <= 256 lines, 128-byte swizzle) for the tile ring.  False when `base` is not 16-byte
+// aligned, `lines` is 0 or above 2^31, or the driver rejects the map; *map is then
+// zeroed and must not be used.
+bool encode_line_map(CUtensorMap* map, const void* base, uint64_t lines, uint32_t box_lines = 256);
 
 }  // namespace rfx

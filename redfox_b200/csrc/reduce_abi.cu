@@ -1,5 +1,6 @@
 // reduce_abi.cu -- C ABI of reduce-by-key / count, and the reference-compatible
 // count_* / total_64_32 entries with device-resident byte sizes (Reduce.cu).
+#include <cstdlib>
 #include <cstring>
 
 #include "host_common.h"
@@ -76,9 +77,33 @@ bool aligned_to(const void* p, uint32_t b) {
   return (reinterpret_cast<uintptr_t>(p) % (b < 16 ? b : 16)) == 0;
 }
 
+// Tiles of the TMA-staged tuple reduce: kRowRedThreads 128-byte lines; the smallest tile
+// (16-byte rows) has kRowRedThreads * 8 rows.
+constexpr int kRowRedThreads = 256;
+
+struct RowLayout {
+  SegRecord* records;
+  uint32_t* counter;
+  size_t total;
+};
+
+RowLayout row_layout(void* ws, uint64_t n, uint32_t row_bytes) {
+  const uint64_t tile_rows = (uint64_t)kRowRedThreads * kRingLineBytes / row_bytes;
+  const uint64_t tiles = (n + tile_rows - 1) / tile_rows + 1;
+  Carver c(ws);
+  RowLayout L;
+  L.records = c.take<SegRecord>(tiles);
+  L.counter = c.take<uint32_t>(1);
+  L.total = align_up(c.used, 256);
+  return L;
+}
+
 }  // namespace
 
-size_t reduce_workspace_impl(uint64_t n) { return red_layout(nullptr, n).total; }
+size_t reduce_workspace_impl(uint64_t n) {
+  const size_t a = red_layout(nullptr, n).total, b = row_layout(nullptr, n, 16).total;
+  return a > b ? a : b;
+}
 
 rfx_status reduce_impl(const void* keys, uint64_t n, const uint64_t* d_n, uint32_t kb, const void* vals, uint32_t vk,
                        void* out_keys, void* out_vals, uint32_t* out_counts, uint64_t* d_groups, void* ws,
@@ -197,6 +222,64 @@ rfx_status launch_tuples_o(uint32_t okb, TupleReduceArgs& a, cudaStream_t s) {
 }  // namespace
 }  // namespace rfx
 
+namespace rfx {
+namespace {
+// The TMA-staged form: rows 16-byte aligned; the workspace of the register-tiled form
+// (kRedTile rows per tile, 52 bytes per tile) always covers its records (32 bytes per
+// tile of at least kRedTile rows).
+template <int RB, int SHAPE>
+rfx_status launch_rows(const void* rows, uint64_t n, RowReduceArgs& a, cudaStream_t s) {
+  constexpr int NT = kRowRedThreads;
+  auto k = reduce_rows_kernel<RB, SHAPE, kRowRedStages, NT>;
+  const size_t smem = (size_t)kRowRedStages * NT * kRingLineBytes + 1024;
+  RFX_CUDA_TRY(allow_smem((const void*)k, smem));
+  CUtensorMap map;
+  const uint64_t lines = n * RB / kRingLineBytes;
+  a.full_lines = encode_line_map(&map, rows, lines, NT) ? lines : 0;
+  const uint64_t tiles = (n * RB + NT * kRingLineBytes - 1) / (NT * kRingLineBytes);
+  const int grid = persistent_grid((const void*)k, NT, smem, tiles ? tiles : 1);
+  k<<<grid, NT, smem, s>>>(map, a);
+  RFX_CUDA_TRY(cudaGetLastError());
+  return RFX_OK;
+}
+
+rfx_status reduce_rows_staged(const void* rows, uint64_t n, const uint64_t* d_n, uint32_t row_bytes,
+                              uint32_t key_shift, uint32_t value_shift, uint64_t val_mask, void* out_keys,
+                              uint32_t out_key_bytes, int64_t* out_sums, uint32_t* out_counts, uint64_t* d_groups,
+                              void* workspace, uint32_t* err, cudaStream_t s) {
+  const RowLayout L = row_layout(workspace, n, row_bytes);
+  SegRecord* rec = L.records;
+  uint32_t* counter = L.counter;
+  RFX_CUDA_TRY(cudaMemsetAsync(workspace, 0, L.total, s));
+  RowReduceArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.rows = static_cast<const uint8_t*>(rows);
+  a.n_max = n;
+  a.d_n = d_n;
+  a.key_shift = key_shift;
+  a.val_shift = value_shift;
+  a.val_mask = val_mask;
+  a.out_key_bytes = out_key_bytes;
+  a.out_keys = static_cast<uint8_t*>(out_keys);
+  a.out_sums = out_sums;
+  a.out_counts = out_counts;
+  a.d_groups = d_groups;
+  a.records = rec;
+  a.tile_counter = counter;
+  a.err = err;
+  if (row_bytes == 16 && value_shift == 0 && val_mask == ~0ull && key_shift == 96)
+    return launch_rows<16, ROW16_K32_V64>(rows, n, a, s);
+  if (row_bytes == 16 && value_shift == 0 && val_mask == ~0ull && key_shift == 64)
+    return launch_rows<16, ROW16_K64_V64>(rows, n, a, s);
+  switch (row_bytes) {
+    case 4: return launch_rows<4, ROW_GENERIC>(rows, n, a, s);
+    case 8: return launch_rows<8, ROW_GENERIC>(rows, n, a, s);
+    default: return launch_rows<16, ROW_GENERIC>(rows, n, a, s);
+  }
+}
+}  // namespace
+}  // namespace rfx
+
 extern "C" rfx_status rfx_reduce_tuples(const void* rows, uint64_t n, const uint64_t* d_n, uint32_t row_bytes,
                                         uint32_t key_shift, uint32_t value_shift, uint32_t value_bits,
                                         void* out_keys, uint32_t out_key_bytes, int64_t* out_sums,
@@ -205,6 +288,7 @@ extern "C" rfx_status rfx_reduce_tuples(const void* rows, uint64_t n, const uint
   if (!(row_bytes == 4 || row_bytes == 8 || row_bytes == 16) || key_shift >= row_bytes * 8u || value_bits == 0 ||
       value_bits > 64 || value_shift + value_bits > row_bytes * 8u)
     return RFX_ERR_UNSUPPORTED;
+  if (!(out_key_bytes == 4 || out_key_bytes == 8 || out_key_bytes == 16)) return RFX_ERR_UNSUPPORTED;
   if (!d_groups || (n && (!rows || !out_keys))) return RFX_ERR_INVALID;
   if (n && (reinterpret_cast<uintptr_t>(rows) % row_bytes) != 0) return RFX_ERR_INVALID;
   cudaStream_t s = as_stream(stream);
@@ -212,6 +296,12 @@ extern "C" rfx_status rfx_reduce_tuples(const void* rows, uint64_t n, const uint
   if (!workspace || workspace_bytes < L.total) return RFX_ERR_WORKSPACE;
   uint32_t* err = device_error_word();
   if (!err) return RFX_ERR_CUDA;
+  const uint64_t vmask = value_bits >= 64 ? ~0ull : ((1ull << value_bits) - 1);
+  if ((reinterpret_cast<uintptr_t>(rows) & 15u) == 0 && std::getenv("RFX_REDUCE_REGS") == nullptr) {
+    if (workspace_bytes < row_layout(nullptr, n, row_bytes).total) return RFX_ERR_WORKSPACE;
+    return reduce_rows_staged(rows, n, d_n, row_bytes, key_shift, value_shift, vmask, out_keys, out_key_bytes,
+                              out_sums, out_counts, d_groups, workspace, err, s);
+  }
   RFX_CUDA_TRY(cudaMemsetAsync(workspace, 0, L.clear_bytes, s));
   TupleReduceArgs a;
   std::memset(&a, 0, sizeof(a));

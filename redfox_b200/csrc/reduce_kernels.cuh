@@ -9,9 +9,11 @@
 // output keys are the run keys in input order.
 #pragma once
 
+#include "lookback.cuh"
 #include "rfx_device.cuh"
 #include "search.cuh"
 #include "sort_kernels.cuh"
+#include "tile_ring.cuh"
 
 namespace rfx {
 
@@ -21,15 +23,11 @@ constexpr int kRedTile = kRedThreads * kRedIPT;
 
 enum ValKind : int { VAL_NONE = 0, VAL_U32 = 1, VAL_I64 = 2 };
 
-struct SegPair {
-  uint64_t f;  // heads
-  uint64_t v;  // running total since the last head (u64 arithmetic, wraps)
-  uint64_t h;  // position of the last head (max); a run's length at its last item i is i - h + 1
-};
+// (f, v, h): run heads, running total since the last head (u64 arithmetic, wraps),
+// position of the last head (max); a run's length at its last item i is i - h + 1.
+using SegPair = SegPayload;
 
-__device__ __forceinline__ SegPair seg_op(const SegPair& a, const SegPair& b) {
-  return SegPair{a.f + b.f, b.f ? b.v : a.v + b.v, a.h > b.h ? a.h : b.h};
-}
+__device__ __forceinline__ SegPair seg_op(const SegPair& a, const SegPair& b) { return lb_combine(a, b); }
 
 template <int K>
 __device__ __forceinline__ bool elem_eq(const Elem<K>& a, const Elem<K>& b) {
@@ -139,6 +137,46 @@ __device__ __forceinline__ SegPair block_seg_exclusive(SegPair x, SegPair* s_war
   SegPair tot{0, 0, 0};
   for (uint32_t w = 0; w < NT / 32; ++w) tot = seg_op(tot, s_warp[w]);
   *total = tot;
+  SegPair ex;
+  ex.f = __shfl_up_sync(0xffffffffu, incl.f, 1);
+  ex.v = __shfl_up_sync(0xffffffffu, incl.v, 1);
+  ex.h = __shfl_up_sync(0xffffffffu, incl.h, 1);
+  if (lane == 0) ex = SegPair{0, 0, 0};
+  return seg_op(wpre, ex);
+}
+
+// The same scan with the warp totals combined by a W-lane shuffle scan in every warp
+// (constant work per thread instead of a loop over the warps).
+template <int NT>
+__device__ __forceinline__ SegPair block_seg_exclusive_fast(SegPair x, SegPair* s_warp, SegPair* total) {
+  constexpr uint32_t W = NT / 32;
+  const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  SegPair incl = x;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    SegPair y;
+    y.f = __shfl_up_sync(0xffffffffu, incl.f, o);
+    y.v = __shfl_up_sync(0xffffffffu, incl.v, o);
+    y.h = __shfl_up_sync(0xffffffffu, incl.h, o);
+    if (lane >= (uint32_t)o) incl = seg_op(y, incl);
+  }
+  if (lane == 31) s_warp[warp] = incl;
+  __syncthreads();
+  SegPair wt = lane < W ? s_warp[lane] : SegPair{0, 0, 0};
+#pragma unroll
+  for (uint32_t o = 1; o < W; o <<= 1) {
+    SegPair y;
+    y.f = __shfl_up_sync(0xffffffffu, wt.f, o);
+    y.v = __shfl_up_sync(0xffffffffu, wt.v, o);
+    y.h = __shfl_up_sync(0xffffffffu, wt.h, o);
+    if (lane >= o) wt = seg_op(y, wt);
+  }
+  const uint32_t src = warp ? warp - 1 : 0;
+  SegPair wpre{__shfl_sync(0xffffffffu, wt.f, src), __shfl_sync(0xffffffffu, wt.v, src),
+               __shfl_sync(0xffffffffu, wt.h, src)};
+  if (warp == 0) wpre = SegPair{0, 0, 0};
+  *total = SegPair{__shfl_sync(0xffffffffu, wt.f, W - 1), __shfl_sync(0xffffffffu, wt.v, W - 1),
+                   __shfl_sync(0xffffffffu, wt.h, W - 1)};
   SegPair ex;
   ex.f = __shfl_up_sync(0xffffffffu, incl.f, 1);
   ex.v = __shfl_up_sync(0xffffffffu, incl.v, 1);
@@ -350,6 +388,278 @@ reduce_tuples_kernel(const TupleReduceArgs ta) {
     }
     __syncthreads();
   }
+  if (n == 0 && blockIdx.x == 0 && t == 0) *a.d_groups = 0;
+}
+
+// ------------------------------------------------------------------ TMA-staged row reduce
+// The same reduction with every 32 KB tile of rows brought into shared memory by the
+// tile ring (tile_ring.cuh) and tile prefixes resolved by the block-wide look-back
+// (lookback.cuh).  Thread t owns the 128-byte line t of the tile (128 / RB rows).
+//   pass 1: head bits of the thread's rows and the running sum since its last head give
+//           the thread's (f, v, h) = (popc(heads), sum, last head); block scan; the tile
+//           aggregate is published;
+//   pass 2: after the look-back, the rows are read again from shared memory; at each
+//           run end the group index is the carried f plus the heads so far.
+// Pipeline of one block over three stages.  Step k: claim tile k+2 and start its copy;
+// resolve the prefix of tile k (warp 0) and run its pass 2; wait for tile k+2's rows,
+// run its pass 1 and publish its aggregate.  A tile is therefore resolved one full step
+// after its aggregate was published, when its predecessors have published theirs too,
+// and only the copy (never a waiting look-back of another tile) lies between a tile's
+// claim and its aggregate: a slow look-back cannot hold up the aggregates that other
+// blocks' look-backs wait for.
+//
+// Row shapes: SHAPE 0 takes key = row >> key_shift and value = (row >> value_shift) &
+// mask at run time; SHAPE 1 / 2 are 16-byte rows with the key in the top 32 / 64 bits
+// and a 64-bit value in the low 64 bits (the join outputs the plans reduce).
+
+enum RowShape : int { ROW_GENERIC = 0, ROW16_K32_V64 = 1, ROW16_K64_V64 = 2 };
+
+template <int RB>
+struct RowWord;
+template <>
+struct RowWord<4> { typedef uint32_t T; };
+template <>
+struct RowWord<8> { typedef uint64_t T; };
+template <>
+struct RowWord<16> { typedef u128 T; };
+
+template <int RB, int SHAPE>
+struct RowAccess {
+  typedef typename RowWord<RB>::T Key;
+  __device__ __forceinline__ static void read(const uint8_t* st, uint32_t r, uint32_t ks, uint32_t vs,
+                                              uint64_t vmask, Key& k, uint64_t& v) {
+    typename RowWord<RB>::T row;
+    if constexpr (RB == 16) {
+      const uint4 w = ring_read<uint4>(st, r * 16u);
+      row = ((u128)(((uint64_t)w.w << 32) | w.z) << 64) | (((uint64_t)w.y << 32) | w.x);
+    } else {
+      row = ring_read<typename RowWord<RB>::T>(st, r * (uint32_t)RB);
+    }
+    k = row >> ks;
+    v = (uint64_t)(row >> vs) & vmask;
+  }
+  __device__ __forceinline__ static Key global_key(const uint8_t* rows, uint64_t i, uint32_t ks) {
+    return (Key)(load_u128<RB>(rows, i) >> ks);
+  }
+};
+template <>
+struct RowAccess<16, ROW16_K32_V64> {
+  typedef uint32_t Key;
+  __device__ __forceinline__ static void read(const uint8_t* st, uint32_t r, uint32_t, uint32_t, uint64_t, Key& k,
+                                              uint64_t& v) {
+    const uint4 w = ring_read<uint4>(st, r * 16u);
+    k = w.w;
+    v = ((uint64_t)w.y << 32) | w.x;
+  }
+  __device__ __forceinline__ static Key global_key(const uint8_t* rows, uint64_t i, uint32_t) {
+    return __ldg(reinterpret_cast<const uint32_t*>(rows + i * 16) + 3);
+  }
+};
+template <>
+struct RowAccess<16, ROW16_K64_V64> {
+  typedef uint64_t Key;
+  __device__ __forceinline__ static void read(const uint8_t* st, uint32_t r, uint32_t, uint32_t, uint64_t, Key& k,
+                                              uint64_t& v) {
+    const uint4 w = ring_read<uint4>(st, r * 16u);
+    k = ((uint64_t)w.w << 32) | w.z;
+    v = ((uint64_t)w.y << 32) | w.x;
+  }
+  __device__ __forceinline__ static Key global_key(const uint8_t* rows, uint64_t i, uint32_t) {
+    return __ldg(reinterpret_cast<const unsigned long long*>(rows + i * 16) + 1);
+  }
+};
+
+struct RowReduceArgs {
+  const uint8_t* rows;
+  uint64_t n_max;
+  const uint64_t* d_n;
+  uint64_t full_lines;   // 128-byte lines covered by the tensor map
+  uint32_t key_shift;
+  uint32_t val_shift;
+  uint64_t val_mask;
+  uint32_t out_key_bytes;
+  uint8_t* out_keys;
+  int64_t* out_sums;
+  uint32_t* out_counts;
+  uint64_t* d_groups;
+  SegRecord* records;
+  uint32_t* tile_counter;
+  uint32_t* err;
+};
+
+constexpr int kRowRedStages = 3;
+
+__device__ __forceinline__ uint8_t* align1024(uint8_t* p) {
+  const uint32_t a = smem_u32(p);
+  return p + ((1024u - (a & 1023u)) & 1023u);
+}
+
+template <typename K>
+__device__ __forceinline__ void store_key(uint8_t* out, uint64_t g, uint32_t okb, K k) {
+  if (okb == 4) reinterpret_cast<uint32_t*>(out)[g] = (uint32_t)k;
+  else if (okb == 8) reinterpret_cast<uint64_t*>(out)[g] = (uint64_t)k;
+  else store_u128<16>(out, g, (u128)k);
+}
+
+// State of an aggregated, not yet resolved tile.
+struct RowTileState {
+  uint64_t tile;
+  SegPair ex, btot;
+  uint32_t heads, nvalid;
+};
+
+template <int RB, int SHAPE, int S, int NT>
+__global__ void __launch_bounds__(NT, 512 / NT) reduce_rows_kernel(const __grid_constant__ CUtensorMap map,
+                                                                     const RowReduceArgs a) {
+  constexpr uint32_t TILE_BYTES = NT * kRingLineBytes;
+  constexpr uint32_t TR = TILE_BYTES / RB;
+  constexpr uint32_t IPT = TR / NT;
+  static_assert(IPT * RB == kRingLineBytes && IPT <= 32, "one 128-byte line per thread");
+  static_assert(S == 3, "stages: the tile in pass 2, the aggregated tile, the tile being copied");
+  typedef RowAccess<RB, SHAPE> RA;
+  typedef typename RA::Key Key;
+  extern __shared__ uint8_t dyn_smem[];
+  uint8_t* stages = align1024(dyn_smem);
+  __shared__ TileRing<S> ring;
+  __shared__ SegPair s_warp[NT / 32];
+  __shared__ SegPair s_pre;
+  const uint32_t t = threadIdx.x;
+  uint64_t n = a.n_max;
+  if (a.d_n) n = min(n, *a.d_n);
+  const uint64_t num_tiles = (n + TR - 1) / TR;
+  const uint64_t covered = a.full_lines * kRingLineBytes;
+  const uint32_t ks = a.key_shift, vs = a.val_shift;
+  const uint64_t vmask = a.val_mask;
+  const uint32_t tb = t * IPT;
+  if (t == 0) {
+    for (int s = 0; s < S; ++s) mbar_init(&ring.bar[s], 1);
+    mbar_fence_init();
+    if (a.full_lines) prefetch_map(&map);
+  }
+  __syncthreads();
+
+  // claim the next tile into stage s and start its copy (thread 0)
+  auto claim = [&](int s) {
+    const uint32_t tl = atomicAdd(a.tile_counter, 1u);
+    ring.tile[s] = tl;
+    if (tl >= num_tiles) return;
+    const uint64_t line0 = (uint64_t)tl * NT;
+    const bool copy = line0 < a.full_lines;
+    mbar_arrive_tx(&ring.bar[s], copy ? TILE_BYTES : 0u);
+    if (copy) tma_load_lines(stages + (size_t)s * TILE_BYTES, &map, (uint32_t)line0, &ring.bar[s]);
+  };
+  // pass 1 of the tile in stage s (its u-th use); tile = ~0 when the claim ran out or a
+  // copy timed out (ok = false)
+  bool ok = true;
+  auto pass1 = [&](int s, uint32_t u) -> RowTileState {
+    RowTileState r;
+    r.tile = ring.tile[s];
+    r.heads = 0;
+    r.nvalid = 0;
+    r.ex = r.btot = SegPair{0, 0, 0};
+    if (r.tile >= num_tiles) return r;
+    uint8_t* st = stages + (size_t)s * TILE_BYTES;
+    bool w = true;
+    if (t == 0) w = mbar_wait(&ring.bar[s], u & 1u);
+    if (!__syncthreads_and(w)) {
+      ok = false;
+      r.tile = ~0ull;
+      return r;
+    }
+    if ((r.tile + 1) * TILE_BYTES > covered) {
+      ring_fill_tail(st, a.rows, r.tile, covered, n * RB, TILE_BYTES);
+      __syncthreads();
+    }
+    const uint64_t first = r.tile * TR + tb;
+    r.nvalid = first >= n ? 0u : (uint32_t)min((uint64_t)IPT, n - first);
+    Key pk = 0;
+    uint64_t v = 0;
+    if (t > 0) RA::read(st, tb - 1, ks, vs, vmask, pk, v);
+    else if (first > 0) pk = RA::global_key(a.rows, first - 1, ks);
+    uint64_t acc = 0;
+#pragma unroll
+    for (uint32_t j = 0; j < IPT; ++j) {
+      if (j < r.nvalid) {
+        Key key;
+        RA::read(st, tb + j, ks, vs, vmask, key, v);
+        const bool h = key != pk || (j == 0 && first == 0);
+        pk = key;
+        r.heads |= (uint32_t)h << j;
+        acc = h ? v : acc + v;
+      }
+    }
+    const SegPair tp{(uint64_t)__popc(r.heads), acc, r.heads ? first + (31u - __clz(r.heads)) : 0ull};
+    r.ex = block_seg_exclusive_fast<NT>(tp, s_warp, &r.btot);
+    lb_publish(a.records, r.tile, r.btot);
+    return r;
+  };
+
+  if (t == 0) {
+    claim(0);
+    claim(1);
+  }
+  __syncthreads();
+  RowTileState cur = pass1(0, 0);
+  RowTileState nxt = pass1(1, 0);
+  for (uint32_t k = 0; ok && cur.tile < num_tiles; ++k) {
+    const int s = (int)(k % S);
+    if (t < 32) {
+      if (t == 0) {
+        // stage of tile k-1: its pass 2 ended before the barriers of the last pass 1
+        fence_proxy_async_smem();
+        claim((int)((k + 2) % S));
+      }
+      const SegPair p = warp_lookback_resolve<4>(a.records, cur.tile, cur.btot, a.err);
+      if (t == 0) s_pre = p;
+    }
+    __syncthreads();
+    const SegPair pre = s_pre;
+    if (t == 0 && cur.tile == num_tiles - 1) *a.d_groups = pre.f + cur.btot.f;
+    // pass 2: one output per run end
+    const uint8_t* st = stages + (size_t)s * TILE_BYTES;
+    const uint64_t first = cur.tile * TR + tb;
+    const SegPair carry = seg_op(pre, cur.ex);
+    const uint32_t heads = cur.heads, nvalid = cur.nvalid;
+    uint64_t acc = carry.v, hpos = carry.h;
+    Key nk = 0;
+    const bool next_valid = first + IPT < n;
+    if (next_valid) {
+      if (t + 1 < (uint32_t)NT) {
+        uint64_t dv;
+        RA::read(st, tb + IPT, ks, vs, vmask, nk, dv);
+      } else {
+        nk = RA::global_key(a.rows, first + IPT, ks);
+      }
+    }
+#pragma unroll
+    for (uint32_t j = 0; j < IPT; ++j) {
+      if (j < nvalid) {
+        Key key;
+        uint64_t v;
+        RA::read(st, tb + j, ks, vs, vmask, key, v);
+        const bool h = (heads >> j) & 1u;
+        acc = h ? v : acc + v;
+        if (h) hpos = first + j;
+        bool tail;
+        if (j + 1 < nvalid) tail = (heads >> (j + 1)) & 1u;
+        else if (j + 1 < IPT) tail = true;            // last valid row of the relation
+        else tail = !next_valid || key != nk;
+        if (tail) {
+          const uint64_t g = carry.f + (uint64_t)__popc(heads & ((2u << j) - 1u)) - 1;
+          if (g < n) {
+            store_key(a.out_keys, g, a.out_key_bytes, key);
+            if (a.out_sums) a.out_sums[g] = (int64_t)acc;
+            if (a.out_counts) a.out_counts[g] = (uint32_t)(first + j - hpos + 1);
+          }
+        }
+      }
+    }
+    __syncthreads();
+    cur = nxt;
+    const int s2 = (int)((k + 2) % S);
+    nxt = pass1(s2, (k + 2) / S);
+  }
+  if (!ok && t == 0) raise_error(a.err, kErrTimeout);
   if (n == 0 && blockIdx.x == 0 && t == 0) *a.d_groups = 0;
 }
 

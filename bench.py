@@ -48,6 +48,8 @@ def parse():
     ap.add_argument("--no-operators", action="store_true")
     ap.add_argument("--batched-queries", type=int, default=512,
                     help="queries of the batched join+aggregate comparison (0: skip it)")
+    ap.add_argument("--serving-queries", type=int, default=150,
+                    help="queries per arrival rate of the serving comparison (0: skip it)")
     return ap.parse_args()
 
 
@@ -487,6 +489,39 @@ def batched_benchmark(dev, nq, reps=3):
     }
 
 
+def serving_benchmark(dev, nq, rates=(100.0, 1000.0, 5000.0), slots=8):
+    """Parameterised select-join-aggregate queries over the resident three-relation data
+    (D1 1.5M, D2 15M, F 60M sorted on fk), Poisson arrivals at each rate: the serving loop
+    (admission against a 40 GB intermediate budget, `slots` queries in flight on their own
+    streams) against serial plain execution of the same trace (one query at a time, FIFO).
+    Latency = host time from a query's arrival to its result on the host."""
+    import torch
+
+    from redfox_b200 import serving as S
+
+    res = S.Resident(device=dev)
+    for q in S.gen_requests(6, 1e6, seed=S.SERVING_SEED + 99):       # untimed warm-up
+        S.run_alone(res, q, device=dev)
+    out = {"resident_gb": res.nbytes() / 1e9, "slots": slots, "budget_gb": S.BUDGET_BYTES / 1e9,
+           "queries_per_rate": nq, "rates": {}}
+    for rate in rates:
+        line = {}
+        for name, k in (("serial", 1), ("serving", slots)):
+            reqs = S.gen_requests(nq, rate)
+            torch.cuda.synchronize()
+            torch.cuda.reset_peak_memory_stats(dev)
+            base = torch.cuda.memory_allocated(dev)
+            sch = S.Server(res, slots=k, device=dev).serve(reqs)
+            line[name] = S.latency_summary(reqs)
+            line[name]["peak_in_flight"] = sch.peak_queries
+            line[name]["peak_intermediate_gb"] = (torch.cuda.max_memory_allocated(dev) - base) / 1e9
+        line["speedup_queries_per_s"] = line["serving"]["queries_per_s"] / line["serial"]["queries_per_s"]
+        out["rates"][str(int(rate))] = line
+    del res
+    torch.cuda.empty_cache()
+    return out
+
+
 # ------------------------------------------------------------------------------ our arm
 def main_ours(args):
     import torch
@@ -643,6 +678,9 @@ def main_ours(args):
             del rows
             torch.cuda.empty_cache()
             result["batched"] = batched_benchmark(dev, args.batched_queries)
+        if world == 1 and args.serving_queries > 0:
+            torch.cuda.empty_cache()
+            result["serving"] = serving_benchmark(dev, args.serving_queries)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()

@@ -26,6 +26,9 @@ typedef int i32;
 typedef unsigned short u16;
 typedef unsigned char u8;
 struct __align__(16) U2 { u64 x, y; };
+// comparison constants, a kernel parameter: plans that differ only in their constants
+// share one compiled kernel
+struct RfxConsts { u64 c[16]; };
 
 static __device__ __forceinline__ u64 s32(u64 v) { return (u64)(i64)(i32)(u32)v; }
 static __device__ __forceinline__ u64 u32v(u64 v) { return (u64)(u32)v; }
@@ -177,8 +180,8 @@ std::string row_body(const ScanProgram& p, const std::string& L) {
   static const char* ops[] = {"", "==", "!=", "<", "<", "<=", "<=", ">", ">", ">=", ">="};
   for (uint32_t c = 0; c < p.ncmp; ++c) {
     const CmpDesc& d = p.cmps[c];
-    std::string a = d.a_var ? "F" + std::to_string(d.a_field) : hex(d.a_const);
-    std::string b = d.b_var ? "F" + std::to_string(d.b_field) : hex(d.b_const);
+    std::string a = d.a_var ? "F" + std::to_string(d.a_field) : "K.c[" + std::to_string(2 * c) + "]";
+    std::string b = d.b_var ? "F" + std::to_string(d.b_field) : "K.c[" + std::to_string(2 * c + 1) + "]";
     s << "keep = keep && (((" << a << ") & " << hex(d.tmask) << ") " << ops[d.op] << " ((" << b << ") & "
       << hex(d.tmask) << "));\n";
   }
@@ -227,7 +230,8 @@ std::string gen_aggregate(const ScanProgram& p, bool priv) {
   s << kPreamble;
   s << "#define NT " << kJitThreads << "\n#define NL " << nl << "\n#define G " << p.ngroups_total << "\n#define NV " << nv
     << "\n#define NS " << p.nsum << "\n#define NACC (G * NV)\n";
-  s << "static __device__ __forceinline__ void process(const u64 (&L)[NL], u64* acc, u32 t, u32* err) {\n";
+  s << "static __device__ __forceinline__ void process(const u64 (&L)[NL], u64* acc, u32 t, u32* err, "
+       "const RfxConsts& K) {\n";
   s << row_body(p, "L");
   s << "if (!keep) return;\n";
   s << "u32 g = 0;\nbool ok = true;\n";
@@ -250,7 +254,7 @@ std::string gen_aggregate(const ScanProgram& p, bool priv) {
 extern "C" __global__ void __launch_bounds__(NT) rfx_plan_aggregate(
     const u8* __restrict__ in, u64 n, unsigned long long* __restrict__ gacc, u32* __restrict__ done,
     u64* __restrict__ out_keys, i64* __restrict__ out_sums, u64* __restrict__ out_counts,
-    u64* __restrict__ d_groups, u32* err) {
+    u64* __restrict__ d_groups, u32* err, const RfxConsts K) {
   extern __shared__ __align__(16) u64 acc[];
   __shared__ bool s_last;
   const u32 t = threadIdx.x, lane = t & 31, warp = t >> 5;
@@ -264,7 +268,7 @@ extern "C" __global__ void __launch_bounds__(NT) rfx_plan_aggregate(
   s << "    u64 L0[NL], L1[NL];\n    const u64 i1 = i + stride;\n";
   s << "    " << load_code(p.in_bytes, "L0", "i") << "\n";
   s << "    if (i1 < n) { " << load_code(p.in_bytes, "L1", "i1") << " }\n";
-  s << "    process(L0, acc, t, err);\n    if (i1 < n) process(L1, acc, t, err);\n  }\n  __syncthreads();\n";
+  s << "    process(L0, acc, t, err, K);\n    if (i1 < n) process(L1, acc, t, err, K);\n  }\n  __syncthreads();\n";
   if (priv)
     s << R"RFX(
   for (u32 k = warp; k < NACC; k += NT / 32) {
@@ -322,7 +326,7 @@ std::string gen_compact(const ScanProgram& p, int mode, uint32_t wout, int rows_
   s << kPreamble;
   s << "#define NT " << kJitThreads << "\n#define NL " << nl << "\n#define NO " << no << "\n#define IPT "
     << rows_per_thread << "\n#define TILE (NT * IPT)\n";
-  s << "static __device__ __forceinline__ bool process(const u64 (&L)[NL], u64 (&O)[NO]) {\n";
+  s << "static __device__ __forceinline__ bool process(const u64 (&L)[NL], u64 (&O)[NO], const RfxConsts& K) {\n";
   s << row_body(p, "L");
   if (mode == 0) {
     s << "for (int l = 0; l < NO; ++l) O[l] = L[l];\n";
@@ -344,7 +348,7 @@ std::string gen_compact(const ScanProgram& p, int mode, uint32_t wout, int rows_
     s << R"RFX(
 extern "C" __global__ void __launch_bounds__(NT) rfx_plan_compact(
     const u8* __restrict__ in, u64 n, u8* __restrict__ out, u64* __restrict__ d_count,
-    u64* __restrict__ status, u32* __restrict__ tile_counter, u32* err) {
+    u64* __restrict__ status, u32* __restrict__ tile_counter, u32* err, const RfxConsts K) {
   const u32 t = threadIdx.x;
   const u64 num_tiles = (n + TILE - 1) / TILE;
   for (u64 tile = blockIdx.x; tile < num_tiles; tile += gridDim.x) {
@@ -358,7 +362,7 @@ extern "C" __global__ void __launch_bounds__(NT) rfx_plan_compact(
 #pragma unroll
     for (int j = 0; j < IPT; ++j) {
       const u64 i = tile * TILE + (u64)j * NT + t;
-      if (i < n) { process(L[j], O[j]); )RFX" << store_code(wout, "O[j]", "i") << R"RFX( }
+      if (i < n) { process(L[j], O[j], K); )RFX" << store_code(wout, "O[j]", "i") << R"RFX( }
     }
   }
 }
@@ -370,7 +374,7 @@ extern "C" __global__ void __launch_bounds__(NT) rfx_plan_compact(
   s << R"RFX(
 extern "C" __global__ void __launch_bounds__(NT) rfx_plan_compact(
     const u8* __restrict__ in, u64 n, u8* __restrict__ out, u64* __restrict__ d_count,
-    u64* __restrict__ status, u32* __restrict__ tile_counter, u32* err) {
+    u64* __restrict__ status, u32* __restrict__ tile_counter, u32* err, const RfxConsts K) {
   __shared__ u32 s_cnt[IPT][NT / 32];
   __shared__ u64 s_prefix;
   __shared__ u32 s_tile;
@@ -393,7 +397,7 @@ extern "C" __global__ void __launch_bounds__(NT) rfx_plan_compact(
 #pragma unroll
     for (int j = 0; j < IPT; ++j) {
       const u64 i = tile * TILE + (u64)j * NT + t;
-      sel[j] = i < n ? process(L[j], O[j]) : false;
+      sel[j] = i < n ? process(L[j], O[j], K) : false;
       const unsigned b = __ballot_sync(0xffffffffu, sel[j]);
       rank[j] = __popc(b & ((1u << lane) - 1u));
       if (lane == 0) s_cnt[j][warp] = __popc(b);
@@ -436,6 +440,28 @@ extern "C" __global__ void __launch_bounds__(NT) rfx_plan_compact(
   return s.str();
 }
 
+struct HostConsts {
+  uint64_t c[16];
+};
+static_assert(kMaxCmp * 2 <= 16, "constant slots");
+
+HostConsts consts_of(const ScanProgram& p) {
+  HostConsts k;
+  for (auto& v : k.c) v = 0;
+  for (uint32_t c = 0; c < p.ncmp; ++c) {
+    k.c[2 * c] = p.cmps[c].a_const;
+    k.c[2 * c + 1] = p.cmps[c].b_const;
+  }
+  return k;
+}
+
+// The source of a plan with its comparison constants cleared: the compile cache key.
+ScanProgram without_consts(const ScanProgram& p) {
+  ScanProgram q = p;
+  for (uint32_t c = 0; c < q.ncmp; ++c) q.cmps[c].a_const = q.cmps[c].b_const = 0;
+  return q;
+}
+
 }  // namespace
 
 // Launches the specialised aggregate kernel; RFX_ERR_UNSUPPORTED when it cannot be
@@ -446,14 +472,15 @@ rfx_status jit_aggregate(const ScanProgram& p, const void* in, uint64_t n, unsig
   const uint32_t nacc = p.ngroups_total * (p.nsum + 1);
   const bool priv = nacc <= 24;
   cudaKernel_t k;
-  rfx_status st = jit_kernel(gen_aggregate(p, priv), "rfx_plan_aggregate", &k);
+  rfx_status st = jit_kernel(gen_aggregate(without_consts(p), priv), "rfx_plan_aggregate", &k);
   if (st != RFX_OK) return st;
   const size_t smem = (priv ? (size_t)nacc * kJitThreads : (size_t)nacc) * sizeof(uint64_t);
   RFX_CUDA_TRY(allow_smem((const void*)k, smem));
   const uint64_t blocks = (n + 2ull * kJitThreads - 1) / (2ull * kJitThreads);
   const int grid = persistent_grid((const void*)k, kJitThreads, smem, blocks ? blocks : 1);
+  HostConsts kc = consts_of(p);
   void* args[] = {(void*)&in, (void*)&n, (void*)&gacc, (void*)&done, (void*)&out_keys, (void*)&out_sums,
-                  (void*)&out_counts, (void*)&d_groups, (void*)&err};
+                  (void*)&out_counts, (void*)&d_groups, (void*)&err, (void*)&kc};
   RFX_CUDA_TRY(cudaLaunchKernel((const void*)k, dim3(grid), dim3(kJitThreads), args, smem, stream));
   return RFX_OK;
 }
@@ -468,11 +495,13 @@ rfx_status jit_compact(const ScanProgram& p, int mode, const void* in, uint64_t 
   if ((uint64_t)ipt * kJitThreads < tile_rows) ipt = (int)(tile_rows / kJitThreads);
   tile_rows = (uint64_t)ipt * kJitThreads;
   cudaKernel_t k;
-  rfx_status st = jit_kernel(gen_compact(p, mode, wout, ipt), "rfx_plan_compact", &k);
+  rfx_status st = jit_kernel(gen_compact(without_consts(p), mode, wout, ipt), "rfx_plan_compact", &k);
   if (st != RFX_OK) return st;
   const uint64_t tiles = (n + tile_rows - 1) / tile_rows;
   const int grid = persistent_grid((const void*)k, kJitThreads, 0, tiles ? tiles : 1);
-  void* args[] = {(void*)&in, (void*)&n, (void*)&out, (void*)&d_count, (void*)&status, (void*)&counter, (void*)&err};
+  HostConsts kc = consts_of(p);
+  void* args[] = {(void*)&in, (void*)&n, (void*)&out, (void*)&d_count, (void*)&status, (void*)&counter, (void*)&err,
+                  (void*)&kc};
   RFX_CUDA_TRY(cudaLaunchKernel((const void*)k, dim3(grid), dim3(kJitThreads), args, 0, stream));
   return RFX_OK;
 }

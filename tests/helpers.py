@@ -88,3 +88,25 @@ def three_relation_oracle(d1, d2, f, list_in, list_out):
     k, sums = O.reduce_sum_i64(key, amt)
     _, counts = O.reduce_count(key)
     return k, sums, counts
+
+
+def serving_query_oracle(d1, d2, f, segment, date_lo, date_hi, keys_list=None):
+    """The parameterised select-join-(intersect)-join-aggregate query on the oracle."""
+    d1s = O.select(d1, [32, 8], oracle_cmps([(O.EQ, (O.OPND_VAR, 1), (O.OPND_CONST, segment), O.I8)]))
+    d2f = O.select(d2, [32, 32, 32], oracle_cmps([(O.GE, (O.OPND_VAR, 2), (O.OPND_CONST, date_lo), O.I32),
+                                                  (O.LT, (O.OPND_VAR, 2), (O.OPND_CONST, date_hi), O.I32)]))
+    d2s = O.project(d2f, [32, 32, 32], [32, 32], [1, 0])
+    d2s = O.sort_pairs(d2s, begin_bit=32, end_bit=64)
+    j1 = O.join_tuples(d1s, 8, d2s, 32, 16)
+    keys = O.project(j1, [32, 8, 32], [32], [2]).view(np.uint32).ravel()
+    keys = O.sort_pairs(keys)
+    if keys_list is not None:
+        keys = O.set_intersection(keys, keys_list)
+    fs = O.sort_pairs(f, begin_bit=64, end_bit=96)
+    j2 = O.join_tuples(keys.view(np.uint8).reshape(-1, 4), 0, fs, 64, 16)
+    limbs = j2.view(np.uint64)
+    key = limbs[:, 1].astype(np.uint32)
+    amt = limbs[:, 0].astype(np.int64)
+    k, sums = O.reduce_sum_i64(key, amt)
+    _, counts = O.reduce_count(key)
+    return k, sums, counts

@@ -18,6 +18,7 @@ constexpr int kSortThreads = 256;
 constexpr int kRadix = 256;
 constexpr int kSortWarps = kSortThreads / 32;
 constexpr int kMaxSortPasses = 16;  // up to 128 key bits per call
+constexpr int kSortLookWindow = 16;  // predecessors examined per look-back round trip
 
 // Items per thread by the bytes moved per item.
 template <int K, int V>
@@ -273,29 +274,49 @@ sort_pass_kernel(const SortPassArgs a) {
       uint32_t wpre = 0;
       for (uint32_t w = 0; w < warp; ++w) wpre += s_scan[w];
       s_local[t] = wpre + incl - count;
-      // decoupled look-back for this digit: predecessors usually hold an inclusive
-      // prefix within one or two steps, so each thread walks its own digit
+      // decoupled look-back for this digit, kSortLookWindow predecessors per round trip
+      // (independent loads, all in flight at once): with hundreds of tiles in flight the
+      // nearest inclusive predecessor is tens of tiles back, and a one-by-one walk would
+      // pay a round trip per tile
       uint32_t* st = a.status + tile * kRadix + t;
       uint32_t prefix = 0;
       if (tile == 0) {
         st_relaxed_u32(st, kSFlagInc | count);
       } else {
         st_relaxed_u32(st, kSFlagAgg | count);
-        int64_t p = (int64_t)tile - 1;
+        int64_t base = (int64_t)tile - 1;
         uint32_t spins = 0;
-        while (p >= 0) {
-          const uint32_t s = ld_relaxed_u32(a.status + (uint64_t)p * kRadix + t);
-          if ((s & ~kSValMask) == 0) {
+        while (base >= 0) {
+          uint32_t w[kSortLookWindow];
+#pragma unroll
+          for (int r = 0; r < kSortLookWindow; ++r) {
+            const int64_t idx = base - r;
+            w[r] = idx >= 0 ? ld_relaxed_u32(a.status + (uint64_t)idx * kRadix + t) : kSFlagInc;
+          }
+          int r_inc = kSortLookWindow;
+#pragma unroll
+          for (int r = kSortLookWindow - 1; r >= 0; --r)
+            if (w[r] & kSFlagInc) r_inc = r;
+          bool busy = false;
+          uint32_t sum = 0;
+#pragma unroll
+          for (int r = 0; r < kSortLookWindow; ++r) {
+            if (r <= r_inc) {
+              busy = busy || (w[r] & ~kSValMask) == 0;
+              sum += w[r] & kSValMask;
+            }
+          }
+          if (busy) {
             if (++spins > kSpinLimit) {
               raise_error(a.err, kErrTimeout);
               break;
             }
-            __nanosleep(spins < 64 ? 20 : 100);
+            __nanosleep(spins < 16 ? 32 : 128);
             continue;
           }
-          prefix += s & kSValMask;
-          if (s & kSFlagInc) break;
-          --p;
+          prefix += sum;
+          if (r_inc < kSortLookWindow) break;
+          base -= kSortLookWindow;
         }
         st_relaxed_u32(st, kSFlagInc | ((prefix + count) & kSValMask));
       }

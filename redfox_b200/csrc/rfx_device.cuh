@@ -54,11 +54,17 @@ constexpr uint64_t kFlagAgg = 1ull << 62;
 constexpr uint64_t kFlagInc = 2ull << 62;
 constexpr uint64_t kValMask = (1ull << 62) - 1;
 
-// Called by the whole warp 0 of a tile.  Publishes `aggregate`, walks predecessors 32
-// at a time and returns the exclusive prefix (same value in every lane).
+// Called by the whole warp 0 of a tile.  Publishes `aggregate`, examines predecessors
+// kLookLanes per lane (a window of 32 * kLookLanes tiles per round trip) and returns the
+// exclusive prefix (same value in every lane).  A wider window pays when the nearest
+// inclusive predecessor is far back (many short tiles in flight, as in the set filters);
+// where it is usually near, the extra loads only add L2 traffic (the 60M-row select runs
+// 2.36 ms with 1, 3.0 ms with 4).
+template <int kLookLanes = 1>
 __device__ __forceinline__ uint64_t lookback_exclusive(uint64_t* status, uint32_t tile,
                                                        uint64_t aggregate, uint32_t* err) {
   const uint32_t lane = threadIdx.x & 31;
+  constexpr uint32_t WIN = 32u * kLookLanes;
   if (tile == 0) {
     if (lane == 0) st_relaxed_u64(&status[0], kFlagInc | (aggregate & kValMask));
     return 0;
@@ -68,27 +74,39 @@ __device__ __forceinline__ uint64_t lookback_exclusive(uint64_t* status, uint32_
   int64_t base = (int64_t)tile - 1;  // highest predecessor not yet folded in
   uint32_t spins = 0;
   while (true) {
-    int64_t idx = base - (int64_t)lane;
-    uint64_t s = idx >= 0 ? ld_relaxed_u64(&status[idx]) : kFlagInc;
-    uint64_t flag = s & ~kValMask;
-    unsigned not_ready = __ballot_sync(0xffffffffu, flag == 0);
-    unsigned inc = __ballot_sync(0xffffffffu, flag == kFlagInc);
-    // lanes up to (and including) the first inclusive one are usable if none of them
-    // is still unpublished
-    unsigned upto = inc ? ((inc & (0u - inc)) << 1) - 1 : 0xffffffffu;  // lanes 0..first_inc
-    if (not_ready & upto) {
+    uint64_t w[kLookLanes];
+#pragma unroll
+    for (int r = 0; r < kLookLanes; ++r) {
+      const int64_t idx = base - (int64_t)(lane * kLookLanes + r);
+      w[r] = idx >= 0 ? ld_relaxed_u64(&status[idx]) : kFlagInc;
+    }
+    uint32_t first = WIN;
+#pragma unroll
+    for (int r = kLookLanes - 1; r >= 0; --r)
+      if ((w[r] & ~kValMask) == kFlagInc) first = lane * kLookLanes + r;
+    const uint32_t dmin = __reduce_min_sync(0xffffffffu, first);
+    bool busy = false;
+    uint64_t v = 0;
+#pragma unroll
+    for (int r = 0; r < kLookLanes; ++r) {
+      if (lane * kLookLanes + r <= dmin) {
+        busy = busy || (w[r] & ~kValMask) == 0;
+        v += w[r] & kValMask;
+      }
+    }
+    if (__any_sync(0xffffffffu, busy)) {
       if (++spins > kSpinLimit) {
         raise_error(err, kErrTimeout);
         break;
       }
-      __nanosleep(spins < 64 ? 20 : 200);
+      __nanosleep(spins < 64 ? 32 : 200);
       continue;
     }
-    uint64_t v = ((upto >> lane) & 1u) ? (s & kValMask) : 0;
+#pragma unroll
     for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
     prefix += v;
-    if (inc) break;
-    base -= 32;
+    if (dmin < WIN) break;
+    base -= WIN;
   }
   if (lane == 0) st_relaxed_u64(&status[tile], kFlagInc | ((prefix + aggregate) & kValMask));
   return prefix;

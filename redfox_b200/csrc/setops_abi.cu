@@ -13,6 +13,7 @@ bool elem_width(uint32_t e) { return e == 1 || e == 2 || e == 4 || e == 8 || e =
 struct FilterLayout {
   uint64_t* status;
   uint32_t* counter;
+  uint64_t* split;   // 3 words per tile (filled by set_split_kernel)
   size_t clear;
   size_t total;
 };
@@ -20,16 +21,25 @@ struct FilterLayout {
 FilterLayout filter_layout(void* ws, uint64_t n) {
   FilterLayout L;
   Carver c(ws);
-  L.status = c.take<uint64_t>((n + kSetTile - 1) / kSetTile + 1);
+  const uint64_t tiles = (n + kSetTile - 1) / kSetTile + 1;
+  L.status = c.take<uint64_t>(tiles);
   L.counter = c.take<uint32_t>(1);
   L.clear = align_up(c.used, 256);
-  L.total = L.clear;
+  c.used = L.clear;
+  L.split = c.take<uint64_t>(3 * tiles);
+  L.total = align_up(c.used, 256);
   return L;
 }
 
 template <int E>
 rfx_status launch_filter(int mode, SetFilterArgs& a, cudaStream_t s) {
   const uint64_t tiles = (a.na + kSetTile - 1) / kSetTile;
+  if (mode != KEEP_HEADS && tiles) {
+    const uint64_t work = 3 * tiles * 32;   // one warp per search
+    const int g = (int)((work + 255) / 256);
+    set_split_kernel<E><<<g, 256, 0, s>>>(a.a, a.na, a.b, a.nb, const_cast<uint64_t*>(a.split));
+    RFX_CUDA_TRY(cudaGetLastError());
+  }
   const void* k = mode == KEEP_MATCHED ? (const void*)set_filter_kernel<E, KEEP_MATCHED>
                 : mode == KEEP_UNMATCHED ? (const void*)set_filter_kernel<E, KEEP_UNMATCHED>
                                          : (const void*)set_filter_kernel<E, KEEP_HEADS>;
@@ -127,6 +137,7 @@ rfx_status set_op_impl(uint32_t op, void* out, uint64_t* d_count, const void* a,
   std::memset(&f, 0, sizeof(f));
   f.status = L.f.status;
   f.tile_counter = L.f.counter;
+  f.split = L.f.split;
   f.err = err;
   if (op == RFX_SET_UNION) {
     f.a = static_cast<const uint8_t*>(b);  // B - A: the copies of B beyond A's

@@ -31,6 +31,7 @@ struct SetFilterArgs {
   const uint8_t* b;
   uint64_t nb;
   const uint8_t* prev;   // KEEP_HEADS: element before each tile (saved before in-place writes)
+  const uint64_t* split; // KEEP_(UN)MATCHED: per tile (run start of its first element, B window)
   uint8_t* out;
   uint64_t* d_count;
   uint64_t* status;
@@ -82,7 +83,6 @@ template <int E, int MODE>
 __global__ void __launch_bounds__(kSetThreads) set_filter_kernel(const SetFilterArgs p) {
   typedef typename std::conditional<(E <= 8), uint64_t, u128>::type WT;
   constexpr int WCAP = E <= 8 ? 2048 : 1024;
-  __shared__ WT s_a[MODE == KEEP_HEADS ? 1 : kSetTile];
   __shared__ WT s_b[MODE == KEEP_HEADS ? 1 : WCAP];
   __shared__ uint64_t s_rs0, s_blo, s_bhi;
   __shared__ uint32_t s_warp[kSetThreads / 32];
@@ -121,44 +121,84 @@ __global__ void __launch_bounds__(kSetThreads) set_filter_kernel(const SetFilter
         keep[j] = i == 0 || v[j] != (j == 0 ? before : v[j - 1]);
       }
     } else {
-      // the tile's own elements and the window of B values they can equal, in shared
-      // memory; the run containing the tile's first element may start in an earlier tile
+      // The window of B values the tile's elements can equal, in shared memory.  A thread's
+      // items are consecutive and sorted: one binary search finds the first candidate in B
+      // for its first item, later items advance from there (merge order), and equal runs
+      // in B are measured by galloping.  An item's rank within its run of equal values is
+      // its distance from the run's first item: the last head (first item of a run) at or
+      // before it, from a block max-scan of the threads' last heads, or -- for the run that
+      // continues from the previous tile -- the run start found by set_split_kernel.
       const uint64_t tfirst = tile * kSetTile;
-      const uint64_t tn = min((uint64_t)kSetTile, p.na - tfirst);
-      if (t == 0) s_rs0 = bsearch<E>(A, A.key(tfirst), 0, tfirst, false);
-      if (t == 32) s_blo = bsearch<E>(B, A.key(tfirst), 0, p.nb, false);
-      if (t == 64) s_bhi = bsearch<E>(B, A.key(tfirst + tn - 1), 0, p.nb, true);
-      for (uint32_t x = t; x < tn; x += kSetThreads) s_a[x] = (WT)A.key(tfirst + x);
+      if (t == 0) s_rs0 = p.split[3 * tile];
+      if (t == 1) s_blo = p.split[3 * tile + 1];
+      if (t == 2) s_bhi = p.split[3 * tile + 2];
       __syncthreads();
       const uint64_t blo0 = s_blo, bn = s_bhi > s_blo ? s_bhi - s_blo : 0;
       const bool staged = bn <= (uint64_t)WCAP;
       if (staged)
         for (uint64_t x = t; x < bn; x += kSetThreads) s_b[x] = (WT)B.key(blo0 + x);
-      __syncthreads();
-      const u128 v0 = (u128)s_a[0];
+      // heads of this thread's items (local index of its last head, or -1)
+      int32_t last_head = -1;
+      uint32_t heads = 0;
+      u128 prev = 0;
+      if (first < p.na && first > tfirst) prev = A.key(first - 1);
 #pragma unroll
       for (int j = 0; j < kSetIPT; ++j) {
         const uint64_t i = first + j;
         if (i >= p.na) continue;
-        const uint32_t li = (uint32_t)(i - tfirst);
-        const uint64_t run_start = v[j] == v0 ? s_rs0 : tfirst + smem_lower(s_a, li, v[j]);
+        const bool h = i == 0 || (i > tfirst && v[j] != (j == 0 ? prev : v[j - 1]));
+        if (h) {
+          heads |= 1u << j;
+          last_head = (int32_t)(i - tfirst);
+        }
+      }
+      // exclusive max-scan of last_head over the block
+      int32_t incl = last_head;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+        if ((t & 31) >= (uint32_t)o) incl = max(incl, y);
+      }
+      if ((t & 31) == 31) s_warp[t >> 5] = (uint32_t)(incl + 1);
+      __syncthreads();
+      int32_t before = -1;
+      for (uint32_t w = 0; w < (t >> 5); ++w) before = max(before, (int32_t)s_warp[w] - 1);
+      const int32_t ex = __shfl_up_sync(0xffffffffu, incl, 1);
+      if ((t & 31) != 0) before = max(before, ex);
+      uint64_t run_start = before >= 0 ? tfirst + (uint64_t)before : s_rs0;
+      // first candidate in B for the first item
+      uint64_t pos = 0;
+      if (first < p.na) {
+        pos = staged ? (uint64_t)smem_lower(s_b, (uint32_t)bn, v[0]) : bsearch<E>(B, v[0], 0, p.nb, false);
+      }
+#pragma unroll
+      for (int j = 0; j < kSetIPT; ++j) {
+        const uint64_t i = first + j;
+        if (i >= p.na) continue;
+        if ((heads >> j) & 1u) run_start = i;
         uint64_t nbeq;
         if (staged) {
-          nbeq = smem_lower_strict(s_b, (uint32_t)bn, v[j]) - smem_lower(s_b, (uint32_t)bn, v[j]);
+          while (pos < bn && (u128)s_b[pos] < v[j]) ++pos;
+          nbeq = 0;
+          if (pos < bn && (u128)s_b[pos] == v[j]) {
+            if (pos + 1 >= bn || (u128)s_b[pos + 1] != v[j]) nbeq = 1;
+            else nbeq = smem_lower_strict(s_b + pos, (uint32_t)(bn - pos), v[j]);
+          }
         } else {
-          const uint64_t l = bsearch<E>(B, v[j], 0, p.nb, false);
-          nbeq = gallop<E>(B, v[j], l, true) - l;
+          pos = j == 0 ? pos : (gallop<E>(B, v[j], pos, false));
+          nbeq = gallop<E>(B, v[j], pos, true) - pos;
         }
         const uint64_t rank = i - run_start;
         keep[j] = MODE == KEEP_MATCHED ? rank < nbeq : rank >= nbeq;
       }
+      __syncthreads();
     }
 #pragma unroll
     for (int j = 0; j < kSetIPT; ++j) kept += keep[j] ? 1u : 0u;
     uint32_t btot;
     const uint64_t ex = block_exclusive_u32(kept, s_warp, &btot);
     if ((t >> 5) == 0) {
-      const uint64_t pre = lookback_exclusive(p.status, (uint32_t)tile, btot, p.err);
+      const uint64_t pre = lookback_exclusive<4>(p.status, (uint32_t)tile, btot, p.err);
       if (t == 0) {
         s_prefix = pre;
         if (tile == num_tiles - 1) *p.d_count = pre + btot;
@@ -175,6 +215,64 @@ __global__ void __launch_bounds__(kSetThreads) set_filter_kernel(const SetFilter
     __syncthreads();
   }
   if (p.na == 0 && blockIdx.x == 0 && t == 0) *p.d_count = 0;
+}
+
+// Warp-cooperative search: the first index in [lo, hi) whose key is >= k (> k when
+// strict), or hi.  Each round the 32 lanes probe 32 evenly spaced keys and the range
+// shrinks 32-fold, so a search over millions of keys costs ~5 dependent round trips
+// instead of ~22 for a one-thread binary search.  All lanes return the same index.
+template <int E>
+__device__ __forceinline__ uint64_t warp_search(const KeyView<E>& v, u128 k, uint64_t lo, uint64_t hi, bool strict) {
+  const uint32_t lane = threadIdx.x & 31;
+  while (hi - lo > 32) {
+    const uint64_t step = (hi - lo + 31) / 32;
+    const uint64_t p = lo + lane * step;
+    bool before = false;
+    if (p < hi) {
+      const u128 m = v.key(p);
+      before = strict ? (m <= k) : (m < k);
+    }
+    const uint32_t cnt = __popc(__ballot_sync(0xffffffffu, before));
+    if (cnt == 0) return lo;
+    const uint64_t nlo = lo + (uint64_t)(cnt - 1) * step + 1;
+    const uint64_t nhi = cnt < 32 ? min(hi, lo + (uint64_t)cnt * step) : hi;
+    lo = nlo;
+    hi = nhi;
+  }
+  bool before = false;
+  if (lo + lane < hi) {
+    const u128 m = v.key(lo + lane);
+    before = strict ? (m <= k) : (m < k);
+  }
+  return lo + __popc(__ballot_sync(0xffffffffu, before));
+}
+
+// Per tile of A (kSetTile elements): the start of the run of equal values containing the
+// tile's first element, and the window of B that can equal the tile's values -- one warp
+// per search, all tiles at once, so the filter kernel's tiles do not each wait on chains
+// of dependent loads.
+template <int E>
+__global__ void set_split_kernel(const uint8_t* a, uint64_t na, const uint8_t* b, uint64_t nb, uint64_t* split) {
+  const KeyView<E> A{a, na, 0};
+  const KeyView<E> B{b, nb, 0};
+  const uint64_t tiles = (na + kSetTile - 1) / kSetTile;
+  const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x / 32);
+  for (uint64_t x = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / 32; x < 3 * tiles; x += warps) {
+    const uint64_t tile = x / 3, kind = x % 3;
+    const uint64_t tfirst = tile * kSetTile;
+    const uint64_t tlast = min(na, tfirst + kSetTile) - 1;
+    uint64_t r;
+    if (kind == 0) {
+      const u128 k0 = A.key(tfirst);
+      // a tile whose first element starts a new run needs no search
+      r = (tfirst == 0 || A.key(tfirst - 1) != k0) ? tfirst : warp_search<E>(A, k0, 0, tfirst, false);
+    } else if (kind == 1) {
+      r = warp_search<E>(B, A.key(tfirst), 0, nb, false);
+    } else {
+      r = warp_search<E>(B, A.key(tlast), 0, nb, true);
+    }
+    if ((threadIdx.x & 31) == 0) split[x] = r;
+  }
 }
 
 // The element before each tile, saved before an in-place pass overwrites it.

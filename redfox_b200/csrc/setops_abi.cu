@@ -21,7 +21,7 @@ struct FilterLayout {
 FilterLayout filter_layout(void* ws, uint64_t n) {
   FilterLayout L;
   Carver c(ws);
-  const uint64_t tiles = (n + kSetTile - 1) / kSetTile + 1;
+  const uint64_t tiles = (n + kSetTileMin - 1) / kSetTileMin + 1;
   L.status = c.take<uint64_t>(tiles);
   L.counter = c.take<uint32_t>(1);
   L.clear = align_up(c.used, 256);
@@ -33,7 +33,7 @@ FilterLayout filter_layout(void* ws, uint64_t n) {
 
 template <int E>
 rfx_status launch_filter(int mode, SetFilterArgs& a, cudaStream_t s) {
-  const uint64_t tiles = (a.na + kSetTile - 1) / kSetTile;
+  const uint64_t tiles = (a.na + set_tile<E>() - 1) / set_tile<E>();
   if (mode != KEEP_HEADS && tiles) {
     const uint64_t work = 3 * tiles * 32;   // one warp per search
     const int g = (int)((work + 255) / 256);
@@ -87,10 +87,10 @@ rfx_status dispatch_merge(uint32_t e, const void* a, uint64_t na, const void* d,
 
 template <int E>
 rfx_status launch_prev(const void* a, uint64_t n, void* prev, cudaStream_t s) {
-  const uint64_t tiles = (n + kSetTile - 1) / kSetTile;
+  const uint64_t tiles = (n + set_tile<E>() - 1) / set_tile<E>();
   const int grid = (int)((tiles + 255) / 256);
   tile_prev_kernel<E><<<grid ? grid : 1, 256, 0, s>>>(static_cast<const uint8_t*>(a), n, static_cast<uint8_t*>(prev),
-                                                      kSetTile);
+                                                      set_tile<E>());
   RFX_CUDA_TRY(cudaGetLastError());
   return RFX_OK;
 }
@@ -163,7 +163,7 @@ size_t unique_workspace_impl(uint64_t n, uint32_t e) {
   FilterLayout f = filter_layout(nullptr, n);
   Carver c(nullptr);
   c.used = f.total;
-  c.take<uint8_t>(((n + kSetTile - 1) / kSetTile + 1) * (e < 16 ? 16 : e));
+  c.take<uint8_t>(((n + kSetTileMin - 1) / kSetTileMin + 1) * (e < 16 ? 16 : e));
   return align_up(c.used, 256);
 }
 
@@ -174,7 +174,7 @@ rfx_status unique_impl(void* data, uint64_t n, uint64_t* d_count, uint32_t e, vo
   FilterLayout f = filter_layout(ws, n);
   Carver c(ws);
   c.used = f.total;
-  uint8_t* prev = c.take<uint8_t>(((n + kSetTile - 1) / kSetTile + 1) * (e < 16 ? 16 : e));
+  uint8_t* prev = c.take<uint8_t>(((n + kSetTileMin - 1) / kSetTileMin + 1) * (e < 16 ? 16 : e));
   if (!ws || wsb < align_up(c.used, 256)) return RFX_ERR_WORKSPACE;
   uint32_t* err = device_error_word();
   if (!err) return RFX_ERR_CUDA;

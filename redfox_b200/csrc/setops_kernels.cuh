@@ -18,8 +18,13 @@
 namespace rfx {
 
 constexpr int kSetThreads = 256;
-constexpr int kSetIPT = 4;
-constexpr int kSetTile = kSetThreads * kSetIPT;
+// Items per thread (8: 16 measured no faster for 4-byte keys); elements up to 8 bytes
+// live in 64-bit registers.
+template <int E>
+__host__ __device__ constexpr int set_ipt() { return 8; }
+template <int E>
+__host__ __device__ constexpr int set_tile() { return kSetThreads * set_ipt<E>(); }
+constexpr int kSetTileMin = kSetThreads * 8;   // the smallest tile: workspace sizing
 constexpr int kMergeVT = 8;
 constexpr int kMergeTile = kSetThreads * kMergeVT;
 
@@ -82,6 +87,8 @@ __device__ __forceinline__ uint32_t smem_lower_strict(const T* w, uint32_t n, u1
 template <int E, int MODE>
 __global__ void __launch_bounds__(kSetThreads) set_filter_kernel(const SetFilterArgs p) {
   typedef typename std::conditional<(E <= 8), uint64_t, u128>::type WT;
+  constexpr int IPT = set_ipt<E>();
+  constexpr int TILE = set_tile<E>();
   constexpr int WCAP = E <= 8 ? 2048 : 1024;
   __shared__ WT s_b[MODE == KEEP_HEADS ? 1 : WCAP];
   __shared__ uint64_t s_rs0, s_blo, s_bhi;
@@ -89,7 +96,7 @@ __global__ void __launch_bounds__(kSetThreads) set_filter_kernel(const SetFilter
   __shared__ uint64_t s_prefix;
   __shared__ uint32_t s_tile;
   const uint32_t t = threadIdx.x;
-  const uint64_t num_tiles = (p.na + kSetTile - 1) / kSetTile;
+  const uint64_t num_tiles = (p.na + TILE - 1) / TILE;
   const KeyView<E> A{p.a, p.na, 0};
   const KeyView<E> B{p.b, p.nb, 0};
   while (true) {
@@ -97,25 +104,25 @@ __global__ void __launch_bounds__(kSetThreads) set_filter_kernel(const SetFilter
     __syncthreads();
     const uint64_t tile = s_tile;
     if (tile >= num_tiles) break;
-    const uint64_t first = tile * kSetTile + (uint64_t)t * kSetIPT;
-    u128 v[kSetIPT];
-    bool keep[kSetIPT];
+    const uint64_t first = tile * TILE + (uint64_t)t * IPT;
+    WT v[IPT];
+    bool keep[IPT];
     uint32_t kept = 0;
     // every input of this tile is read before its aggregate is published, which keeps
     // the in-place unique safe (writes land below the inputs of later tiles)
 #pragma unroll
-    for (int j = 0; j < kSetIPT; ++j) {
+    for (int j = 0; j < IPT; ++j) {
       const uint64_t i = first + j;
       keep[j] = false;
-      if (i < p.na) v[j] = A.key(i);
+      if (i < p.na) v[j] = (WT)A.key(i);
     }
     if constexpr (MODE == KEEP_HEADS) {
-      u128 before = 0;
+      WT before = 0;
       if (first < p.na && first > 0) {
-        before = (t == 0) ? load_u128<E>(p.prev, tile) : A.key(first - 1);
+        before = (WT)((t == 0) ? load_u128<E>(p.prev, tile) : A.key(first - 1));
       }
 #pragma unroll
-      for (int j = 0; j < kSetIPT; ++j) {
+      for (int j = 0; j < IPT; ++j) {
         const uint64_t i = first + j;
         if (i >= p.na) continue;
         keep[j] = i == 0 || v[j] != (j == 0 ? before : v[j - 1]);
@@ -128,7 +135,7 @@ __global__ void __launch_bounds__(kSetThreads) set_filter_kernel(const SetFilter
       // its distance from the run's first item: the last head (first item of a run) at or
       // before it, from a block max-scan of the threads' last heads, or -- for the run that
       // continues from the previous tile -- the run start found by set_split_kernel.
-      const uint64_t tfirst = tile * kSetTile;
+      const uint64_t tfirst = tile * TILE;
       if (t == 0) s_rs0 = p.split[3 * tile];
       if (t == 1) s_blo = p.split[3 * tile + 1];
       if (t == 2) s_bhi = p.split[3 * tile + 2];
@@ -140,10 +147,10 @@ __global__ void __launch_bounds__(kSetThreads) set_filter_kernel(const SetFilter
       // heads of this thread's items (local index of its last head, or -1)
       int32_t last_head = -1;
       uint32_t heads = 0;
-      u128 prev = 0;
-      if (first < p.na && first > tfirst) prev = A.key(first - 1);
+      WT prev = 0;
+      if (first < p.na && first > tfirst) prev = (WT)A.key(first - 1);
 #pragma unroll
-      for (int j = 0; j < kSetIPT; ++j) {
+      for (int j = 0; j < IPT; ++j) {
         const uint64_t i = first + j;
         if (i >= p.na) continue;
         const bool h = i == 0 || (i > tfirst && v[j] != (j == 0 ? prev : v[j - 1]));
@@ -172,16 +179,16 @@ __global__ void __launch_bounds__(kSetThreads) set_filter_kernel(const SetFilter
         pos = staged ? (uint64_t)smem_lower(s_b, (uint32_t)bn, v[0]) : bsearch<E>(B, v[0], 0, p.nb, false);
       }
 #pragma unroll
-      for (int j = 0; j < kSetIPT; ++j) {
+      for (int j = 0; j < IPT; ++j) {
         const uint64_t i = first + j;
         if (i >= p.na) continue;
         if ((heads >> j) & 1u) run_start = i;
         uint64_t nbeq;
         if (staged) {
-          while (pos < bn && (u128)s_b[pos] < v[j]) ++pos;
+          while (pos < bn && s_b[pos] < v[j]) ++pos;
           nbeq = 0;
-          if (pos < bn && (u128)s_b[pos] == v[j]) {
-            if (pos + 1 >= bn || (u128)s_b[pos + 1] != v[j]) nbeq = 1;
+          if (pos < bn && s_b[pos] == v[j]) {
+            if (pos + 1 >= bn || s_b[pos + 1] != v[j]) nbeq = 1;
             else nbeq = smem_lower_strict(s_b + pos, (uint32_t)(bn - pos), v[j]);
           }
         } else {
@@ -194,7 +201,7 @@ __global__ void __launch_bounds__(kSetThreads) set_filter_kernel(const SetFilter
       __syncthreads();
     }
 #pragma unroll
-    for (int j = 0; j < kSetIPT; ++j) kept += keep[j] ? 1u : 0u;
+    for (int j = 0; j < IPT; ++j) kept += keep[j] ? 1u : 0u;
     uint32_t btot;
     const uint64_t ex = block_exclusive_u32(kept, s_warp, &btot);
     if ((t >> 5) == 0) {
@@ -207,7 +214,7 @@ __global__ void __launch_bounds__(kSetThreads) set_filter_kernel(const SetFilter
     __syncthreads();
     uint64_t pos = s_prefix + ex;
 #pragma unroll
-    for (int j = 0; j < kSetIPT; ++j) {
+    for (int j = 0; j < IPT; ++j) {
       if (!keep[j]) continue;
       if (pos < p.na) store_u128<E>(p.out, pos, v[j]);
       ++pos;
@@ -247,7 +254,7 @@ __device__ __forceinline__ uint64_t warp_search(const KeyView<E>& v, u128 k, uin
   return lo + __popc(__ballot_sync(0xffffffffu, before));
 }
 
-// Per tile of A (kSetTile elements): the start of the run of equal values containing the
+// Per tile of A (set_tile<E>() elements): the start of the run of equal values containing the
 // tile's first element, and the window of B that can equal the tile's values -- one warp
 // per search, all tiles at once, so the filter kernel's tiles do not each wait on chains
 // of dependent loads.
@@ -255,12 +262,12 @@ template <int E>
 __global__ void set_split_kernel(const uint8_t* a, uint64_t na, const uint8_t* b, uint64_t nb, uint64_t* split) {
   const KeyView<E> A{a, na, 0};
   const KeyView<E> B{b, nb, 0};
-  const uint64_t tiles = (na + kSetTile - 1) / kSetTile;
+  const uint64_t tiles = (na + set_tile<E>() - 1) / set_tile<E>();
   const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x / 32);
   for (uint64_t x = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / 32; x < 3 * tiles; x += warps) {
     const uint64_t tile = x / 3, kind = x % 3;
-    const uint64_t tfirst = tile * kSetTile;
-    const uint64_t tlast = min(na, tfirst + kSetTile) - 1;
+    const uint64_t tfirst = tile * set_tile<E>();
+    const uint64_t tlast = min(na, tfirst + set_tile<E>()) - 1;
     uint64_t r;
     if (kind == 0) {
       const u128 k0 = A.key(tfirst);

@@ -417,6 +417,81 @@ def operator_benchmarks(dev, fact_rows, peak, reps=5):
     return ops
 
 
+def tuning_benchmark(dev, fact_rows, reps=5):
+    """Default variant vs the autotuner's choice per size class for the tuned operators:
+    select (plan-specialised compaction, rows per thread), the staged reduce (256- or
+    128-line tiles) and the set filters (8 or 4 items per thread), each at a large and a
+    small size.  Device time per call (CUDA events), same inputs both ways."""
+    import torch
+
+    from redfox_b200 import plans as PL
+    from redfox_b200 import rfx as R
+    from redfox_b200 import workloads as WL
+
+    cases = []
+    small_rows = fact_rows[:600_000]
+    for name, rows in (("select_fact_60M", fact_rows), ("select_fact_600K", small_rows)):
+        out = torch.empty_like(rows)
+        cnt = torch.zeros(1, dtype=torch.int64, device=dev)
+        t = R.Tuple.of(WL.FACT_WIDTHS)
+        cm = R.make_cmps(WL.fact_predicate())
+        wsb = R.LIB.rfx_select_workspace(rows.shape[0], R.C.byref(t))
+        ws = R._empty_bytes(wsb, dev)
+
+        def f(rows=rows, out=out, cnt=cnt, t=t, cm=cm, ws=ws, wsb=wsb):
+            R.check("sel", R.LIB.rfx_select(R._ptr(out), R._ptr(cnt), R._ptr(rows), rows.shape[0], R.C.byref(t), cm,
+                                            1, R._ptr(ws), wsb, R._stream()))
+        cases.append((name, f, (out, ws)))
+    for name, (nr, ns, dom) in (("reduce_join_19M", (1_000_000, 4_000_000, 1 << 18)),
+                                ("reduce_join_190K", (10_000, 40_000, 1 << 11))):
+        r, s_ = PL.gen_join_aggregate(nr, ns, key_domain=dom, device=dev)
+        R.sort_pairs(r, begin_bit=32, end_bit=64)
+        R.sort_pairs(s_, begin_bit=64, end_bit=96)
+        jout, total = R.join_tuples_two_step(r, 32, s_, 64, 16)
+        g = torch.zeros(1, dtype=torch.int64, device=dev)
+        ok = torch.empty(total, dtype=torch.int32, device=dev)
+        osum = torch.empty(total, dtype=torch.int64, device=dev)
+        ocnt = torch.empty(total, dtype=torch.int32, device=dev)
+        wsb = R.LIB.rfx_reduce_by_key_workspace(total)
+        ws = R._empty_bytes(wsb, dev)
+
+        def f(jout=jout, total=total, g=g, ok=ok, osum=osum, ocnt=ocnt, ws=ws, wsb=wsb):
+            R.check("rt", R.LIB.rfx_reduce_tuples(R._ptr(jout), total, None, 16, 96, 0, 64, R._ptr(ok), 4,
+                                                  R._ptr(osum), R._ptr(ocnt), R._ptr(g), R._ptr(ws), wsb,
+                                                  R._stream()))
+        cases.append((name, f, (jout, ok, osum, ocnt, ws)))
+    for name, (na, nb) in (("intersect_5M_2M", (5_000_000, 2_000_000)), ("intersect_50K_20K", (50_000, 20_000))):
+        a = R.gen_uniform_rows(na, [32], 31, [0], [15_000_000], device=dev).view(torch.int32).view(-1).clone()
+        b = R.gen_uniform_rows(nb, [32], 32, [0], [15_000_000], device=dev).view(torch.int32).view(-1).clone()
+        R.sort_pairs(a)
+        R.sort_pairs(b)
+        a = R.unique(a).clone()
+        b = R.unique(b).clone()
+        out = torch.empty(a.shape[0] + b.shape[0], dtype=torch.int32, device=dev)
+        c = torch.zeros(1, dtype=torch.int64, device=dev)
+        wsb = R.LIB.rfx_set_op_workspace(R.SET_INTERSECTION, a.shape[0], b.shape[0], 4)
+        ws = R._empty_bytes(wsb, dev)
+
+        def f(a=a, b=b, out=out, c=c, ws=ws, wsb=wsb):
+            R.check("set", R.LIB.rfx_set_op(R.SET_INTERSECTION, R._ptr(out), R._ptr(c), R._ptr(a), a.shape[0],
+                                            R._ptr(b), b.shape[0], 4, R._ptr(ws), wsb, R._stream()))
+        cases.append((name, f, (a, b, out, ws)))
+    res = {}
+    R.tune(0)
+    R.tune_reset()
+    for name, f, _ in cases:
+        res[name] = {"default_ms": _time_ms(f, reps)}
+    R.tune(1)
+    for name, f, _ in cases:
+        f()                      # the tuning call of this class
+        torch.cuda.synchronize()
+        res[name]["tuned_ms"] = _time_ms(f, reps)
+    table = R.tune_table()
+    R.tune(0)
+    R.tune_reset()
+    return {"cases": res, "table": table}
+
+
 def batched_benchmark(dev, nq, reps=3):
     """512 (nq) independent sort + join + aggregate queries, |R|, |S| log-uniform in
     [1e4, 8e6]: one plain launch sequence per query, back to back, against the batched plan
@@ -674,6 +749,7 @@ def main_ours(args):
         if world == 1 and not args.no_operators:
             del dev_in_keep
             result["operators"] = operator_benchmarks(dev, rows, peak)
+            result["tuning"] = tuning_benchmark(dev, rows)
         if world == 1 and args.batched_queries > 0:
             del rows
             torch.cuda.empty_cache()

@@ -355,6 +355,21 @@ rfx_status rfx_filter_aggregate_noalloc(const void* in, uint64_t n, const rfx_tu
 rfx_status rfx_gen_uniform_rows(void* out, uint64_t n, const rfx_tuple* type, uint64_t seed,
                                 const uint64_t* lo, const uint64_t* hi, void* stream);
 
+/* ---------------------------------------------------------------- autotuning
+ * No counterpart in the reference (its kernels have fixed launch shapes).  Operators with
+ * several compiled variants (the TMA-staged rfx_reduce_tuples: 256- or 128-line tiles; the
+ * set filters behind rfx_set_op: 8 or 4 items per thread; the plan-specialised rfx_select /
+ * rfx_select_project: items per thread) run their default unless tuning is on.  With
+ * mode 1 (or RFX_TUNE=1 in the environment) the first call of each (operator, shape, size
+ * class of 4x in n) times every variant on the caller's inputs and stream (CUDA events,
+ * best of three after one untimed run, synchronising the stream) and later calls of that
+ * class run the fastest.  Do not enable it while capturing a stream into a graph. */
+void rfx_tune_set(int mode);
+void rfx_tune_reset(void);
+/* The tuning table as text lines "op=.. shape=.. class=.. variant=.. ms=t0,t1,..";
+ * returns the bytes needed (including the terminating 0); writes at most cap bytes. */
+size_t rfx_tune_dump(char* buf, size_t cap);
+
 #ifdef __cplusplus
 }
 #endif

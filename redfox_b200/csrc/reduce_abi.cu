@@ -5,6 +5,7 @@
 
 #include "host_common.h"
 #include "reduce_kernels.cuh"
+#include "tune.h"
 
 namespace rfx {
 namespace {
@@ -77,9 +78,9 @@ bool aligned_to(const void* p, uint32_t b) {
   return (reinterpret_cast<uintptr_t>(p) % (b < 16 ? b : 16)) == 0;
 }
 
-// Tiles of the TMA-staged tuple reduce: kRowRedThreads 128-byte lines; the smallest tile
-// (16-byte rows) has kRowRedThreads * 8 rows.
-constexpr int kRowRedThreads = 256;
+// Tiles of the TMA-staged tuple reduce: 256 (default) or 128 128-byte lines; records are
+// sized for the smaller tile.
+constexpr int kRowRedThreadsMin = 128;
 
 struct RowLayout {
   SegRecord* records;
@@ -88,7 +89,7 @@ struct RowLayout {
 };
 
 RowLayout row_layout(void* ws, uint64_t n, uint32_t row_bytes) {
-  const uint64_t tile_rows = (uint64_t)kRowRedThreads * kRingLineBytes / row_bytes;
+  const uint64_t tile_rows = (uint64_t)kRowRedThreadsMin * kRingLineBytes / row_bytes;
   const uint64_t tiles = (n + tile_rows - 1) / tile_rows + 1;
   Carver c(ws);
   RowLayout L;
@@ -227,9 +228,8 @@ namespace {
 // The TMA-staged form: rows 16-byte aligned; the workspace of the register-tiled form
 // (kRedTile rows per tile, 52 bytes per tile) always covers its records (32 bytes per
 // tile of at least kRedTile rows).
-template <int RB, int SHAPE>
+template <int RB, int SHAPE, int NT>
 rfx_status launch_rows(const void* rows, uint64_t n, RowReduceArgs& a, cudaStream_t s) {
-  constexpr int NT = kRowRedThreads;
   auto k = reduce_rows_kernel<RB, SHAPE, kRowRedStages, NT>;
   const size_t smem = (size_t)kRowRedStages * NT * kRingLineBytes + 1024;
   RFX_CUDA_TRY(allow_smem((const void*)k, smem));
@@ -243,14 +243,17 @@ rfx_status launch_rows(const void* rows, uint64_t n, RowReduceArgs& a, cudaStrea
   return RFX_OK;
 }
 
+// Variant 0: 256-line tiles, 1: 128-line tiles.
+template <int RB, int SHAPE>
+rfx_status launch_rows_v(int v, const void* rows, uint64_t n, RowReduceArgs& a, cudaStream_t s) {
+  return v == 0 ? launch_rows<RB, SHAPE, 256>(rows, n, a, s) : launch_rows<RB, SHAPE, 128>(rows, n, a, s);
+}
+
 rfx_status reduce_rows_staged(const void* rows, uint64_t n, const uint64_t* d_n, uint32_t row_bytes,
                               uint32_t key_shift, uint32_t value_shift, uint64_t val_mask, void* out_keys,
                               uint32_t out_key_bytes, int64_t* out_sums, uint32_t* out_counts, uint64_t* d_groups,
                               void* workspace, uint32_t* err, cudaStream_t s) {
   const RowLayout L = row_layout(workspace, n, row_bytes);
-  SegRecord* rec = L.records;
-  uint32_t* counter = L.counter;
-  RFX_CUDA_TRY(cudaMemsetAsync(workspace, 0, L.total, s));
   RowReduceArgs a;
   std::memset(&a, 0, sizeof(a));
   a.rows = static_cast<const uint8_t*>(rows);
@@ -264,18 +267,24 @@ rfx_status reduce_rows_staged(const void* rows, uint64_t n, const uint64_t* d_n,
   a.out_sums = out_sums;
   a.out_counts = out_counts;
   a.d_groups = d_groups;
-  a.records = rec;
-  a.tile_counter = counter;
+  a.records = L.records;
+  a.tile_counter = L.counter;
   a.err = err;
-  if (row_bytes == 16 && value_shift == 0 && val_mask == ~0ull && key_shift == 96)
-    return launch_rows<16, ROW16_K32_V64>(rows, n, a, s);
-  if (row_bytes == 16 && value_shift == 0 && val_mask == ~0ull && key_shift == 64)
-    return launch_rows<16, ROW16_K64_V64>(rows, n, a, s);
-  switch (row_bytes) {
-    case 4: return launch_rows<4, ROW_GENERIC>(rows, n, a, s);
-    case 8: return launch_rows<8, ROW_GENERIC>(rows, n, a, s);
-    default: return launch_rows<16, ROW_GENERIC>(rows, n, a, s);
-  }
+  const int shape = (row_bytes == 16 && value_shift == 0 && val_mask == ~0ull && key_shift == 96)   ? 1
+                    : (row_bytes == 16 && value_shift == 0 && val_mask == ~0ull && key_shift == 64) ? 2
+                                                                                                   : 0;
+  auto run = [&](int v) -> rfx_status {
+    RFX_CUDA_TRY(cudaMemsetAsync(workspace, 0, L.total, s));
+    if (shape == 1) return launch_rows_v<16, ROW16_K32_V64>(v, rows, n, a, s);
+    if (shape == 2) return launch_rows_v<16, ROW16_K64_V64>(v, rows, n, a, s);
+    switch (row_bytes) {
+      case 4: return launch_rows_v<4, ROW_GENERIC>(v, rows, n, a, s);
+      case 8: return launch_rows_v<8, ROW_GENERIC>(v, rows, n, a, s);
+      default: return launch_rows_v<16, ROW_GENERIC>(v, rows, n, a, s);
+    }
+  };
+  const uint64_t shape_key = ((uint64_t)row_bytes << 32) | ((uint64_t)shape << 24) | (key_shift << 8) | value_shift;
+  return run(tune_pick(TUNE_REDUCE_ROWS, shape_key, n, 2, run, s));
 }
 }  // namespace
 }  // namespace rfx

@@ -3,6 +3,7 @@
 #include <cstring>
 
 #include "scan_launch.cuh"
+#include "tune.h"
 
 namespace rfx {
 
@@ -10,7 +11,7 @@ rfx_status jit_aggregate(const ScanProgram& p, const void* in, uint64_t n, unsig
                          uint64_t* out_keys, int64_t* out_sums, uint64_t* out_counts, uint64_t* d_groups, uint32_t* err,
                          cudaStream_t stream);
 rfx_status jit_compact(const ScanProgram& p, int mode, const void* in, uint64_t n, void* out, uint64_t* d_count,
-                       uint64_t* status, uint32_t* counter, uint32_t* err, cudaStream_t stream, uint64_t tile_rows);
+                       uint64_t* status, uint32_t* counter, uint32_t* err, cudaStream_t stream, uint64_t tile_rows, int variant = 0);
 
 template <int W>
 rfx_status launch_compact(int, uint32_t, const ScanLaunch&);
@@ -75,10 +76,18 @@ rfx_status run_compact(int mode, const ScanProgram& p, void* out, uint64_t* d_co
   uint64_t* status = c.take<uint64_t>(tiles + 1);
   uint32_t* counter = c.take<uint32_t>(1);
   if (!ws || ws_bytes < c.used) return RFX_ERR_WORKSPACE;
-  RFX_CUDA_TRY(cudaMemsetAsync(ws, 0, c.used, s));
-  // the plan-specialised kernel when runtime compilation is available
-  rfx_status st = jit_compact(p, mode, in, n, out, d_count, status, counter, err, s, kScanTile);
+  // the plan-specialised kernel when runtime compilation is available; its rows per
+  // thread are tuned per plan shape and size class when tuning is on
+  const size_t clear = c.used;
+  auto run = [&](int v) -> rfx_status {
+    RFX_CUDA_TRY(cudaMemsetAsync(ws, 0, clear, s));
+    return jit_compact(p, mode, in, n, out, d_count, status, counter, err, s, kScanTile, v);
+  };
+  const uint64_t shape = ((uint64_t)p.in_bytes << 40) | ((uint64_t)(mode == 0 ? p.in_bytes : p.out_bytes) << 24) |
+                         ((uint64_t)mode << 16) | ((uint64_t)p.ncmp << 8) | p.ninstr;
+  rfx_status st = run(tune_pick(TUNE_SCAN_COMPACT, shape, n, 3, run, s));
   if (st != RFX_ERR_UNSUPPORTED) return st;
+  RFX_CUDA_TRY(cudaMemsetAsync(ws, 0, clear, s));
   ScanLaunch a{&p, in, n, out, d_count, status, counter, err, s};
   return dispatch_compact(p.in_bytes, mode, mode == 0 ? p.in_bytes : p.out_bytes, a);
 }

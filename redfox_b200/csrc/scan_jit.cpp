@@ -486,12 +486,16 @@ rfx_status jit_aggregate(const ScanProgram& p, const void* in, uint64_t n, unsig
 }
 
 rfx_status jit_compact(const ScanProgram& p, int mode, const void* in, uint64_t n, void* out, uint64_t* d_count,
-                       uint64_t* status, uint32_t* counter, uint32_t* err, cudaStream_t stream, uint64_t tile_rows) {
+                       uint64_t* status, uint32_t* counter, uint32_t* err, cudaStream_t stream, uint64_t tile_rows,
+                       int variant) {
   const uint32_t wout = mode == 0 ? p.in_bytes : p.out_bytes;
-  // rows per thread by row width (registers hold one tile's rows);
-  // tiles are never smaller than the workspace's tile_rows, so its status array suffices
+  // rows per thread by row width (registers hold one tile's rows), doubled by variant 1
+  // and halved by variant 2; tiles are never smaller than the workspace's tile_rows, so
+  // its status array suffices
   const uint32_t wmax = p.in_bytes > wout ? p.in_bytes : wout;
   int ipt = wmax >= 32 ? 2 : wmax >= 16 ? 4 : 8;
+  if (variant == 1 && ipt < 16) ipt *= 2;
+  if (variant == 2) ipt /= 2;
   if ((uint64_t)ipt * kJitThreads < tile_rows) ipt = (int)(tile_rows / kJitThreads);
   tile_rows = (uint64_t)ipt * kJitThreads;
   cudaKernel_t k;

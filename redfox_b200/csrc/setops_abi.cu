@@ -4,6 +4,7 @@
 
 #include "host_common.h"
 #include "setops_kernels.cuh"
+#include "tune.h"
 
 namespace rfx {
 namespace {
@@ -31,33 +32,47 @@ FilterLayout filter_layout(void* ws, uint64_t n) {
   return L;
 }
 
-template <int E>
-rfx_status launch_filter(int mode, SetFilterArgs& a, cudaStream_t s) {
-  const uint64_t tiles = (a.na + set_tile<E>() - 1) / set_tile<E>();
+template <int E, int IPT>
+rfx_status launch_filter_ipt(int mode, SetFilterArgs& a, cudaStream_t s) {
+  constexpr int TILE = kSetThreads * IPT;
+  const uint64_t tiles = (a.na + TILE - 1) / TILE;
   if (mode != KEEP_HEADS && tiles) {
     const uint64_t work = 3 * tiles * 32;   // one warp per search
     const int g = (int)((work + 255) / 256);
-    set_split_kernel<E><<<g, 256, 0, s>>>(a.a, a.na, a.b, a.nb, const_cast<uint64_t*>(a.split));
+    set_split_kernel<E, TILE><<<g, 256, 0, s>>>(a.a, a.na, a.b, a.nb, const_cast<uint64_t*>(a.split));
     RFX_CUDA_TRY(cudaGetLastError());
   }
-  const void* k = mode == KEEP_MATCHED ? (const void*)set_filter_kernel<E, KEEP_MATCHED>
-                : mode == KEEP_UNMATCHED ? (const void*)set_filter_kernel<E, KEEP_UNMATCHED>
-                                         : (const void*)set_filter_kernel<E, KEEP_HEADS>;
+  const void* k = mode == KEEP_MATCHED ? (const void*)set_filter_kernel<E, KEEP_MATCHED, IPT>
+                : mode == KEEP_UNMATCHED ? (const void*)set_filter_kernel<E, KEEP_UNMATCHED, IPT>
+                                         : (const void*)set_filter_kernel<E, KEEP_HEADS, IPT>;
   const int grid = persistent_grid(k, kSetThreads, 0, tiles ? tiles : 1);
-  if (mode == KEEP_MATCHED) set_filter_kernel<E, KEEP_MATCHED><<<grid, kSetThreads, 0, s>>>(a);
-  else if (mode == KEEP_UNMATCHED) set_filter_kernel<E, KEEP_UNMATCHED><<<grid, kSetThreads, 0, s>>>(a);
-  else set_filter_kernel<E, KEEP_HEADS><<<grid, kSetThreads, 0, s>>>(a);
+  if (mode == KEEP_MATCHED) set_filter_kernel<E, KEEP_MATCHED, IPT><<<grid, kSetThreads, 0, s>>>(a);
+  else if (mode == KEEP_UNMATCHED) set_filter_kernel<E, KEEP_UNMATCHED, IPT><<<grid, kSetThreads, 0, s>>>(a);
+  else set_filter_kernel<E, KEEP_HEADS, IPT><<<grid, kSetThreads, 0, s>>>(a);
   RFX_CUDA_TRY(cudaGetLastError());
   return RFX_OK;
 }
 
-rfx_status dispatch_filter(uint32_t e, int mode, SetFilterArgs& a, cudaStream_t s) {
+// Variant 0: 8 items per thread, 1: 4 (unique: always 8).  `clear` zeroes the look-back
+// status and tile counter before each launch.
+template <int E>
+rfx_status launch_filter(int mode, SetFilterArgs& a, cudaStream_t s, void* clear = nullptr, size_t clear_bytes = 0) {
+  auto run = [&](int v) -> rfx_status {
+    if (clear) RFX_CUDA_TRY(cudaMemsetAsync(clear, 0, clear_bytes, s));
+    return v == 0 || mode == KEEP_HEADS ? launch_filter_ipt<E, 8>(mode, a, s) : launch_filter_ipt<E, 4>(mode, a, s);
+  };
+  if (mode == KEEP_HEADS || !clear) return run(0);
+  return run(tune_pick(TUNE_SET_FILTER, ((uint64_t)E << 8) | (uint64_t)mode, a.na + a.nb, 2, run, s));
+}
+
+rfx_status dispatch_filter(uint32_t e, int mode, SetFilterArgs& a, cudaStream_t s, void* clear = nullptr,
+                           size_t clear_bytes = 0) {
   switch (e) {
-    case 1: return launch_filter<1>(mode, a, s);
-    case 2: return launch_filter<2>(mode, a, s);
-    case 4: return launch_filter<4>(mode, a, s);
-    case 8: return launch_filter<8>(mode, a, s);
-    case 16: return launch_filter<16>(mode, a, s);
+    case 1: return launch_filter<1>(mode, a, s, clear, clear_bytes);
+    case 2: return launch_filter<2>(mode, a, s, clear, clear_bytes);
+    case 4: return launch_filter<4>(mode, a, s, clear, clear_bytes);
+    case 8: return launch_filter<8>(mode, a, s, clear, clear_bytes);
+    case 16: return launch_filter<16>(mode, a, s, clear, clear_bytes);
     default: return RFX_ERR_UNSUPPORTED;
   }
 }
@@ -87,10 +102,10 @@ rfx_status dispatch_merge(uint32_t e, const void* a, uint64_t na, const void* d,
 
 template <int E>
 rfx_status launch_prev(const void* a, uint64_t n, void* prev, cudaStream_t s) {
-  const uint64_t tiles = (n + set_tile<E>() - 1) / set_tile<E>();
+  const uint64_t tiles = (n + kSetTile - 1) / kSetTile;
   const int grid = (int)((tiles + 255) / 256);
   tile_prev_kernel<E><<<grid ? grid : 1, 256, 0, s>>>(static_cast<const uint8_t*>(a), n, static_cast<uint8_t*>(prev),
-                                                      set_tile<E>());
+                                                      kSetTile);
   RFX_CUDA_TRY(cudaGetLastError());
   return RFX_OK;
 }
@@ -132,7 +147,6 @@ rfx_status set_op_impl(uint32_t op, void* out, uint64_t* d_count, const void* a,
   if (!ws || wsb < L.total) return RFX_ERR_WORKSPACE;
   uint32_t* err = device_error_word();
   if (!err) return RFX_ERR_CUDA;
-  RFX_CUDA_TRY(cudaMemsetAsync(ws, 0, L.f.clear, s));
   SetFilterArgs f;
   std::memset(&f, 0, sizeof(f));
   f.status = L.f.status;
@@ -146,7 +160,7 @@ rfx_status set_op_impl(uint32_t op, void* out, uint64_t* d_count, const void* a,
     f.nb = na;
     f.out = L.diff;
     f.d_count = L.d_nd;
-    rfx_status st = dispatch_filter(e, KEEP_UNMATCHED, f, s);
+    rfx_status st = dispatch_filter(e, KEEP_UNMATCHED, f, s, ws, L.f.clear);
     if (st != RFX_OK) return st;
     return dispatch_merge(e, a, na, L.diff, nb, L.d_nd, out, d_count, s);
   }
@@ -156,7 +170,7 @@ rfx_status set_op_impl(uint32_t op, void* out, uint64_t* d_count, const void* a,
   f.nb = nb;
   f.out = static_cast<uint8_t*>(out);
   f.d_count = d_count;
-  return dispatch_filter(e, op == RFX_SET_INTERSECTION ? KEEP_MATCHED : KEEP_UNMATCHED, f, s);
+  return dispatch_filter(e, op == RFX_SET_INTERSECTION ? KEEP_MATCHED : KEEP_UNMATCHED, f, s, ws, L.f.clear);
 }
 
 size_t unique_workspace_impl(uint64_t n, uint32_t e) {

@@ -18,13 +18,11 @@
 namespace rfx {
 
 constexpr int kSetThreads = 256;
-// Items per thread (8: 16 measured no faster for 4-byte keys); elements up to 8 bytes
-// live in 64-bit registers.
-template <int E>
-__host__ __device__ constexpr int set_ipt() { return 8; }
-template <int E>
-__host__ __device__ constexpr int set_tile() { return kSetThreads * set_ipt<E>(); }
-constexpr int kSetTileMin = kSetThreads * 8;   // the smallest tile: workspace sizing
+// Items per thread: 8 by default, 4 as the tuner's alternative (unique always 8);
+// elements up to 8 bytes live in 64-bit registers.
+constexpr int kSetIPT = 8;
+constexpr int kSetTile = kSetThreads * kSetIPT;
+constexpr int kSetTileMin = kSetThreads * 4;   // the smallest tile: workspace sizing
 constexpr int kMergeVT = 8;
 constexpr int kMergeTile = kSetThreads * kMergeVT;
 
@@ -84,11 +82,10 @@ __device__ __forceinline__ uint32_t smem_lower_strict(const T* w, uint32_t n, u1
   return lo;
 }
 
-template <int E, int MODE>
+template <int E, int MODE, int IPT>
 __global__ void __launch_bounds__(kSetThreads) set_filter_kernel(const SetFilterArgs p) {
   typedef typename std::conditional<(E <= 8), uint64_t, u128>::type WT;
-  constexpr int IPT = set_ipt<E>();
-  constexpr int TILE = set_tile<E>();
+  constexpr int TILE = kSetThreads * IPT;
   constexpr int WCAP = E <= 8 ? 2048 : 1024;
   __shared__ WT s_b[MODE == KEEP_HEADS ? 1 : WCAP];
   __shared__ uint64_t s_rs0, s_blo, s_bhi;
@@ -254,20 +251,20 @@ __device__ __forceinline__ uint64_t warp_search(const KeyView<E>& v, u128 k, uin
   return lo + __popc(__ballot_sync(0xffffffffu, before));
 }
 
-// Per tile of A (set_tile<E>() elements): the start of the run of equal values containing the
+// Per tile of A (TILE elements): the start of the run of equal values containing the
 // tile's first element, and the window of B that can equal the tile's values -- one warp
 // per search, all tiles at once, so the filter kernel's tiles do not each wait on chains
 // of dependent loads.
-template <int E>
+template <int E, int TILE>
 __global__ void set_split_kernel(const uint8_t* a, uint64_t na, const uint8_t* b, uint64_t nb, uint64_t* split) {
   const KeyView<E> A{a, na, 0};
   const KeyView<E> B{b, nb, 0};
-  const uint64_t tiles = (na + set_tile<E>() - 1) / set_tile<E>();
+  const uint64_t tiles = (na + TILE - 1) / TILE;
   const uint64_t warps = (uint64_t)gridDim.x * (blockDim.x / 32);
   for (uint64_t x = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) / 32; x < 3 * tiles; x += warps) {
     const uint64_t tile = x / 3, kind = x % 3;
-    const uint64_t tfirst = tile * set_tile<E>();
-    const uint64_t tlast = min(na, tfirst + set_tile<E>()) - 1;
+    const uint64_t tfirst = tile * TILE;
+    const uint64_t tlast = min(na, tfirst + TILE) - 1;
     uint64_t r;
     if (kind == 0) {
       const u128 k0 = A.key(tfirst);

@@ -522,3 +522,42 @@ def join_tuples_two_step(left, lvbits, right, rvbits, out_bytes, stream=None):
         _ptr(out), out_bytes, total, _ptr(left), left.shape[0], _width(left), _ptr(right), right.shape[0],
         _width(right), rvbits, _ptr(tj.ws), tj.wsb, _stream(stream)))
     return out[:total], total
+
+
+# ---------------------------------------------------------------- autotuning
+def _declare_tune():
+    LIB.rfx_tune_set.restype = None
+    LIB.rfx_tune_set.argtypes = [C.c_int]
+    LIB.rfx_tune_reset.restype = None
+    LIB.rfx_tune_reset.argtypes = []
+    LIB.rfx_tune_dump.restype = C.c_size_t
+    LIB.rfx_tune_dump.argtypes = [C.c_char_p, C.c_size_t]
+
+
+_declare_tune()
+
+TUNE_OPS = {1: "reduce_tuples", 2: "set_filter", 3: "select_compact"}
+
+
+def tune(mode=1):
+    """1: time each operator variant on first use per (shape, size class) and keep the
+    fastest; 0: run the defaults."""
+    LIB.rfx_tune_set(int(mode))
+
+
+def tune_reset():
+    LIB.rfx_tune_reset()
+
+
+def tune_table():
+    """The tuning decisions: list of dicts (op, shape, size_class, variant, ms per variant)."""
+    need = LIB.rfx_tune_dump(None, 0)
+    buf = C.create_string_buffer(need)
+    LIB.rfx_tune_dump(buf, need)
+    out = []
+    for line in buf.value.decode().splitlines():
+        kv = dict(p.split("=", 1) for p in line.split())
+        out.append({"op": TUNE_OPS.get(int(kv["op"]), kv["op"]), "shape": kv["shape"],
+                    "size_class": int(kv["class"]), "variant": int(kv["variant"]),
+                    "ms": [float(x) for x in kv["ms"].split(",") if x]})
+    return out

@@ -71,6 +71,37 @@ static __device__ __forceinline__ void st_relaxed_u64(u64* p, u64 v) {
 #define VAL_MASK ((1ull << 62) - 1)
 #define SPIN_LIMIT (1u << 22)
 // warp 0 of a tile: publish the aggregate, return the exclusive prefix (bounded waits)
+static __device__ __forceinline__ void lb_publish(u64* status, u32 tile, u64 agg) {
+  st_relaxed_u64(&status[tile], (tile == 0 ? FLAG_INC : FLAG_AGG) | (agg & VAL_MASK));
+}
+// Look-back of a tile whose aggregate was published earlier (lb_publish); whole warp.
+static __device__ __forceinline__ u64 lookback_resolve(u64* status, u32 tile, u64 agg, u32* err) {
+  const u32 lane = threadIdx.x & 31;
+  if (tile == 0) return 0;
+  u64 prefix = 0;
+  long long base = (long long)tile - 1;
+  u32 spins = 0;
+  while (true) {
+    const long long idx = base - (long long)lane;
+    const u64 s = idx >= 0 ? ld_relaxed_u64(&status[idx]) : FLAG_INC;
+    const u64 flag = s & ~VAL_MASK;
+    const unsigned not_ready = __ballot_sync(0xffffffffu, flag == 0);
+    const unsigned inc = __ballot_sync(0xffffffffu, flag == FLAG_INC);
+    const unsigned upto = inc ? ((inc & (0u - inc)) << 1) - 1 : 0xffffffffu;
+    if (not_ready & upto) {
+      if (++spins > SPIN_LIMIT) { raise_error(err, 4u); break; }
+      __nanosleep(spins < 64 ? 20 : 200);
+      continue;
+    }
+    u64 v = ((upto >> lane) & 1u) ? (s & VAL_MASK) : 0;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    prefix += v;
+    if (inc) break;
+    base -= 32;
+  }
+  if (lane == 0) st_relaxed_u64(&status[tile], FLAG_INC | ((prefix + agg) & VAL_MASK));
+  return prefix;
+}
 static __device__ __forceinline__ u64 lookback(u64* status, u32 tile, u64 agg, u32* err) {
   const u32 lane = threadIdx.x & 31;
   if (tile == 0) {
@@ -369,22 +400,29 @@ extern "C" __global__ void __launch_bounds__(NT) rfx_plan_compact(
 )RFX";
     return s.str();
   }
-  // Compaction: tiles claimed in order from a counter, kept rows ranked by warp ballots
-  // and a block scan, tile offsets by decoupled look-back.
+  // Compaction, one tile ahead: a block claims, loads and evaluates tile k+1, stages its
+  // kept rows (compacted, limb-major) in shared memory and publishes the tile's count
+  // before it resolves tile k's offset by look-back and writes tile k's staged rows out
+  // as one contiguous run.  No look-back stands between a claim and that tile's count,
+  // and a tile is resolved a whole step after its count was published, so predecessors
+  // have published theirs by then.
   s << R"RFX(
 extern "C" __global__ void __launch_bounds__(NT) rfx_plan_compact(
     const u8* __restrict__ in, u64 n, u8* __restrict__ out, u64* __restrict__ d_count,
     u64* __restrict__ status, u32* __restrict__ tile_counter, u32* err, const RfxConsts K) {
-  __shared__ u32 s_cnt[IPT][NT / 32];
+  extern __shared__ __align__(16) u64 sstage[];      // [2][NO][TILE]
+  __shared__ u32 s_cnt[2][IPT][NT / 32];
+  __shared__ u32 s_total[2];
+  __shared__ u32 s_tile[2];
   __shared__ u64 s_prefix;
-  __shared__ u32 s_tile;
   const u32 t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const u64 num_tiles = (n + TILE - 1) / TILE;
-  while (true) {
-    if (t == 0) s_tile = atomicAdd(tile_counter, 1u);
+  // claim, load, evaluate, rank and stage one tile into buffer b; publish its count
+  auto fill = [&](int b) -> u64 {
+    if (t == 0) s_tile[b] = atomicAdd(tile_counter, 1u);
     __syncthreads();
-    const u64 tile = s_tile;
-    if (tile >= num_tiles) break;
+    const u64 tile = s_tile[b];
+    if (tile >= num_tiles) return tile;
     u64 L[IPT][NL];
 #pragma unroll
     for (int j = 0; j < IPT; ++j) {
@@ -398,9 +436,9 @@ extern "C" __global__ void __launch_bounds__(NT) rfx_plan_compact(
     for (int j = 0; j < IPT; ++j) {
       const u64 i = tile * TILE + (u64)j * NT + t;
       sel[j] = i < n ? process(L[j], O[j], K) : false;
-      const unsigned b = __ballot_sync(0xffffffffu, sel[j]);
-      rank[j] = __popc(b & ((1u << lane) - 1u));
-      if (lane == 0) s_cnt[j][warp] = __popc(b);
+      const unsigned bal = __ballot_sync(0xffffffffu, sel[j]);
+      rank[j] = __popc(bal & ((1u << lane) - 1u));
+      if (lane == 0) s_cnt[b][j][warp] = __popc(bal);
     }
     __syncthreads();
     if (warp == 0) {
@@ -409,31 +447,57 @@ extern "C" __global__ void __launch_bounds__(NT) rfx_plan_compact(
       u32 total = 0;
       for (u32 c0 = 0; c0 < NC; c0 += 32) {
         const u32 idx = c0 + lane;
-        const u32 c = idx < NC ? s_cnt[idx / (NT / 32)][idx % (NT / 32)] : 0u;
+        const u32 c = idx < NC ? s_cnt[b][idx / (NT / 32)][idx % (NT / 32)] : 0u;
         u32 incl = c;
         for (int o = 1; o < 32; o <<= 1) {
           const u32 v = __shfl_up_sync(0xffffffffu, incl, o);
           if (lane >= (u32)o) incl += v;
         }
-        if (idx < NC) s_cnt[idx / (NT / 32)][idx % (NT / 32)] = total + incl - c;
+        if (idx < NC) s_cnt[b][idx / (NT / 32)][idx % (NT / 32)] = total + incl - c;
         total += __shfl_sync(0xffffffffu, incl, 31);
       }
-      const u64 prefix = lookback(status, (u32)tile, total, err);
+      if (lane == 0) {
+        s_total[b] = total;
+        lb_publish(status, (u32)tile, total);
+      }
+    }
+    __syncthreads();
+    u64* st = sstage + (size_t)b * NO * TILE;
+#pragma unroll
+    for (int j = 0; j < IPT; ++j) {
+      if (sel[j]) {
+        const u32 r = s_cnt[b][j][warp] + rank[j];
+#pragma unroll
+        for (int l = 0; l < NO; ++l) st[(size_t)l * TILE + r] = O[j][l];
+      }
+    }
+    return tile;
+  };
+  u64 tc = fill(0);
+  for (int b = 0; tc < num_tiles; b ^= 1) {
+    const u64 tn = fill(b ^ 1);
+    if (warp == 0) {
+      const u64 prefix = lookback_resolve(status, (u32)tc, s_total[b], err);
       if (lane == 0) {
         s_prefix = prefix;
-        if (tile == num_tiles - 1) *d_count = prefix + total;
+        if (tc == num_tiles - 1) *d_count = prefix + s_total[b];
       }
     }
     __syncthreads();
     const u64 base = s_prefix;
+    const u32 total = s_total[b];
+    const u64* st = sstage + (size_t)b * NO * TILE;
+    for (u32 r = t; r < total; r += NT) {
+      const u64 pos = base + r;
+      if (pos < n) {
+        u64 O1[NO];
 #pragma unroll
-    for (int j = 0; j < IPT; ++j) {
-      if (sel[j]) {
-        const u64 pos = base + s_cnt[j][warp] + rank[j];
-        if (pos < n) { )RFX" << store_code(wout, "O[j]", "pos") << R"RFX( }
+        for (int l = 0; l < NO; ++l) O1[l] = st[(size_t)l * TILE + r];
+        )RFX" << store_code(wout, "O1", "pos") << R"RFX(
       }
     }
     __syncthreads();
+    tc = tn;
   }
 }
 )RFX";
@@ -502,11 +566,14 @@ rfx_status jit_compact(const ScanProgram& p, int mode, const void* in, uint64_t 
   rfx_status st = jit_kernel(gen_compact(without_consts(p), mode, wout, ipt), "rfx_plan_compact", &k);
   if (st != RFX_OK) return st;
   const uint64_t tiles = (n + tile_rows - 1) / tile_rows;
-  const int grid = persistent_grid((const void*)k, kJitThreads, 0, tiles ? tiles : 1);
+  const uint32_t no = (wout + 7) / 8;
+  const size_t smem = mode == 2 ? 0 : 2ull * no * tile_rows * sizeof(uint64_t);
+  if (smem) RFX_CUDA_TRY(allow_smem((const void*)k, smem));
+  const int grid = persistent_grid((const void*)k, kJitThreads, smem, tiles ? tiles : 1);
   HostConsts kc = consts_of(p);
   void* args[] = {(void*)&in, (void*)&n, (void*)&out, (void*)&d_count, (void*)&status, (void*)&counter, (void*)&err,
                   (void*)&kc};
-  RFX_CUDA_TRY(cudaLaunchKernel((const void*)k, dim3(grid), dim3(kJitThreads), args, 0, stream));
+  RFX_CUDA_TRY(cudaLaunchKernel((const void*)k, dim3(grid), dim3(kJitThreads), args, smem, stream));
   return RFX_OK;
 }
 

@@ -400,14 +400,16 @@ extern "C" __global__ void __launch_bounds__(NT) rfx_plan_compact(
 )RFX";
     return s.str();
   }
-  // Compaction, one tile ahead: a block claims, loads and evaluates tile k+1, stages its
-  // kept rows (compacted, limb-major) in shared memory and publishes the tile's count
-  // before it resolves tile k's offset by look-back and writes tile k's staged rows out
-  // as one contiguous run.  No look-back stands between a claim and that tile's count,
-  // and a tile is resolved a whole step after its count was published, so predecessors
-  // have published theirs by then.
+  // Compaction, one tile ahead, with a look-back warp: the eight compute warps claim,
+  // load and evaluate tile k+1, stage its kept rows (compacted, limb-major) in shared
+  // memory and publish its count, while the ninth warp resolves tile k's offset by
+  // look-back; then all warps write tile k's staged rows out as one contiguous run.  No
+  // look-back stands between a claim and that tile's count, a tile is resolved a whole
+  // step after its count was published, and the look-back's L2 round trips overlap the
+  // next tile's loads.
   s << R"RFX(
-extern "C" __global__ void __launch_bounds__(NT) rfx_plan_compact(
+#define NTB (NT + 32)
+extern "C" __global__ void __launch_bounds__(NTB) rfx_plan_compact(
     const u8* __restrict__ in, u64 n, u8* __restrict__ out, u64* __restrict__ d_count,
     u64* __restrict__ status, u32* __restrict__ tile_counter, u32* err, const RfxConsts K) {
   extern __shared__ __align__(16) u64 sstage[];      // [2][NO][TILE]
@@ -417,12 +419,13 @@ extern "C" __global__ void __launch_bounds__(NT) rfx_plan_compact(
   __shared__ u64 s_prefix;
   const u32 t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const u64 num_tiles = (n + TILE - 1) / TILE;
-  // claim, load, evaluate, rank and stage one tile into buffer b; publish its count
-  auto fill = [&](int b) -> u64 {
+  // compute warps only (barrier 1 over NT threads): claim, load, evaluate, rank and
+  // stage one tile into buffer b; publish its count
+  auto fill = [&](int b) {
     if (t == 0) s_tile[b] = atomicAdd(tile_counter, 1u);
-    __syncthreads();
+    asm volatile("bar.sync 1, %0;" ::"n"(NT) : "memory");
     const u64 tile = s_tile[b];
-    if (tile >= num_tiles) return tile;
+    if (tile >= num_tiles) return;
     u64 L[IPT][NL];
 #pragma unroll
     for (int j = 0; j < IPT; ++j) {
@@ -440,7 +443,7 @@ extern "C" __global__ void __launch_bounds__(NT) rfx_plan_compact(
       rank[j] = __popc(bal & ((1u << lane) - 1u));
       if (lane == 0) s_cnt[b][j][warp] = __popc(bal);
     }
-    __syncthreads();
+    asm volatile("bar.sync 1, %0;" ::"n"(NT) : "memory");
     if (warp == 0) {
       // exclusive scan of the IPT x warps counts, 32 at a time
       const u32 NC = IPT * (NT / 32);
@@ -461,7 +464,7 @@ extern "C" __global__ void __launch_bounds__(NT) rfx_plan_compact(
         lb_publish(status, (u32)tile, total);
       }
     }
-    __syncthreads();
+    asm volatile("bar.sync 1, %0;" ::"n"(NT) : "memory");
     u64* st = sstage + (size_t)b * NO * TILE;
 #pragma unroll
     for (int j = 0; j < IPT; ++j) {
@@ -471,12 +474,14 @@ extern "C" __global__ void __launch_bounds__(NT) rfx_plan_compact(
         for (int l = 0; l < NO; ++l) st[(size_t)l * TILE + r] = O[j][l];
       }
     }
-    return tile;
   };
-  u64 tc = fill(0);
+  if (t < NT) fill(0);
+  __syncthreads();
+  u64 tc = s_tile[0];
   for (int b = 0; tc < num_tiles; b ^= 1) {
-    const u64 tn = fill(b ^ 1);
-    if (warp == 0) {
+    if (t < NT) {
+      fill(b ^ 1);
+    } else {
       const u64 prefix = lookback_resolve(status, (u32)tc, s_total[b], err);
       if (lane == 0) {
         s_prefix = prefix;
@@ -487,7 +492,7 @@ extern "C" __global__ void __launch_bounds__(NT) rfx_plan_compact(
     const u64 base = s_prefix;
     const u32 total = s_total[b];
     const u64* st = sstage + (size_t)b * NO * TILE;
-    for (u32 r = t; r < total; r += NT) {
+    for (u32 r = t; r < total; r += NTB) {
       const u64 pos = base + r;
       if (pos < n) {
         u64 O1[NO];
@@ -496,8 +501,8 @@ extern "C" __global__ void __launch_bounds__(NT) rfx_plan_compact(
         )RFX" << store_code(wout, "O1", "pos") << R"RFX(
       }
     }
+    tc = s_tile[b ^ 1];
     __syncthreads();
-    tc = tn;
   }
 }
 )RFX";
@@ -569,11 +574,12 @@ rfx_status jit_compact(const ScanProgram& p, int mode, const void* in, uint64_t 
   const uint32_t no = (wout + 7) / 8;
   const size_t smem = mode == 2 ? 0 : 2ull * no * tile_rows * sizeof(uint64_t);
   if (smem) RFX_CUDA_TRY(allow_smem((const void*)k, smem));
-  const int grid = persistent_grid((const void*)k, kJitThreads, smem, tiles ? tiles : 1);
+  const int threads = mode == 2 ? kJitThreads : kJitThreads + 32;   // + the look-back warp
+  const int grid = persistent_grid((const void*)k, threads, smem, tiles ? tiles : 1);
   HostConsts kc = consts_of(p);
   void* args[] = {(void*)&in, (void*)&n, (void*)&out, (void*)&d_count, (void*)&status, (void*)&counter, (void*)&err,
                   (void*)&kc};
-  RFX_CUDA_TRY(cudaLaunchKernel((const void*)k, dim3(grid), dim3(kJitThreads), args, smem, stream));
+  RFX_CUDA_TRY(cudaLaunchKernel((const void*)k, dim3(grid), dim3(threads), args, smem, stream));
   return RFX_OK;
 }
 

@@ -359,7 +359,8 @@ rfx_status rfx_gen_uniform_rows(void* out, uint64_t n, const rfx_tuple* type, ui
  * No counterpart in the reference (its kernels have fixed launch shapes).  Operators with
  * several compiled variants (the TMA-staged rfx_reduce_tuples: 256- or 128-line tiles; the
  * set filters behind rfx_set_op: 8 or 4 items per thread; the plan-specialised rfx_select /
- * rfx_select_project: items per thread) run their default unless tuning is on.  With
+ * rfx_select_project: items per thread; the plan-specialised rfx_filter_aggregate: rows per
+ * thread per iteration) run their default unless tuning is on.  With
  * mode 1 (or RFX_TUNE=1 in the environment) the first call of each (operator, shape, size
  * class of 4x in n) times every variant on the caller's inputs and stream (CUDA events,
  * best of three after one untimed run, synchronising the stream) and later calls of that

@@ -9,7 +9,7 @@ namespace rfx {
 
 rfx_status jit_aggregate(const ScanProgram& p, const void* in, uint64_t n, unsigned long long* gacc, uint32_t* done,
                          uint64_t* out_keys, int64_t* out_sums, uint64_t* out_counts, uint64_t* d_groups, uint32_t* err,
-                         cudaStream_t stream);
+                         cudaStream_t stream, int variant = 0);
 rfx_status jit_compact(const ScanProgram& p, int mode, const void* in, uint64_t n, void* out, uint64_t* d_count,
                        uint64_t* status, uint32_t* counter, uint32_t* err, cudaStream_t stream, uint64_t tile_rows, int variant = 0);
 
@@ -202,9 +202,18 @@ extern "C" rfx_status rfx_filter_aggregate(const void* in, uint64_t n, const rfx
   unsigned long long* gacc = c.take<unsigned long long>((size_t)p.ngroups_total * (nsum + 1));
   uint32_t* done = c.take<uint32_t>(1);
   if (!workspace || workspace_bytes < c.used) return RFX_ERR_WORKSPACE;
-  RFX_CUDA_TRY(cudaMemsetAsync(workspace, 0, c.used, s));
-  st = jit_aggregate(p, in, n, gacc, done, out_keys, out_sums, out_counts, d_groups, err, s);
+  // the plan-specialised kernel (rows per thread per iteration tuned per plan shape and
+  // size class when tuning is on), else the interpreting kernel
+  const size_t clear = c.used;
+  auto run = [&](int v) -> rfx_status {
+    RFX_CUDA_TRY(cudaMemsetAsync(workspace, 0, clear, s));
+    return jit_aggregate(p, in, n, gacc, done, out_keys, out_sums, out_counts, d_groups, err, s, v);
+  };
+  const uint64_t shape = ((uint64_t)p.in_bytes << 40) | ((uint64_t)p.ngroups_total << 16) | ((uint64_t)nsum << 8) |
+                         p.ncmp;
+  st = run(tune_pick(TUNE_SCAN_AGGREGATE, shape, n, 3, run, s));
   if (st != RFX_ERR_UNSUPPORTED) return st;
+  RFX_CUDA_TRY(cudaMemsetAsync(workspace, 0, clear, s));
   AggLaunch a{&p, in, n, gacc, done, out_keys, out_sums, out_counts, d_groups, err, s};
   return dispatch_aggregate(p.in_bytes, a);
 }

@@ -21,6 +21,7 @@ enum TuneOp : uint32_t {
   TUNE_REDUCE_ROWS = 1,   // rfx_reduce_tuples, TMA-staged: 256- or 128-line tiles
   TUNE_SET_FILTER = 2,    // set intersection / difference / union's B - A: 8 or 4 items per thread
   TUNE_SCAN_COMPACT = 3,  // plan-specialised select / project: items per thread
+  TUNE_SCAN_AGGREGATE = 4,  // plan-specialised filter-aggregate: rows per thread per iteration
 };
 
 // Size class of n: floor(log2(n)) / 2 (classes of 4x).

@@ -536,7 +536,7 @@ def _declare_tune():
 
 _declare_tune()
 
-TUNE_OPS = {1: "reduce_tuples", 2: "set_filter", 3: "select_compact"}
+TUNE_OPS = {1: "reduce_tuples", 2: "set_filter", 3: "select_compact", 4: "filter_aggregate"}
 
 
 def tune(mode=1):

@@ -146,24 +146,34 @@ sort_histogram_kernel(const uint8_t* __restrict__ keys, uint64_t n, uint32_t beg
   const uint32_t t = threadIdx.x, lane = t & 31;
   for (uint32_t k = t; k < passes * kRadix; k += kSortThreads) (&h[0][0])[k] = 0;
   __syncthreads();
+  // R elements per thread per iteration, all loaded before any is counted (a read-only
+  // stream needs several loads in flight per thread to approach HBM bandwidth)
+  constexpr int R = K <= 16 ? 4 : 2;
   const uint64_t stride = (uint64_t)gridDim.x * kSortThreads;
-  const uint64_t nround = (n + stride - 1) / stride * stride;  // whole warps stay converged
-  for (uint64_t i = (uint64_t)blockIdx.x * kSortThreads + t; i < nround; i += stride) {
-    const bool valid = i < n;
-    Elem<K> e;
-    if (valid) e = load_elem<K>(keys, i);
-    const unsigned vmask = __ballot_sync(0xffffffffu, valid);
-    for (uint32_t p = 0; p < passes; ++p) {
-      const uint32_t shift = begin_bit + 8 * p;
-      const uint32_t w = end_bit - shift < 8 ? end_bit - shift : 8;
-      const uint32_t d = valid ? (elem_bits<K>(e, shift) & ((1u << w) - 1)) : kRadix;
-      // a digit shared by the whole warp (constant high digits) is one add, not 32
-      // conflicting atomics; otherwise plain shared atomics
-      const uint32_t d0 = __shfl_sync(0xffffffffu, d, 0);
-      if (__all_sync(0xffffffffu, d == d0 || !valid) && vmask == 0xffffffffu) {
-        if (lane == 0) atomicAdd(&h[p][d0], 32u);
-      } else if (valid) {
-        atomicAdd(&h[p][d], 1u);
+  const uint64_t nround = (n + R * stride - 1) / (R * stride) * (R * stride);  // warps stay converged
+  for (uint64_t i0 = (uint64_t)blockIdx.x * kSortThreads + t; i0 < nround; i0 += R * stride) {
+    Elem<K> e[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const uint64_t i = i0 + (uint64_t)r * stride;
+      if (i < n) e[r] = load_elem<K>(keys, i);
+    }
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const bool valid = i0 + (uint64_t)r * stride < n;
+      const unsigned vmask = __ballot_sync(0xffffffffu, valid);
+      for (uint32_t p = 0; p < passes; ++p) {
+        const uint32_t shift = begin_bit + 8 * p;
+        const uint32_t w = end_bit - shift < 8 ? end_bit - shift : 8;
+        const uint32_t d = valid ? (elem_bits<K>(e[r], shift) & ((1u << w) - 1)) : kRadix;
+        // a digit shared by the whole warp (constant high digits) is one add, not 32
+        // conflicting atomics; otherwise plain shared atomics
+        const uint32_t d0 = __shfl_sync(0xffffffffu, d, 0);
+        if (__all_sync(0xffffffffu, d == d0 || !valid) && vmask == 0xffffffffu) {
+          if (lane == 0) atomicAdd(&h[p][d0], 32u);
+        } else if (valid) {
+          atomicAdd(&h[p][d], 1u);
+        }
       }
     }
   }

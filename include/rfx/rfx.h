@@ -371,6 +371,30 @@ void rfx_tune_reset(void);
  * returns the bytes needed (including the terminating 0); writes at most cap bytes. */
 size_t rfx_tune_dump(char* buf, size_t cap);
 
+/* ---------------------------------------------------------------- plan executor
+ * The part of Harmony's runtime that runs an RA plan's kernel sequence
+ * (harmony/runtime/implementation/Runtime.cpp:295-445): variables allocated at their
+ * first definition and freed after their last use, output sizes read back where the next
+ * operator is sized by them, inputs loaded from packed relation files
+ * (Runtime.cpp:191-206) or bound to caller memory -- with a JSON plan instead of the HIR
+ * protobuf (the grammar is in redfox_b200/csrc/exec.cpp).  Device memory comes from the
+ * stream-ordered allocator and is held within `budget_bytes` (0: no limit); an operator
+ * that would exceed it fails with RFX_ERR_CAPACITY.  No counterpart in the C ABI of the
+ * reference (its runtime called the kernel library). */
+typedef struct rfx_exec rfx_exec;
+rfx_status rfx_exec_create(rfx_exec** out, const char* plan_json, uint64_t budget_bytes, char* err,
+                           size_t err_cap);
+void rfx_exec_destroy(rfx_exec* exec);
+rfx_status rfx_exec_bind(rfx_exec* exec, const char* name, void* device_ptr, uint64_t bytes);
+rfx_status rfx_exec_load(rfx_exec* exec, const char* name, const char* path, void* stream);
+rfx_status rfx_exec_run(rfx_exec* exec, void* stream);
+rfx_status rfx_exec_output(rfx_exec* exec, const char* name, void** device_ptr, uint64_t* rows,
+                           uint32_t* row_bytes);
+rfx_status rfx_exec_stats(rfx_exec* exec, uint64_t* in_use, uint64_t* peak, uint64_t* ops, char* err,
+                          size_t err_cap);
+/* Copies a variable's rows (after a run) to caller device memory of cap_bytes. */
+rfx_status rfx_exec_copy_out(rfx_exec* exec, const char* name, void* dst, uint64_t cap_bytes, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

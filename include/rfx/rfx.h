@@ -329,6 +329,41 @@ rfx_status rfx_intersection_compat(void* result, uint64_t* size, void* lbegin, v
                                    void* rbegin, void* rend, uint32_t type);
 rfx_status rfx_unique_compat(void* begin, uint64_t* size, uint64_t type);
 
+/* ---------------------------------------------------------------- string keys */
+/* A string column is n 64-bit device pointers to NUL-terminated strings.  Order is the
+ * reference's compare_sort_string / compare_string2 (ModernGPUSort.cu:44-67,
+ * ModernGPUJoin.cu:72-98): lexicographic on signed char, a proper prefix first.  Equality
+ * is compare_string's (Reduce.cu:30-51): the same characters.  No string is read past its
+ * terminator.  n < 2^30. */
+
+/* Dictionary codes of a string column: codes[i] = the rank of element i's string among
+ * the column's distinct strings (may be NULL), perm[k] = the element at position k of the
+ * stable sorted order (may be NULL), *ndistinct (host; may be NULL) = distinct strings.
+ * Returns after `stream` has drained. */
+rfx_status rfx_string_codes(const void* ptrs, uint64_t n, uint32_t* codes, uint32_t* perm,
+                            uint64_t* ndistinct, void* stream);
+
+/* redfox::sort_string_key / sort_string_pair (ModernGPUSort.cu:148-470) and
+ * redfox::sort_string (Sort.cu:176-195): stable sort of the pointer column by string,
+ * values (value_type I8..I512; 0 = none) moved with their keys.  Synchronous on the
+ * default stream. */
+rfx_status rfx_sort_string_compat(void* keys, void* values, uint64_t n, uint64_t value_type);
+
+/* redfox::find_bounds_string (ModernGPUJoin.cu:213-300): both columns sorted by string;
+ * lower bounds, the exclusive scan of equal-string counts and *result_size (device) as
+ * rfx_find_bounds_compat. */
+rfx_status rfx_find_bounds_string_compat(int32_t* lower_bound, int32_t* left_count,
+                                         uint64_t* result_size, const void* left_key,
+                                         uint64_t left_size, const void* right_key,
+                                         uint64_t right_size);
+
+/* redfox::count_string / total_string_32 (Reduce.cu:424-480, :665-740): runs of
+ * consecutive equal strings, per run its first key pointer and the u32 sum of its values;
+ * *key_size / *value_size are device-resident byte counts (in and out). */
+rfx_status rfx_count_string_compat(const void* key_begin, const void* value_begin,
+                                   void* result_key_begin, void* result_value_begin,
+                                   uint64_t* key_size, uint64_t* value_size);
+
 /* rfx_filter_aggregate for callers that cannot allocate device memory when they call it:
  * a runtime that has already handed all device memory out by liveness, code recording a
  * stream capture, or a request path that must not touch the allocator.  It has no

@@ -94,6 +94,10 @@ def _declare(L):
         "orc_arith_rows": (C.c_int, [P, P, sz, P, P]),
         "orc_project": (None, [P, P, sz, P, P, P]),
         "orc_filter_aggregate": (i64, [P, sz, P, P, u32, P, u32, P, u32, P, u32, P, P, P, u64, C.c_int]),
+        "orc_str_sort": (None, [P, P, sz, P, u32]),
+        "orc_str_find_bounds": (None, [P, P, P, P, P, sz, P, sz]),
+        "orc_str_count": (u64, [P, P, sz, P, P, P]),
+        "orc_str_codes": (u64, [P, P, sz, P]),
         "orc_rand": (u64, [u64, u64, u64]),
         "orc_uniform": (u64, [u64, u64, u64, u64, u64]),
         "orc_gen_uniform_u64": (None, [P, sz, u64, u64, u64, u64, C.c_int]),
@@ -217,6 +221,57 @@ def reduce_count(keys, vals=None):
     v = None if vals is None else np.ascontiguousarray(vals, np.uint32)
     g = lib().orc_reduce_count(_p(keys), n, kb, _p(v), _p(ok), _p(oc))
     return ok[:g], oc[:g]
+
+
+# ---------------------------------------------------------------- string keys
+def str_pool(strings):
+    """(pool, offs): the byte strings (no NUL inside) NUL-terminated back to back in one
+    uint8 array, and their uint64 offsets -- a string column, offsets standing for the
+    reference's pointers."""
+    lens = np.fromiter((len(x) + 1 for x in strings), dtype=np.uint64, count=len(strings))
+    offs = np.zeros(len(strings), dtype=np.uint64)
+    if len(strings) > 1:
+        np.cumsum(lens[:-1], out=offs[1:])
+    pool = np.frombuffer(b"".join(x + b"\0" for x in strings) or b"\0", dtype=np.uint8).copy()
+    return pool, offs
+
+
+def str_sort(pool, offs, vals=None):
+    """Stable sort of a string column (sort_string_key / sort_string_pair); returns the
+    sorted offsets (and values)."""
+    o = np.ascontiguousarray(offs, np.uint64).copy()
+    v = None if vals is None else np.ascontiguousarray(vals).copy()
+    vb = 0 if v is None else v.dtype.itemsize * (1 if v.ndim == 1 else v.shape[1])
+    lib().orc_str_sort(_p(pool), _p(o), o.shape[0], _p(v), vb)
+    return o if v is None else (o, v)
+
+
+def str_find_bounds(pool, loffs, roffs):
+    lo = np.ascontiguousarray(loffs, np.uint64)
+    ro = np.ascontiguousarray(roffs, np.uint64)
+    lb = np.zeros(lo.shape[0], np.int32)
+    sc = np.zeros(lo.shape[0], np.int32)
+    tot = np.zeros(1, np.uint64)
+    lib().orc_str_find_bounds(_p(lb), _p(sc), _p(tot), _p(pool), _p(lo), lo.shape[0], _p(ro), ro.shape[0])
+    return lb, sc, int(tot[0])
+
+
+def str_count(pool, offs, vals):
+    """count_string: (first offset of each run of equal strings, u32 sums)."""
+    o = np.ascontiguousarray(offs, np.uint64)
+    v = np.ascontiguousarray(vals, np.uint32)
+    oo = np.zeros(o.shape[0], np.uint64)
+    os_ = np.zeros(o.shape[0], np.uint32)
+    g = lib().orc_str_count(_p(pool), _p(o), o.shape[0], _p(v), _p(oo), _p(os_))
+    return oo[:g], os_[:g]
+
+
+def str_codes(pool, offs):
+    """(codes, distinct): the rank of each string among the column's distinct strings."""
+    o = np.ascontiguousarray(offs, np.uint64)
+    c = np.zeros(o.shape[0], np.uint32)
+    d = lib().orc_str_codes(_p(pool), _p(o), o.shape[0], _p(c))
+    return c, int(d)
 
 
 # ---------------------------------------------------------------- set ops

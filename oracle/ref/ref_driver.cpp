@@ -158,6 +158,14 @@ REF_REDUCE(count_32, 4, 4)
 REF_REDUCE(count_128, 16, 4)
 REF_REDUCE(total_64_32, 8, 4)
 
+/* ---- string keys: columns of pointers to NUL-terminated strings (host pointers here) ---- */
+REF_REDUCE(count_string, 8, 4)
+REF_REDUCE(total_string_32, 8, 4)
+extern "C" void ref_sort_string(uint64_t* keys, size_t n)
+{
+    redfox::sort_string(keys, keys + n);
+}
+
 /* thrust::reduce_by_key with plus<long long>: the algorithm of every Reduce.cu entry,
  * at the int64 value type the build adds (the reference has only double / u32 sums). */
 extern "C" uint64_t ref_reduce_sum_i64_u32(const uint32_t* k, const int64_t* v, uint32_t* ok, int64_t* ov, size_t n)

@@ -865,3 +865,129 @@ void orc_gen_zipf_u64(uint64_t* out, size_t n, uint64_t seed, uint64_t stream,
         out[i] = lo < domain ? lo : domain - 1;
     }
 }
+
+/* ------------------------------------------------------------------------------------
+ * String keys.  A column is offsets into one pool of NUL-terminated strings (the
+ * reference's columns are device pointers to such strings).
+ * ----------------------------------------------------------------------------------*/
+
+/* compare_sort_string (ModernGPUSort.cu:44-67) = compare_string2 (ModernGPUJoin.cu:72-98):
+ * walk while both strings continue; the first differing char decides (as signed char);
+ * else a is less exactly when it ended and b did not. */
+int orc_str_less(const char* a, const char* b)
+{
+    size_t i = 0;
+    while (a[i] != 0 && b[i] != 0) {
+        if (a[i] != b[i]) return (signed char)a[i] < (signed char)b[i];
+        ++i;
+    }
+    return a[i] == 0 && b[i] != 0;
+}
+
+/* compare_string (Reduce.cu:30-51): equal when both end at the same place with the same
+ * characters before it. */
+int orc_str_equal(const char* a, const char* b)
+{
+    size_t i = 0;
+    while (a[i] != 0 && b[i] != 0) {
+        if (a[i] != b[i]) return 0;
+        ++i;
+    }
+    return a[i] == 0 && b[i] == 0;
+}
+
+typedef struct { const char* s; size_t idx; } str_item;
+
+static int str_item_cmp(const void* x, const void* y)
+{
+    const str_item* a = (const str_item*)x;
+    const str_item* b = (const str_item*)y;
+    if (orc_str_less(a->s, b->s)) return -1;
+    if (orc_str_less(b->s, a->s)) return 1;
+    return a->idx < b->idx ? -1 : (a->idx > b->idx);   /* stable */
+}
+
+/* sort_string_key / sort_string_pair (ModernGPUSort.cu:148-470): MergesortKeys /
+ * MergesortPairs with compare_sort_string -- a stable sort, equal strings keep their input
+ * order; values of vbytes (0 = none) move with their keys. */
+void orc_str_sort(const char* pool, uint64_t* offs, size_t n, void* vals, uint32_t vbytes)
+{
+    if (n == 0) return;
+    str_item* it = (str_item*)malloc(n * sizeof(str_item));
+    for (size_t i = 0; i < n; ++i) { it[i].s = pool + offs[i]; it[i].idx = i; }
+    qsort(it, n, sizeof(str_item), str_item_cmp);
+    uint64_t* o2 = (uint64_t*)malloc(n * sizeof(uint64_t));
+    uint8_t* v2 = vbytes ? (uint8_t*)malloc(n * vbytes) : NULL;
+    for (size_t k = 0; k < n; ++k) {
+        o2[k] = offs[it[k].idx];
+        if (vbytes) memcpy(v2 + k * vbytes, (const uint8_t*)vals + it[k].idx * vbytes, vbytes);
+    }
+    memcpy(offs, o2, n * sizeof(uint64_t));
+    if (vbytes) memcpy(vals, v2, n * vbytes);
+    free(v2);
+    free(o2);
+    free(it);
+}
+
+/* find_bounds_string (ModernGPUJoin.cu:213-300): SortedSearch lower bounds of each left
+ * string in the right column and SortedEqualityCount under compare_string2, then the
+ * exclusive scan of the counts (mgpu::Scan) and its total. */
+void orc_str_find_bounds(int32_t* lb, int32_t* cnt, uint64_t* total, const char* pool,
+                         const uint64_t* loffs, size_t nl, const uint64_t* roffs, size_t nr)
+{
+    uint64_t run = 0;
+    for (size_t i = 0; i < nl; ++i) {
+        const char* key = pool + loffs[i];
+        size_t lo = 0, hi = nr;
+        while (lo < hi) {   /* first right string not less than key */
+            size_t mid = lo + (hi - lo) / 2;
+            if (orc_str_less(pool + roffs[mid], key)) lo = mid + 1; else hi = mid;
+        }
+        size_t a = lo;
+        hi = nr;
+        while (lo < hi) {   /* first right string greater than key */
+            size_t mid = lo + (hi - lo) / 2;
+            if (!orc_str_less(key, pool + roffs[mid])) lo = mid + 1; else hi = mid;
+        }
+        lb[i] = (int32_t)a;
+        cnt[i] = (int32_t)(uint32_t)run;
+        run += lo - a;
+    }
+    *total = run;
+}
+
+/* count_string / total_string_32 (Reduce.cu:424-480, :665-740): thrust::reduce_by_key
+ * with compare_string and plus<unsigned>: runs of consecutive equal strings, each
+ * reported by its first key and the u32 sum of its values. */
+uint64_t orc_str_count(const char* pool, const uint64_t* offs, size_t n, const uint32_t* vals,
+                       uint64_t* out_offs, uint32_t* out_sums)
+{
+    uint64_t g = 0;
+    size_t i = 0;
+    while (i < n) {
+        uint32_t s = 0;
+        size_t j = i;
+        while (j < n && orc_str_equal(pool + offs[i], pool + offs[j])) s += vals[j++];
+        out_offs[g] = offs[i];
+        out_sums[g++] = s;
+        i = j;
+    }
+    return g;
+}
+
+/* Dense codes: codes[i] = the number of distinct strings of the column less than string
+ * i (the order of orc_str_less).  Returns the number of distinct strings. */
+uint64_t orc_str_codes(const char* pool, const uint64_t* offs, size_t n, uint32_t* codes)
+{
+    if (n == 0) return 0;
+    str_item* it = (str_item*)malloc(n * sizeof(str_item));
+    for (size_t i = 0; i < n; ++i) { it[i].s = pool + offs[i]; it[i].idx = i; }
+    qsort(it, n, sizeof(str_item), str_item_cmp);
+    uint64_t code = 0;
+    for (size_t k = 0; k < n; ++k) {
+        if (k > 0 && orc_str_less(it[k - 1].s, it[k].s)) ++code;
+        codes[it[k].idx] = (uint32_t)code;
+    }
+    free(it);
+    return code + 1;
+}

@@ -145,6 +145,17 @@ void orc_zipf_cdf(double* cdf, size_t n, double s);
 void orc_gen_zipf_u64(uint64_t* out, size_t n, uint64_t seed, uint64_t stream,
                       const double* cdf, size_t domain, int threads);
 
+/* ---- string keys: string i of a column is the NUL-terminated text at pool + offs[i]
+ * (the reference passes device pointers; offsets into one pool stand for them) ---- */
+int orc_str_less(const char* a, const char* b);
+int orc_str_equal(const char* a, const char* b);
+void orc_str_sort(const char* pool, uint64_t* offs, size_t n, void* vals, uint32_t vbytes);
+void orc_str_find_bounds(int32_t* lb, int32_t* cnt, uint64_t* total, const char* pool,
+                         const uint64_t* loffs, size_t nl, const uint64_t* roffs, size_t nr);
+uint64_t orc_str_count(const char* pool, const uint64_t* offs, size_t n, const uint32_t* vals,
+                       uint64_t* out_offs, uint32_t* out_sums);
+uint64_t orc_str_codes(const char* pool, const uint64_t* offs, size_t n, uint32_t* codes);
+
 #ifdef __cplusplus
 }
 #endif

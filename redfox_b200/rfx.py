@@ -561,3 +561,80 @@ def tune_table():
                     "size_class": int(kv["class"]), "variant": int(kv["variant"]),
                     "ms": [float(x) for x in kv["ms"].split(",") if x]})
     return out
+
+
+# ---------------------------------------------------------------------------- string keys
+def _declare_strings():
+    P, u64, st = C.c_void_p, C.c_uint64, C.c_int
+    more = {
+        "rfx_string_codes": (st, [P, u64, P, P, P, P]),
+        "rfx_sort_string_compat": (st, [P, P, u64, u64]),
+        "rfx_find_bounds_string_compat": (st, [P, P, P, P, u64, P, u64]),
+        "rfx_count_string_compat": (st, [P, P, P, P, P, P]),
+    }
+    for name, (res, args) in more.items():
+        f = getattr(LIB, name)
+        f.restype = res
+        f.argtypes = args
+
+
+_declare_strings()
+
+
+def string_column(pool, offs, device="cuda"):
+    """A host string column (uint8 pool of NUL-terminated strings, uint64 offsets) on the
+    device: (dpool, ptrs), ptrs an int64 tensor of the strings' device addresses.  The
+    column lives as long as dpool does."""
+    import numpy as np
+    import torch
+    dpool = torch.from_numpy(np.ascontiguousarray(pool, np.uint8)).to(device)
+    ptrs = torch.from_numpy(np.ascontiguousarray(offs, np.uint64).view(np.int64)).to(device) + dpool.data_ptr()
+    return dpool, ptrs
+
+
+def string_codes(ptrs, stream=None):
+    """(codes, perm, distinct): per element the rank of its string among the distinct
+    strings, the stable sorted order, and the number of distinct strings (int32 tensors
+    holding u32 values)."""
+    import torch
+    n = ptrs.shape[0]
+    codes = torch.empty(n, dtype=torch.int32, device=ptrs.device)
+    perm = torch.empty(n, dtype=torch.int32, device=ptrs.device)
+    d = C.c_uint64(0)
+    check("rfx_string_codes", LIB.rfx_string_codes(_ptr(ptrs), n, _ptr(codes), _ptr(perm), C.byref(d),
+                                                   _stream(stream)))
+    return codes, perm, d.value
+
+
+def sort_strings(ptrs, values=None, value_type=0):
+    """sort_string_key / sort_string_pair in place (values: value_type a DataType code)."""
+    check("rfx_sort_string_compat", LIB.rfx_sort_string_compat(_ptr(ptrs), _ptr(values), ptrs.shape[0],
+                                                               value_type))
+
+
+def find_bounds_string(left, right):
+    """find_bounds_string: (lower_bound, left_count scan, total) over sorted pointer columns."""
+    import torch
+    nl = left.shape[0]
+    lb = torch.empty(nl, dtype=torch.int32, device=left.device)
+    sc = torch.empty(nl, dtype=torch.int32, device=left.device)
+    tot = torch.zeros(1, dtype=torch.int64, device=left.device)
+    check("rfx_find_bounds_string_compat",
+          LIB.rfx_find_bounds_string_compat(_ptr(lb), _ptr(sc), _ptr(tot), _ptr(left), nl, _ptr(right),
+                                            right.shape[0]))
+    return lb, sc, int(tot.item())
+
+
+def count_string(ptrs, values):
+    """count_string: (first pointer of each run of equal strings, u32 sums as int32)."""
+    import torch
+    n = ptrs.shape[0]
+    ok = torch.empty(max(n, 1), dtype=torch.int64, device=ptrs.device)
+    ov = torch.empty(max(n, 1), dtype=torch.int32, device=ptrs.device)
+    ks = torch.tensor([8 * n], dtype=torch.int64, device=ptrs.device)
+    vs = torch.tensor([4 * n], dtype=torch.int64, device=ptrs.device)
+    check("rfx_count_string_compat", LIB.rfx_count_string_compat(_ptr(ptrs), _ptr(values), _ptr(ok), _ptr(ov),
+                                                                 _ptr(ks), _ptr(vs)))
+    g = int(ks.item()) // 8
+    assert int(vs.item()) // 4 == g
+    return ok[:g], ov[:g]

@@ -1,7 +1,7 @@
 // redfox_ra.cpp -- libredfox_ra.so: the reference's redfox:: entry points for joins,
 // reductions and set operations, with its C++ linkage and signatures
-// (redfox/ra/interface/ModernGPUJoin.h:15-41, Reduce.h:43-83 and :132-137, Union.h:13,
-// Difference.h:13, Unique.h:15), each forwarding to the rfx_*_compat entry of librfx.so
+// (redfox/ra/interface/ModernGPUJoin.h:15-41, Reduce.h:43-83 and :132-144, Union.h:13,
+// Difference.h:13, Unique.h:15, Sort.h:15-17), each forwarding to the rfx_*_compat entry of librfx.so
 // that keeps the reference's argument meaning (element counts for find_bounds / join, byte
 // counts for reduce / count / set operations, device-resident result sizes, synchronous
 // on the default stream).  A generated extern "C" wrapper of the reference links against
@@ -73,6 +73,47 @@ void difference(void* result, unsigned long long int* size, void* lbegin, void* 
 
 void unique(void* begin, unsigned long long int* size, unsigned long long int type) {
   report("unique", rfx_unique_compat(begin, reinterpret_cast<uint64_t*>(size), type));
+}
+
+// string keys: columns of device pointers to NUL-terminated strings
+void find_bounds_string(void* lower_bound, void* left_count, unsigned long long int* result_size, void* left_key,
+                        unsigned long long int left_size, void* right_key, unsigned long long int right_size) {
+  report("find_bounds_string",
+         rfx_find_bounds_string_compat(static_cast<int32_t*>(lower_bound), static_cast<int32_t*>(left_count),
+                                       reinterpret_cast<uint64_t*>(result_size), left_key, left_size, right_key,
+                                       right_size));
+}
+
+void count_string(const void* key_begin, const void* value_begin, void* result_key_begin, void* result_value_begin,
+                  unsigned long long int* key_size, unsigned long long int* value_size) {
+  report("count_string", rfx_count_string_compat(key_begin, value_begin, result_key_begin, result_value_begin,
+                                                 reinterpret_cast<uint64_t*>(key_size),
+                                                 reinterpret_cast<uint64_t*>(value_size)));
+}
+
+// the same computation as count_string in the reference (Reduce.cu:665-740)
+void total_string_32(const void* key_begin, const void* value_begin, void* result_key_begin,
+                     void* result_value_begin, unsigned long long int* key_size, unsigned long long int* value_size) {
+  report("total_string_32", rfx_count_string_compat(key_begin, value_begin, result_key_begin, result_value_begin,
+                                                    reinterpret_cast<uint64_t*>(key_size),
+                                                    reinterpret_cast<uint64_t*>(value_size)));
+}
+
+// Sort.h: whole-key ascending sort of [begin, end) of a DataType (thrust::sort in
+// Sort.cu:198-300; keys only, so any correct sort gives the same bytes)
+void sort(void* begin, void* end, unsigned long long int type) {
+  static const unsigned long long width[] = {0, 1, 2, 4, 8, 16, 32, 64};
+  if (type == 0 || type >= sizeof(width) / sizeof(width[0])) {
+    report("sort", RFX_ERR_UNSUPPORTED);
+    return;
+  }
+  const unsigned long long bytes = static_cast<char*>(end) - static_cast<char*>(begin);
+  report("sort", rfx_mgpu_sort_key(begin, bytes / width[type], type));
+}
+
+void sort_string(void* begin, void* end) {
+  const unsigned long long bytes = static_cast<char*>(end) - static_cast<char*>(begin);
+  report("sort_string", rfx_sort_string_compat(begin, nullptr, bytes / 8, 0));
 }
 
 }  // namespace redfox

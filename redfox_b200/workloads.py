@@ -66,3 +66,51 @@ def fact_plan(n, device="cuda"):
 
 def fact_row_bytes():
     return R.container_bytes(sum(FACT_WIDTHS))
+
+
+# ---------------------------------------------------------------- string keys
+STRING_SEED = SEED_BASE + 7
+# Name-like prefixes (shared runs longer than one 7-character refinement chunk) and bytes
+# that are negative as `char`.
+STRING_PREFIXES = [b"", b"Customer#0000", b"Supplier#000000000", b"Clerk#", b"\x80\xfe\x7f",
+                   b"aaaaaaaaaaaaaaaaaaaaaa"]
+
+
+def gen_strings(n, seed=STRING_SEED, distinct=None, max_len=40):
+    """A seeded string column: (pool, offs), n NUL-terminated strings back to back in one
+    uint8 array (every element its own copy, so equal strings have distinct addresses)
+    and their offsets.  `distinct` base strings (default n // 4 + 1) are drawn with
+    replacement; they cover the cases the string order has to get right: empty strings,
+    proper prefixes of other strings, bytes >= 0x80, long shared prefixes and narrow
+    alphabets ('a'/'b' only, digits only) that tie over many chunks."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    m = distinct or n // 4 + 1
+    width = max_len + 1
+    lens = rng.integers(0, max_len + 1, m)
+    kind = rng.integers(0, 4, m)
+    full = rng.integers(1, 256, (m, width), dtype=np.uint8)
+    ab = rng.integers(ord("a"), ord("c"), (m, width), dtype=np.uint8)
+    digits = rng.integers(ord("0"), ord("9") + 1, (m, width), dtype=np.uint8)
+    mat = np.where((kind == 1)[:, None], ab, np.where((kind == 2)[:, None], digits, full))
+    pre = rng.integers(0, len(STRING_PREFIXES), m)
+    for k, p in enumerate(STRING_PREFIXES):
+        if p:
+            rows = np.nonzero((pre == k) & (kind == 3))[0]
+            mat[rows, :len(p)] = np.frombuffer(p, np.uint8)
+            lens[rows] = np.maximum(lens[rows], len(p))
+    # every eighth string is a proper prefix of the one before it
+    j = np.arange(7, m, 8)
+    mat[j] = mat[j - 1]
+    lens[j] = lens[j - 1] // 2
+    lens[rng.random(m) < 0.02] = 0
+    idx = rng.integers(0, m, n)
+    rows = mat[idx]
+    rl = lens[idx]
+    cols = np.arange(width)[None, :]
+    rows[cols == rl[:, None]] = 0
+    pool = rows[cols <= rl[:, None]]
+    offs = np.zeros(n, np.uint64)
+    if n > 1:
+        np.cumsum(rl[:-1] + 1, out=offs[1:])
+    return (pool if n else np.zeros(1, np.uint8)), offs

@@ -18,6 +18,8 @@ Sources of truth:
   * sort.npz         -- redfox::sort (Sort.cu) per element type.
   * fact_plan.npz    -- the filter-project-aggregate plan written with the reference's
                         Tuple.h / Comparisons.h / Project.h and thrust (ref_fact_plan).
+  * strings.npz      -- a seeded string column (pool + offsets) through redfox::sort_string
+                        (Sort.cu) and redfox::count_string (Reduce.cu), sorted and unsorted.
 """
 import ctypes as C
 import os
@@ -45,7 +47,8 @@ def main():
         sys.exit("oracle/_ref/libredfox_ref.so missing: run `make -C oracle ref` first")
     for fn in ("ref_set_union", "ref_difference", "ref_unique", "ref_intersection_u32",
                "ref_count_8", "ref_count_16", "ref_count_32", "ref_count_128", "ref_total_64_32",
-               "ref_reduce_sum_i64_u32", "ref_reduce_sum_i64_u64", "ref_fact_plan"):
+               "ref_reduce_sum_i64_u32", "ref_reduce_sum_i64_u64", "ref_fact_plan", "ref_count_string",
+               "ref_total_string_32"):
         getattr(ref, fn).restype = C.c_uint64 if fn != "ref_fact_plan" else C.c_int64
     rng = np.random.default_rng(20101130)
 
@@ -171,6 +174,22 @@ def main():
     g = ref.ref_fact_plan(ptr(rows), C.c_size_t(n), 2475, ptr(ok), ptr(s1), ptr(s2), ptr(cnt))
     np.savez_compressed(os.path.join(HERE, "fact_plan.npz"), n=np.array([n]), cutoff=np.array([2475]),
                         keys=ok[:g], s1=s1[:g], s2=s2[:g], counts=cnt[:g])
+    # ---- string keys: columns of pointers into one pool (host pointers here)
+    from redfox_b200 import workloads as WL
+    pool, offs = WL.gen_strings(4000, seed=20101130, distinct=900)
+    base = np.uint64(pool.ctypes.data)
+    keys = offs + base
+    ref.ref_sort_string(ptr(keys), C.c_size_t(len(keys)))
+    sorted_offs = keys - base
+    vals = rng.integers(0, 2**32, len(offs), dtype=np.uint64).astype(np.uint32)
+    strs = {"pool": pool, "offs": offs, "sorted": sorted_offs, "vals": vals}
+    for name, col in (("count_sorted", sorted_offs), ("count_unsorted", offs)):
+        k = col + base
+        ok = np.zeros(len(col), np.uint64)
+        ov = np.zeros(len(col), np.uint32)
+        g = ref.ref_count_string(ptr(k), ptr(vals), ptr(ok), ptr(ov), C.c_size_t(len(col)))
+        strs[name + "_offs"], strs[name + "_sums"] = ok[:g] - base, ov[:g]
+    np.savez_compressed(os.path.join(HERE, "strings.npz"), **strs)
     print("golden fixtures written to", HERE)
 
 

@@ -74,6 +74,28 @@ def test_sort_matches_reference():
         assert np.array_equal(O.sort_pairs(g["e%d_in" % e]), g["e%d_out" % e]), e
 
 
+def test_strings_match_reference():
+    """redfox::sort_string (Sort.cu) and redfox::count_string (Reduce.cu) on a column with
+    empty strings, proper prefixes, bytes >= 0x80 and long shared prefixes."""
+    g = load("strings.npz")
+    pool, offs = g["pool"], g["offs"]
+    assert np.array_equal(O.str_sort(pool, offs), g["sorted"])
+    for name, col in (("count_sorted", g["sorted"]), ("count_unsorted", offs)):
+        ko, ks = O.str_count(pool, col, g["vals"])
+        assert np.array_equal(ko, g[name + "_offs"]) and np.array_equal(ks, g[name + "_sums"]), name
+
+
+def test_string_order_known_answers():
+    """Signed-char order, a proper prefix first, equality by content."""
+    pool, offs = O.str_pool([b"b", b"", b"ab", b"a", b"\x80", b"\x7f", b"ab\xff", b"ab"])
+    order = O.str_sort(pool, offs)
+    text = [bytes(pool[o:pool.tolist().index(0, int(o))]) for o in order]
+    assert text == [b"", b"\x80", b"a", b"ab", b"ab", b"ab\xff", b"b", b"\x7f"]
+    assert order[3] < order[4]   # equal strings keep their input order
+    ko, ks = O.str_count(pool, order, np.ones(8, np.uint32))
+    assert ks.tolist() == [1, 1, 1, 2, 1, 1, 1]
+
+
 def test_fact_plan_matches_reference_composition():
     g = load("fact_plan.npz")
     rows = fact_rows_oracle(int(g["n"][0]))

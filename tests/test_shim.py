@@ -1,5 +1,5 @@
 """The reference's own redfox:: entry points (C++ linkage, the signatures of
-redfox/ra/interface/*.h) exported by the shim libraries over librfx.so: the exact
+redfox/ra/interface/*.h, string keys included) exported by the shim libraries over librfx.so: the exact
 signatures are present, and on the GPU each computes what the oracle does."""
 import ctypes as C
 import os
@@ -25,11 +25,18 @@ EXPECTED = {
     + ["redfox::total_64_32(void const*, void const*, void*, void*, %s*, %s*)" % (ULL, ULL),
        "redfox::set_union(void*, %s*, void*, void*, void*, void*, unsigned int)" % ULL,
        "redfox::difference(void*, %s*, void*, void*, void*, void*, unsigned int)" % ULL,
-       "redfox::unique(void*, %s*, %s)" % (ULL, ULL)],
+       "redfox::unique(void*, %s*, %s)" % (ULL, ULL),
+       "redfox::find_bounds_string(void*, void*, %s*, void*, %s, void*, %s)" % (ULL, ULL, ULL),
+       "redfox::count_string(void const*, void const*, void*, void*, %s*, %s*)" % (ULL, ULL),
+       "redfox::total_string_32(void const*, void const*, void*, void*, %s*, %s*)" % (ULL, ULL),
+       "redfox::sort(void*, void*, %s)" % ULL,
+       "redfox::sort_string(void*, void*)"],
     "b40c": ["redfox::sort_pair(void*, void*, %s, %s, %s)" % (ULL, ULL, ULL),
              "redfox::sort_key(void*, %s, %s)" % (ULL, ULL)],
     "mgpu": ["redfox::sort_pair(void*, void*, %s, %s, %s)" % (ULL, ULL, ULL),
-             "redfox::sort_key(void*, %s, %s)" % (ULL, ULL)],
+             "redfox::sort_key(void*, %s, %s)" % (ULL, ULL),
+             "redfox::sort_string_pair(void*, void*, %s, %s, %s)" % (ULL, ULL, ULL),
+             "redfox::sort_string_key(void*, %s, %s)" % (ULL, ULL)],
 }
 
 

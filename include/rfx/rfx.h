@@ -232,6 +232,55 @@ rfx_status rfx_total_i64_compat(const void* key_begin, const void* value_begin,
                                 void* result_key_begin, void* result_value_begin,
                                 uint64_t* key_size, uint64_t* value_size, uint32_t key_bytes);
 
+/* ---------------------------------------------------------------- double values */
+/* Operations of rfx_reduce_f64. */
+enum { RFX_F64_SUM = 0, RFX_F64_MIN = 1 };
+
+size_t rfx_reduce_f64_workspace(uint64_t n);
+
+/* Reduce-by-key over double values: thrust::reduce_by_key with plus<double>
+ * (total_{8,16,32,64,128}_double, Reduce.cu:819-1453) or minimum<double> (min_32_double,
+ * :1455-1536).  keys: n containers of key_bytes (1/2/4/8/16, compared bitwise; 0 = one run
+ * over all values, thrust::reduce of total_double :976-1015).  Per run in input order:
+ * the key (out_keys; unused when key_bytes is 0) and the value; *d_groups = runs.
+ * RFX_F64_SUM is the exact sum of the run rounded once to nearest-even (independent of
+ * evaluation order; a sequential double sum differs from it by at most its own rounding
+ * error).  NaN if a term is NaN or both infinities occur, an infinity if one occurs, -0
+ * only when every term is -0.  RFX_F64_MIN is the reference's fold acc = acc < v ? acc : v
+ * bit for bit (a later equal element replaces an earlier one; a NaN replaces the
+ * accumulator and the next element replaces the NaN).  Sums return after `stream`
+ * drains (a value far below the largest one triggers a second, full-range pass).
+ * n < 2^30. */
+rfx_status rfx_reduce_f64(const void* keys, uint64_t n, uint32_t key_bytes, const double* values,
+                          uint32_t op, void* out_keys, double* out_values, uint64_t* d_groups,
+                          void* workspace, size_t workspace_bytes, void* stream);
+
+/* redfox::total_{8,16,32,64,128}_double (Reduce.cu:819-1453) with the reference's byte-size
+ * convention (*key_size / *value_size device byte counts, in and out); key_bytes = 1, 2,
+ * 4, 8 or 16.  Synchronous on the default stream. */
+rfx_status rfx_total_double_compat(const void* key_begin, const void* value_begin,
+                                   void* result_key_begin, void* result_value_begin,
+                                   uint64_t* key_size, uint64_t* value_size, uint32_t key_bytes);
+/* redfox::total_string_double (Reduce.cu:742-817): string keys (device pointers to
+ * NUL-terminated strings, runs of equal content), the first pointer of each run. */
+rfx_status rfx_total_string_double_compat(const void* key_begin, const void* value_begin,
+                                          void* result_key_begin, void* result_value_begin,
+                                          uint64_t* key_size, uint64_t* value_size);
+/* redfox::min_32_double (Reduce.cu:1455-1536): u32 keys, minimum<double>. */
+rfx_status rfx_min_32_double_compat(const void* key_begin, const void* value_begin,
+                                    void* result_key_begin, void* result_value_begin,
+                                    uint64_t* key_size, uint64_t* value_size);
+/* redfox::total_double(result, begin, end) (Reduce.cu:976-1015): the sum of the doubles
+ * in [begin, end) into the device double *result (0.0 when empty). */
+rfx_status rfx_sum_double_compat(void* result, const void* begin, const void* end);
+/* redfox::max_double (Reduce.cu:1058-1136): the maximum of [begin, end) compared as
+ * unsigned 64-bit words with initial value 0, as the reference reduces it, into the device
+ * word *result. */
+rfx_status rfx_max_double_compat(void* result, const void* begin, const void* end);
+/* redfox::count(result, begin, end) (Reduce.cu:1017-1056): the u32 sum (mod 2^32) of the
+ * u32 words in [begin, end) into *result. */
+rfx_status rfx_count_u32_compat(void* result, const void* begin, const void* end);
+
 /* ---------------------------------------------------------------- join */
 size_t rfx_join_find_bounds_workspace(uint64_t nl);
 

@@ -98,6 +98,7 @@ def _declare(L):
         "orc_str_find_bounds": (None, [P, P, P, P, P, sz, P, sz]),
         "orc_str_count": (u64, [P, P, sz, P, P, P]),
         "orc_str_codes": (u64, [P, P, sz, P]),
+        "orc_reduce_f64_seq": (u64, [P, sz, u32, P, P, P, C.c_int]),
         "orc_rand": (u64, [u64, u64, u64]),
         "orc_uniform": (u64, [u64, u64, u64, u64, u64]),
         "orc_gen_uniform_u64": (None, [P, sz, u64, u64, u64, u64, C.c_int]),
@@ -221,6 +222,69 @@ def reduce_count(keys, vals=None):
     v = None if vals is None else np.ascontiguousarray(vals, np.uint32)
     g = lib().orc_reduce_count(_p(keys), n, kb, _p(v), _p(ok), _p(oc))
     return ok[:g], oc[:g]
+
+
+# ---------------------------------------------------------------- double values
+def reduce_f64_seq(keys, vals, op_min=False):
+    """The reference's sequential fold per run of equal keys (keys None: one run)."""
+    v = np.ascontiguousarray(vals, np.float64)
+    n = v.shape[0]
+    if keys is None:
+        kb, k, ok = 0, None, None
+    else:
+        k = np.ascontiguousarray(keys)
+        kb = k.dtype.itemsize * (1 if k.ndim == 1 else k.shape[1])
+        ok = np.zeros_like(k)
+    ov = np.zeros(n, np.float64)
+    g = lib().orc_reduce_f64_seq(_p(k), n, kb, _p(v), _p(ok), _p(ov), int(op_min))
+    return (ok[:g] if ok is not None else None), ov[:g]
+
+
+def run_starts(keys, n):
+    """Start index of every run of equal keys (rows of a 2-D byte array compare whole)."""
+    if n == 0:
+        return np.zeros(0, np.int64)
+    if keys is None:
+        return np.zeros(1, np.int64)
+    k = np.ascontiguousarray(keys)
+    diff = (k[1:] != k[:-1]) if k.ndim == 1 else np.any(k[1:] != k[:-1], axis=1)
+    return np.concatenate([[0], np.nonzero(diff)[0] + 1]).astype(np.int64)
+
+
+def exact_sum(x):
+    """The sum of the doubles x computed exactly and rounded once to nearest-even, with
+    IEEE addition's specials: NaN for a NaN or both infinities, else the infinity; an
+    exact zero is -0 only if every term is -0; overflow gives the signed infinity."""
+    import math
+    from fractions import Fraction
+    x = np.asarray(x, np.float64)
+    if np.isnan(x).any() or (np.isposinf(x).any() and np.isneginf(x).any()):
+        return math.nan
+    if np.isposinf(x).any():
+        return math.inf
+    if np.isneginf(x).any():
+        return -math.inf
+    try:
+        s = math.fsum(x.tolist())
+    except OverflowError:
+        f = sum((Fraction(float(v)) for v in x.tolist()), Fraction(0))
+        try:
+            return float(f)   # int / int division in Python rounds correctly
+        except OverflowError:
+            return math.inf if f > 0 else -math.inf
+    if s == 0.0:
+        return -0.0 if np.all(np.signbit(x)) and not np.any(x) else 0.0
+    return s
+
+
+def reduce_f64_exact(keys, vals):
+    """Per run of equal keys: (first key, exact_sum of the run's values)."""
+    v = np.ascontiguousarray(vals, np.float64)
+    st = run_starts(keys, v.shape[0])
+    ends = np.concatenate([st[1:], [v.shape[0]]]) if st.size else st
+    sums = np.array([exact_sum(v[a:b]) for a, b in zip(st, ends)], np.float64)
+    ok = None if keys is None else np.ascontiguousarray(keys)[st]
+    return ok, sums
 
 
 # ---------------------------------------------------------------- string keys

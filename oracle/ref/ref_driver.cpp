@@ -158,6 +158,33 @@ REF_REDUCE(count_32, 4, 4)
 REF_REDUCE(count_128, 16, 4)
 REF_REDUCE(total_64_32, 8, 4)
 
+/* ---- double values (thrust::reduce_by_key / reduce with plus / minimum<double>) ---- */
+REF_REDUCE(total_8_double, 1, 8)
+REF_REDUCE(total_16_double, 2, 8)
+REF_REDUCE(total_32_double, 4, 8)
+REF_REDUCE(total_64_double, 8, 8)
+REF_REDUCE(total_128_double, 16, 8)
+REF_REDUCE(total_string_double, 8, 8)
+REF_REDUCE(min_32_double, 4, 8)
+extern "C" double ref_total_double(const double* v, size_t n)
+{
+    double r = 0;
+    redfox::total_double(&r, v, v + n);
+    return r;
+}
+extern "C" uint64_t ref_max_double(const double* v, size_t n)
+{
+    unsigned long long r = 0;
+    redfox::max_double(&r, v, v + n);
+    return r;
+}
+extern "C" uint32_t ref_count(const uint32_t* v, size_t n)
+{
+    unsigned int r = 0;
+    redfox::count(&r, v, v + n);
+    return r;
+}
+
 /* ---- string keys: columns of pointers to NUL-terminated strings (host pointers here) ---- */
 REF_REDUCE(count_string, 8, 4)
 REF_REDUCE(total_string_32, 8, 4)

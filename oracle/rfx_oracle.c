@@ -991,3 +991,33 @@ uint64_t orc_str_codes(const char* pool, const uint64_t* offs, size_t n, uint32_
     free(it);
     return code + 1;
 }
+
+/* ------------------------------------------------------------------------------------
+ * Double values.
+ * ----------------------------------------------------------------------------------*/
+
+/* total_{8,16,32,64,128}_double / min_32_double / total_double (Reduce.cu:819-1536,
+ * :976-1015) on the CPU: thrust::reduce_by_key's sequential fold over runs of bitwise
+ * equal keys (kb = 0: one run), acc = acc + v or acc = (acc < v ? acc : v) in input
+ * order, the run's first key reported.  This is the order the reference's own code has
+ * when built for the CPU. */
+uint64_t orc_reduce_f64_seq(const void* keys, size_t n, uint32_t kb, const double* vals,
+                            void* out_keys, double* out_vals, int op_min)
+{
+    const uint8_t* K = (const uint8_t*)keys;
+    uint8_t* OK = (uint8_t*)out_keys;
+    uint64_t g = 0;
+    size_t i = 0;
+    while (i < n) {
+        double acc = vals[i];
+        size_t j = i + 1;
+        while (j < n && (kb == 0 || memcmp(K + j * kb, K + i * kb, kb) == 0)) {
+            double v = vals[j++];
+            acc = op_min ? (acc < v ? acc : v) : acc + v;
+        }
+        if (kb) memcpy(OK + g * kb, K + i * kb, kb);
+        out_vals[g++] = acc;
+        i = j;
+    }
+    return g;
+}

@@ -156,6 +156,10 @@ uint64_t orc_str_count(const char* pool, const uint64_t* offs, size_t n, const u
                        uint64_t* out_offs, uint32_t* out_sums);
 uint64_t orc_str_codes(const char* pool, const uint64_t* offs, size_t n, uint32_t* codes);
 
+/* ---- double values: the reference's sequential thrust folds (sum, minimum) ---- */
+uint64_t orc_reduce_f64_seq(const void* keys, size_t n, uint32_t kb, const double* vals,
+                            void* out_keys, double* out_vals, int op_min);
+
 #ifdef __cplusplus
 }
 #endif

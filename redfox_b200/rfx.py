@@ -638,3 +638,45 @@ def count_string(ptrs, values):
     g = int(ks.item()) // 8
     assert int(vs.item()) // 4 == g
     return ok[:g], ov[:g]
+
+
+# ---------------------------------------------------------------------------- double values
+F64_SUM, F64_MIN = 0, 1
+
+
+def _declare_f64():
+    P, u32, u64, sz, st = C.c_void_p, C.c_uint32, C.c_uint64, C.c_size_t, C.c_int
+    more = {
+        "rfx_reduce_f64_workspace": (sz, [u64]),
+        "rfx_reduce_f64": (st, [P, u64, u32, P, u32, P, P, P, P, sz, P]),
+        "rfx_total_double_compat": (st, [P, P, P, P, P, P, u32]),
+        "rfx_total_string_double_compat": (st, [P, P, P, P, P, P]),
+        "rfx_min_32_double_compat": (st, [P, P, P, P, P, P]),
+        "rfx_sum_double_compat": (st, [P, P, P]),
+        "rfx_max_double_compat": (st, [P, P, P]),
+        "rfx_count_u32_compat": (st, [P, P, P]),
+    }
+    for name, (res, args) in more.items():
+        f = getattr(LIB, name)
+        f.restype = res
+        f.argtypes = args
+
+
+_declare_f64()
+
+
+def reduce_f64(keys, values, op=F64_SUM, stream=None):
+    """Runs of equal keys (None: one run) over float64 values -> (out_keys or None,
+    out_values, groups).  SUM is the exact sum rounded once; MIN the reference's fold."""
+    import torch
+    n = values.shape[0]
+    kb = 0 if keys is None else _width(keys)
+    out_k = None if keys is None else torch.empty_like(keys)
+    out_v = torch.empty(max(n, 1), dtype=torch.float64, device=values.device)
+    g = torch.zeros(1, dtype=torch.int64, device=values.device)
+    wsb = LIB.rfx_reduce_f64_workspace(n)
+    ws = _empty_bytes(wsb, values.device)
+    check("rfx_reduce_f64", LIB.rfx_reduce_f64(_ptr(keys), n, kb, _ptr(values), op, _ptr(out_k), _ptr(out_v), _ptr(g),
+                                               _ptr(ws), wsb, _stream(stream)))
+    k = int(g.item())
+    return (out_k[:k] if out_k is not None else None), out_v[:k], k

@@ -1,6 +1,6 @@
 // redfox_ra.cpp -- libredfox_ra.so: the reference's redfox:: entry points for joins,
 // reductions and set operations, with its C++ linkage and signatures
-// (redfox/ra/interface/ModernGPUJoin.h:15-41, Reduce.h:43-83 and :132-144, Union.h:13,
+// (redfox/ra/interface/ModernGPUJoin.h:15-41, Reduce.h:43-158, Union.h:13,
 // Difference.h:13, Unique.h:15, Sort.h:15-17), each forwarding to the rfx_*_compat entry of librfx.so
 // that keeps the reference's argument meaning (element counts for find_bounds / join, byte
 // counts for reduce / count / set operations, device-resident result sizes, synchronous
@@ -73,6 +73,53 @@ void difference(void* result, unsigned long long int* size, void* lbegin, void* 
 
 void unique(void* begin, unsigned long long int* size, unsigned long long int type) {
   report("unique", rfx_unique_compat(begin, reinterpret_cast<uint64_t*>(size), type));
+}
+
+// double values (Reduce.h:85-158): exact sums rounded once, the minimum as the
+// reference's fold, max_double / count as the reference reduces them
+#define RFX_SHIM_TOTAL_DOUBLE(W, BYTES)                                                                    \
+  void total_##W##_double(const void* key_begin, const void* value_begin, void* result_key_begin,         \
+                          void* result_value_begin, unsigned long long int* key_size,                     \
+                          unsigned long long int* value_size) {                                           \
+    report("total_" #W "_double",                                                                          \
+           rfx_total_double_compat(key_begin, value_begin, result_key_begin, result_value_begin,          \
+                                   reinterpret_cast<uint64_t*>(key_size),                                 \
+                                   reinterpret_cast<uint64_t*>(value_size), BYTES));                      \
+  }
+
+RFX_SHIM_TOTAL_DOUBLE(8, 1)
+RFX_SHIM_TOTAL_DOUBLE(16, 2)
+RFX_SHIM_TOTAL_DOUBLE(32, 4)
+RFX_SHIM_TOTAL_DOUBLE(64, 8)
+RFX_SHIM_TOTAL_DOUBLE(128, 16)
+#undef RFX_SHIM_TOTAL_DOUBLE
+
+void total_string_double(const void* key_begin, const void* value_begin, void* result_key_begin,
+                         void* result_value_begin, unsigned long long int* key_size,
+                         unsigned long long int* value_size) {
+  report("total_string_double",
+         rfx_total_string_double_compat(key_begin, value_begin, result_key_begin, result_value_begin,
+                                        reinterpret_cast<uint64_t*>(key_size),
+                                        reinterpret_cast<uint64_t*>(value_size)));
+}
+
+void min_32_double(const void* key_begin, const void* value_begin, void* result_key_begin, void* result_value_begin,
+                   unsigned long long int* key_size, unsigned long long int* value_size) {
+  report("min_32_double", rfx_min_32_double_compat(key_begin, value_begin, result_key_begin, result_value_begin,
+                                                   reinterpret_cast<uint64_t*>(key_size),
+                                                   reinterpret_cast<uint64_t*>(value_size)));
+}
+
+void total_double(void* result, const void* begin, const void* end) {
+  report("total_double", rfx_sum_double_compat(result, begin, end));
+}
+
+void max_double(void* result, const void* begin, const void* end) {
+  report("max_double", rfx_max_double_compat(result, begin, end));
+}
+
+void count(void* result, const void* begin, const void* end) {
+  report("count", rfx_count_u32_compat(result, begin, end));
 }
 
 // string keys: columns of device pointers to NUL-terminated strings

@@ -18,6 +18,8 @@ Sources of truth:
   * sort.npz         -- redfox::sort (Sort.cu) per element type.
   * fact_plan.npz    -- the filter-project-aggregate plan written with the reference's
                         Tuple.h / Comparisons.h / Project.h and thrust (ref_fact_plan).
+  * f64.npz          -- redfox::total_{8,16,32,64,128}_double, min_32_double, total_double,
+                        max_double and count (Reduce.cu) on seeded double columns.
   * strings.npz      -- a seeded string column (pool + offsets) through redfox::sort_string
                         (Sort.cu) and redfox::count_string (Reduce.cu), sorted and unsorted.
 """
@@ -190,6 +192,41 @@ def main():
         g = ref.ref_count_string(ptr(k), ptr(vals), ptr(ok), ptr(ov), C.c_size_t(len(col)))
         strs[name + "_offs"], strs[name + "_sums"] = ok[:g] - base, ov[:g]
     np.savez_compressed(os.path.join(HERE, "strings.npz"), **strs)
+    # ---- double values
+    for fn in ("ref_total_8_double", "ref_total_16_double", "ref_total_32_double", "ref_total_64_double",
+               "ref_total_128_double", "ref_min_32_double", "ref_max_double"):
+        getattr(ref, fn).restype = C.c_uint64
+    ref.ref_total_double.restype = C.c_double
+    ref.ref_count.restype = C.c_uint32
+    f64 = {}
+    n = 5000
+    vals = rng.uniform(1.0, 2.0, n) * np.exp2(rng.integers(-30, 31, n)) * rng.choice([1.0, -1.0], n)
+    vals[rng.integers(0, n, 40)] = rng.choice([0.0, -0.0, np.nan, np.inf], 40)
+    f64["vals"] = vals
+    groups = np.sort(rng.integers(0, 300, n))
+    for kb, dt in ((1, np.uint8), (2, np.uint16), (4, np.uint32), (8, np.uint64)):
+        k = (groups.astype(np.uint64) * np.uint64(2654435761)).astype(dt)
+        ok = np.zeros_like(k)
+        ov = np.zeros(n, np.float64)
+        g = getattr(ref, "ref_total_%d_double" % (kb * 8))(ptr(k), ptr(vals), ptr(ok), ptr(ov), C.c_size_t(n))
+        f64["k%d" % kb], f64["k%d_okeys" % kb], f64["k%d_sums" % kb] = k, ok[:g].copy(), ov[:g].copy()
+        if kb == 4:
+            g = ref.ref_min_32_double(ptr(k), ptr(vals), ptr(ok), ptr(ov), C.c_size_t(n))
+            f64["k4_min_okeys"], f64["k4_mins"] = ok[:g], ov[:g]
+    k16 = np.zeros((n, 2), np.uint64)
+    k16[:, 0] = groups.astype(np.uint64) * np.uint64(0x9E3779B97F4A7C15)
+    k16[:, 1] = groups.astype(np.uint64)
+    ok = np.zeros_like(k16)
+    ov = np.zeros(n, np.float64)
+    g = ref.ref_total_128_double(ptr(k16), ptr(vals), ptr(ok), ptr(ov), C.c_size_t(n))
+    f64["k16"], f64["k16_okeys"], f64["k16_sums"] = k16, ok[:g], ov[:g]
+    fin = np.ascontiguousarray(vals[np.isfinite(vals)])
+    f64["total"] = np.array([ref.ref_total_double(ptr(fin), C.c_size_t(len(fin)))])
+    f64["max_bits"] = np.array([ref.ref_max_double(ptr(vals), C.c_size_t(n))], np.uint64)
+    u = rng.integers(0, 2**32, n, dtype=np.uint64).astype(np.uint32)
+    f64["u32"], f64["count"] = u, np.array([ref.ref_count(ptr(u), C.c_size_t(n))], np.uint32)
+    np.savez_compressed(os.path.join(HERE, "f64.npz"), **f64)
+
     print("golden fixtures written to", HERE)
 
 

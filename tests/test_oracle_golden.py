@@ -74,6 +74,42 @@ def test_sort_matches_reference():
         assert np.array_equal(O.sort_pairs(g["e%d_in" % e]), g["e%d_out" % e]), e
 
 
+def _same_bits(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return bool(np.all((np.isnan(a) & np.isnan(b)) | (a.view(np.uint64) == b.view(np.uint64))))
+
+
+def test_f64_reduces_match_reference():
+    """The sequential folds of the oracle reproduce redfox::total_*_double, min_32_double,
+    total_double, max_double and count (Reduce.cu) bit for bit; the exact sums the GPU
+    computes lie within the sequential sums' rounding error."""
+    g = load("f64.npz")
+    vals = g["vals"]
+    for kb in (1, 2, 4, 8, 16):
+        ok, ov = O.reduce_f64_seq(g["k%d" % kb], vals)
+        assert np.array_equal(ok, g["k%d_okeys" % kb]) and _same_bits(ov, g["k%d_sums" % kb]), kb
+        ek, es = O.reduce_f64_exact(g["k%d" % kb], vals)
+        assert np.array_equal(ek, ok)
+        fin = np.isfinite(ov)
+        assert np.all(np.abs(es[fin] - ov[fin]) <= 1e-12 * np.maximum(np.abs(ov[fin]), 1.0))
+        assert np.array_equal(np.isnan(es), np.isnan(ov))
+    ok, ov = O.reduce_f64_seq(g["k4"], vals, op_min=True)
+    assert np.array_equal(ok, g["k4_min_okeys"]) and np.array_equal(ov.view(np.uint64), g["k4_mins"].view(np.uint64))
+    fin = vals[np.isfinite(vals)]
+    _, tot = O.reduce_f64_seq(None, fin)
+    assert _same_bits(tot, g["total"])
+    assert vals.view(np.uint64).max() == g["max_bits"][0]
+    assert int(g["u32"].astype(np.uint64).sum() % 2**32) == int(g["count"][0])
+
+
+def test_exact_sum_known_answers():
+    assert O.exact_sum([1e16, 1.0]) == 1e16                    # tie -> even
+    assert O.exact_sum([1e16, 1.0, 1.0]) == 1e16 + 2.0
+    assert O.exact_sum([1e308, 1e308, -1e308]) == 1e308        # no intermediate overflow
+    assert np.signbit(O.exact_sum([-0.0, -0.0])) and not np.signbit(O.exact_sum([-0.0, 0.0]))
+    assert np.isnan(O.exact_sum([np.inf, -np.inf])) and O.exact_sum([np.inf, 1.0]) == np.inf
+
+
 def test_strings_match_reference():
     """redfox::sort_string (Sort.cu) and redfox::count_string (Reduce.cu) on a column with
     empty strings, proper prefixes, bytes >= 0x80 and long shared prefixes."""

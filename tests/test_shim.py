@@ -30,7 +30,14 @@ EXPECTED = {
        "redfox::count_string(void const*, void const*, void*, void*, %s*, %s*)" % (ULL, ULL),
        "redfox::total_string_32(void const*, void const*, void*, void*, %s*, %s*)" % (ULL, ULL),
        "redfox::sort(void*, void*, %s)" % ULL,
-       "redfox::sort_string(void*, void*)"],
+       "redfox::sort_string(void*, void*)"]
+    + ["redfox::total_%d_double(void const*, void const*, void*, void*, %s*, %s*)" % (w, ULL, ULL)
+       for w in (8, 16, 32, 64, 128)]
+    + ["redfox::total_string_double(void const*, void const*, void*, void*, %s*, %s*)" % (ULL, ULL),
+       "redfox::min_32_double(void const*, void const*, void*, void*, %s*, %s*)" % (ULL, ULL),
+       "redfox::total_double(void*, void const*, void const*)",
+       "redfox::max_double(void*, void const*, void const*)",
+       "redfox::count(void*, void const*, void const*)"],
     "b40c": ["redfox::sort_pair(void*, void*, %s, %s, %s)" % (ULL, ULL, ULL),
              "redfox::sort_key(void*, %s, %s)" % (ULL, ULL)],
     "mgpu": ["redfox::sort_pair(void*, void*, %s, %s, %s)" % (ULL, ULL, ULL),

@@ -417,6 +417,63 @@ def operator_benchmarks(dev, fact_rows, peak, reps=5):
     return ops
 
 
+def string_f64_benchmarks(dev, peak, reps=5):
+    """The string-keyed and double-valued operators (data resident in HBM)."""
+    import numpy as np
+    import torch
+
+    from redfox_b200 import rfx as R
+    from redfox_b200 import workloads as WL
+
+    ops = {}
+    # double SUM / MIN by u32 key: 19.3M rows, 256K groups (the join-output reduce shape)
+    n, groups = 19_300_000, 256_000
+    rng = np.random.default_rng(17)
+    keys = torch.from_numpy(np.sort(rng.integers(0, groups, n)).astype(np.int32)).to(dev)
+    vals = torch.from_numpy(np.round(rng.uniform(900.0, 105000.0, n), 2)).to(dev)
+    ok = torch.empty_like(keys)
+    ov = torch.empty(n, dtype=torch.float64, device=dev)
+    g = torch.zeros(1, dtype=torch.int64, device=dev)
+    wsb = R.LIB.rfx_reduce_f64_workspace(n)
+    ws = R._empty_bytes(wsb, dev)
+    for name, op in (("reduce_f64_sum_19M_u32key", R.F64_SUM), ("reduce_f64_min_19M_u32key", R.F64_MIN)):
+        def run(op=op):
+            R.check("f64", R.LIB.rfx_reduce_f64(R._ptr(keys), n, 4, R._ptr(vals), op, R._ptr(ok), R._ptr(ov),
+                                                R._ptr(g), R._ptr(ws), wsb, R._stream()))
+        ms = _time_ms(run, reps)
+        k = int(g.item())
+        pre = n * 8 if op == R.F64_SUM else 0   # the exponent pre-pass reads the values once more
+        ops[name] = _op_line(n, n * 12 + k * 12, ms, peak, groups=k, traffic_floor_bytes=n * 12 + k * 12 + pre)
+    # one run over 60M doubles (total_double)
+    n1 = 60_000_000
+    v1 = torch.from_numpy(np.round(rng.uniform(900.0, 105000.0, n1), 2)).to(dev)
+    res = torch.zeros(1, dtype=torch.float64, device=dev)
+    ms = _time_ms(lambda: R.check("sum", R.LIB.rfx_sum_double_compat(R._ptr(res), R._ptr(v1),
+                                                                    R.C.c_void_p(v1.data_ptr() + 8 * n1))), reps)
+    ops["sum_double_60M"] = _op_line(n1, n1 * 8, ms, peak, note="compat entry: allocates, synchronises")
+    del v1, keys, vals, ok, ov, ws
+    # strings: 2M names (about 21 characters on average, many shared prefixes)
+    ns = 2_000_000
+    pool, offs = WL.gen_strings(ns, distinct=500_000)
+    dpool, ptrs = R.string_column(pool, offs, dev)
+    sbytes = ns * 8 + int(pool.shape[0])
+    work = ptrs.clone()
+    codes = torch.empty(ns, dtype=torch.int32, device=dev)
+    perm = torch.empty(ns, dtype=torch.int32, device=dev)
+    nd = R.C.c_uint64(0)
+    ms = _time_ms(lambda: R.check("codes", R.LIB.rfx_string_codes(R._ptr(ptrs), ns, R._ptr(codes), R._ptr(perm),
+                                                                  R.C.byref(nd), R._stream())), 3)
+    ops["string_codes_2M"] = _op_line(ns, sbytes, ms, peak, distinct=nd.value,
+                                      note="rounds of 7 characters through the radix sort; wall-clock bound")
+    ms = _time_ms(lambda: R.sort_strings(work), 3, setup=lambda: work.copy_(ptrs))
+    ops["sort_string_key_2M"] = _op_line(ns, sbytes, ms, peak)
+    R.sort_strings(work)
+    cv = torch.ones(ns, dtype=torch.int32, device=dev)
+    ms = _time_ms(lambda: R.count_string(work, cv), 3)
+    ops["count_string_2M_sorted"] = _op_line(ns, sbytes + ns * 4, ms, peak)
+    return ops
+
+
 def tuning_benchmark(dev, fact_rows, reps=5):
     """Default variant vs the autotuner's choice per size class for the tuned operators:
     select (plan-specialised compaction, rows per thread), the staged reduce (256- or
@@ -749,6 +806,7 @@ def main_ours(args):
         if world == 1 and not args.no_operators:
             del dev_in_keep
             result["operators"] = operator_benchmarks(dev, rows, peak)
+            result["operators"].update(string_f64_benchmarks(dev, peak))
             result["tuning"] = tuning_benchmark(dev, rows)
         if world == 1 and args.batched_queries > 0:
             del rows

@@ -3,14 +3,14 @@
 // scalar total_double / max_double / count of Reduce.cu:742-1536.
 //
 // Sums are exact, then rounded once (round to nearest, ties to even): every double is a
-// 53-bit integer times a power of two, so a run's sum is accumulated as an integer in
-// units of 2^L over D signed 64-bit digits of 32 bits each (carry-save; a digit absorbs
-// 2^30 additions without overflow).  Integer addition is associative, so the result does
-// not depend on how the work is split -- unlike a floating-point tree, whose rounding
-// follows its shape.  The fast window is D = 6 digits with L set from the largest
-// exponent in the input (a pre-pass): exact for every value within 2^107 of the largest.
-// A value below that window with bits that would be lost raises a flag and the reduction
-// re-runs with D = 68 digits and L = -1074, which covers every finite double.  Specials
+// 53-bit integer times a power of two, so a run's sum is accumulated as a two's-complement
+// integer in units of 2^L over W 64-bit limbs (add with carry).  Integer addition is
+// associative, so the result does not depend on how the work is split -- unlike a
+// floating-point tree, whose rounding follows its shape.  The fast window is W = 3 limbs
+// with L set from the largest exponent in the input (a pre-pass): exact for every value
+// within 2^107 of the largest, with room for 2^30 terms.  A value below that window with
+// bits that would be lost raises a flag and the reduction re-runs with W = 34 limbs and
+// L = -1074, which covers every finite double.  Specials
 // follow IEEE addition: NaN if any NaN or both infinities, else the infinity, and an
 // exact zero is -0 only when every term is -0.
 //
@@ -37,27 +37,60 @@ constexpr int kF64Threads = 256;
 constexpr int kF64Items = 8;
 constexpr int kF64Tile = kF64Threads * kF64Items;
 constexpr int kFixThreads = 256;
-constexpr int kNarrowDigits = 6;
-constexpr int kWideDigits = 68;
+constexpr int kNarrowLimbs = 3;   // 192 bits: every value within 2^107 of the largest
+constexpr int kWideLimbs = 34;    // 2176 bits: every finite double
 constexpr int kWideL = -1074;
 
 enum : uint32_t { kSumNaN = 1, kSumPosInf = 2, kSumNegInf = 4, kSumNotNegZero = 8 };
 
 // ------------------------------------------------------------------ exact sum
-template <int D>
+// W 64-bit limbs holding a two's-complement integer (limb 0 lowest) in units of 2^L.
+// Additions are exact modulo 2^(64W); the true sum stays inside the signed range by the
+// choice of L, so the result is exact and independent of the order of the additions.
+template <int W>
 struct SumOp {
   struct P {
-    long long d[D];
+    unsigned long long l[W];
     uint32_t flags;
     uint32_t pad;
   };
   __device__ __forceinline__ static P identity() {
     P p;
 #pragma unroll
-    for (int k = 0; k < D; ++k) p.d[k] = 0;
+    for (int k = 0; k < W; ++k) p.l[k] = 0;
     p.flags = 0;
     p.pad = 0;
     return p;
+  }
+  // acc += a (neg: acc -= a) where a has limbs lo at q, hi at q + 1.
+  __device__ __forceinline__ static void accumulate(unsigned long long* acc, int q, unsigned long long lo,
+                                                    unsigned long long hi, bool neg) {
+    if constexpr (W == 3) {
+      const unsigned long long a0 = q == 0 ? lo : 0ull, a1 = q == 0 ? hi : lo, a2 = q == 0 ? 0ull : hi;
+      if (!neg)
+        asm("add.cc.u64 %0, %0, %3;\n\taddc.cc.u64 %1, %1, %4;\n\taddc.u64 %2, %2, %5;"
+            : "+l"(acc[0]), "+l"(acc[1]), "+l"(acc[2])
+            : "l"(a0), "l"(a1), "l"(a2));
+      else
+        asm("sub.cc.u64 %0, %0, %3;\n\tsubc.cc.u64 %1, %1, %4;\n\tsubc.u64 %2, %2, %5;"
+            : "+l"(acc[0]), "+l"(acc[1]), "+l"(acc[2])
+            : "l"(a0), "l"(a1), "l"(a2));
+    } else {
+      unsigned long long c = 0;
+      for (int k = q; k < W; ++k) {
+        const unsigned long long a = k == q ? lo : k == q + 1 ? hi : 0ull;
+        if (!neg) {
+          const unsigned __int128 t = (unsigned __int128)acc[k] + a + c;
+          acc[k] = (unsigned long long)t;
+          c = (unsigned long long)(t >> 64);
+        } else {
+          const unsigned __int128 t = (unsigned __int128)acc[k] - a - c;
+          acc[k] = (unsigned long long)t;
+          c = (unsigned long long)(t >> 64) ? 1ull : 0ull;
+        }
+        if (k > q && c == 0) break;
+      }
+    }
   }
   __device__ __forceinline__ static void add(P& p, double x, int L, uint32_t* inexact) {
     const unsigned long long b = (unsigned long long)__double_as_longlong(x);
@@ -78,49 +111,50 @@ struct SumOp {
       m = r >= 64 ? 0 : m >> r;
       s = 0;
     }
-    const int q = s >> 5, o = s & 31;
-    const unsigned long long lo = m << o;
-    const unsigned long long hi = o ? m >> (64 - o) : 0ull;
-    const long long t0 = (long long)(lo & 0xffffffffull), t1 = (long long)(lo >> 32), t2 = (long long)hi;
-    if (q + 2 >= D) {  // above the window: only when L was not set from this input's maximum
+    const int q = s >> 6, o = s & 63;
+    if (q + 1 >= W) {  // above the window: only when L was not set from this input's maximum
       atomicOr(inexact, 1u);
       return;
     }
-    if constexpr (D <= 8) {
-#pragma unroll
-      for (int k = 0; k < D; ++k) {
-        const long long v = k == q ? t0 : k == q + 1 ? t1 : k == q + 2 ? t2 : 0;
-        p.d[k] += neg ? -v : v;
-      }
-    } else {
-      p.d[q] += neg ? -t0 : t0;
-      p.d[q + 1] += neg ? -t1 : t1;
-      p.d[q + 2] += neg ? -t2 : t2;
-    }
+    const unsigned long long lo = m << o;
+    const unsigned long long hi = o ? m >> (64 - o) : 0ull;
+    accumulate(p.l, q, lo, hi, neg);
   }
   __device__ __forceinline__ static P combine(const P& a, const P& b) {
     P r;
-#pragma unroll
-    for (int k = 0; k < D; ++k) r.d[k] = a.d[k] + b.d[k];
+    if constexpr (W == 3) {
+      r.l[0] = a.l[0];
+      r.l[1] = a.l[1];
+      r.l[2] = a.l[2];
+      asm("add.cc.u64 %0, %0, %3;\n\taddc.cc.u64 %1, %1, %4;\n\taddc.u64 %2, %2, %5;"
+          : "+l"(r.l[0]), "+l"(r.l[1]), "+l"(r.l[2])
+          : "l"(b.l[0]), "l"(b.l[1]), "l"(b.l[2]));
+    } else {
+      unsigned long long c = 0;
+      for (int k = 0; k < W; ++k) {
+        const unsigned __int128 t = (unsigned __int128)a.l[k] + b.l[k] + c;
+        r.l[k] = (unsigned long long)t;
+        c = (unsigned long long)(t >> 64);
+      }
+    }
     r.flags = a.flags | b.flags;
     r.pad = 0;
     return r;
   }
-  // Bits [pos, pos + len) of the D 32-bit digits r (len <= 64, pos >= 0).
-  __device__ static unsigned long long bits_at(const uint32_t* r, int pos, int len) {
+  // Bits [pos, pos + len) of the limbs (len <= 64, pos >= 0).
+  __device__ static unsigned long long bits_at(const unsigned long long* l, int pos, int len) {
     if (len <= 0) return 0;
-    const int k = pos >> 5, o = pos & 31;
-    const unsigned long long d0 = k < D ? r[k] : 0u, d1 = k + 1 < D ? r[k + 1] : 0u, d2 = k + 2 < D ? r[k + 2] : 0u;
-    const unsigned long long lo = d0 | (d1 << 32);
-    unsigned long long v = (lo >> o) | (o ? d2 << (64 - o) : 0ull);
+    const int k = pos >> 6, o = pos & 63;
+    const unsigned long long d0 = k < W ? l[k] : 0ull, d1 = k + 1 < W ? l[k + 1] : 0ull;
+    unsigned long long v = (d0 >> o) | (o ? d1 << (64 - o) : 0ull);
     if (len < 64) v &= (1ull << len) - 1;
     return v;
   }
-  __device__ static bool any_below(const uint32_t* r, int pos) {
-    const int k = pos >> 5;
-    for (int i = 0; i < k && i < D; ++i)
-      if (r[i]) return true;
-    if (k < D && (pos & 31) && (r[k] & ((1u << (pos & 31)) - 1))) return true;
+  __device__ static bool any_below(const unsigned long long* l, int pos) {
+    const int k = pos >> 6;
+    for (int i = 0; i < k && i < W; ++i)
+      if (l[i]) return true;
+    if (k < W && (pos & 63) && (l[k] & ((1ull << (pos & 63)) - 1))) return true;
     return false;
   }
   // The correctly rounded double of the accumulated value, as bits.
@@ -128,28 +162,23 @@ struct SumOp {
     if ((p.flags & kSumNaN) || ((p.flags & kSumPosInf) && (p.flags & kSumNegInf))) return 0x7ff8000000000000ull;
     if (p.flags & kSumPosInf) return 0x7ff0000000000000ull;
     if (p.flags & kSumNegInf) return 0xfff0000000000000ull;
-    uint32_t r[D];
-    long long c = 0;
+    unsigned long long r[W];
 #pragma unroll
-    for (int k = 0; k < D; ++k) {
-      const long long t = p.d[k] + c;
-      r[k] = (uint32_t)t;
-      c = t >> 32;
-    }
-    const bool neg = c < 0;
-    if (neg) {
-      unsigned long long carry = 1;
+    for (int k = 0; k < W; ++k) r[k] = p.l[k];
+    const bool neg = (r[W - 1] >> 63) != 0;
+    if (neg) {  // magnitude = two's complement negation
+      unsigned long long c = 1;
 #pragma unroll
-      for (int k = 0; k < D; ++k) {
-        const unsigned long long t = (unsigned long long)(uint32_t)~r[k] + carry;
-        r[k] = (uint32_t)t;
-        carry = t >> 32;
+      for (int k = 0; k < W; ++k) {
+        const unsigned long long t = ~r[k] + c;
+        c = (c && t == 0) ? 1ull : 0ull;
+        r[k] = t;
       }
     }
     int top = -1;
-    for (int k = D - 1; k >= 0; --k)
+    for (int k = W - 1; k >= 0; --k)
       if (r[k]) {
-        top = 32 * k + 31 - __clz(r[k]);
+        top = 64 * k + 63 - __clzll(r[k]);
         break;
       }
     if (top < 0) return (p.flags & kSumNotNegZero) ? 0ull : 0x8000000000000000ull;
@@ -157,13 +186,13 @@ struct SumOp {
     int e = top + L;  // the value lies in [2^e, 2^(e+1))
     if (e > 1023) return sgn | 0x7ff0000000000000ull;
     const bool normal = e >= -1022;
-    const int lsb = normal ? top - 52 : -1074 - L;  // digit bit that becomes the result's LSB
+    const int lsb = normal ? top - 52 : -1074 - L;  // bit that becomes the result's LSB
     unsigned long long mant;
     if (lsb <= 0) {
       mant = bits_at(r, 0, top + 1) << (-lsb);
     } else {
       mant = bits_at(r, lsb, top - lsb + 1);
-      const bool round = ((bits_at(r, lsb - 1, 1)) & 1ull) != 0;
+      const bool round = (bits_at(r, lsb - 1, 1) & 1ull) != 0;
       const bool sticky = any_below(r, lsb - 1);
       if (round && (sticky || (mant & 1ull))) ++mant;
     }
@@ -589,8 +618,8 @@ F64Layout f64_layout(void* ws, uint64_t n) {
 }
 
 size_t f64_workspace(uint64_t n) {
-  const size_t a = f64_layout<SumOp<kNarrowDigits>>(nullptr, n).total;
-  const size_t b = f64_layout<SumOp<kWideDigits>>(nullptr, n).total;
+  const size_t a = f64_layout<SumOp<kNarrowLimbs>>(nullptr, n).total;
+  const size_t b = f64_layout<SumOp<kWideLimbs>>(nullptr, n).total;
   const size_t c = f64_layout<MinOp>(nullptr, n).total;
   return a > b ? (a > c ? a : c) : (b > c ? b : c);
 }
@@ -634,14 +663,14 @@ rfx_status f64_run(F64Args a, void* ws, bool narrow_sum, int fixed_L, cudaStream
 template <int KB>
 rfx_status f64_dispatch_op(F64Args a, uint32_t op, void* ws, cudaStream_t s) {
   if (op == RFX_F64_MIN) return f64_run<KB, MinOp>(a, ws, false, 0, s);
-  rfx_status st = f64_run<KB, SumOp<kNarrowDigits>>(a, ws, true, 0, s);
+  rfx_status st = f64_run<KB, SumOp<kNarrowLimbs>>(a, ws, true, 0, s);
   if (st != RFX_OK) return st;
-  const F64Layout l = f64_layout<SumOp<kNarrowDigits>>(ws, a.n);
+  const F64Layout l = f64_layout<SumOp<kNarrowLimbs>>(ws, a.n);
   uint32_t inexact = 0;
   RFX_CUDA_TRY(cudaMemcpyAsync(&inexact, l.inexact, sizeof(inexact), cudaMemcpyDeviceToHost, s));
   RFX_CUDA_TRY(cudaStreamSynchronize(s));
   if (!inexact) return RFX_OK;
-  return f64_run<KB, SumOp<kWideDigits>>(a, ws, false, kWideL, s);  // values span beyond the window
+  return f64_run<KB, SumOp<kWideLimbs>>(a, ws, false, kWideL, s);  // values span beyond the window
 }
 
 rfx_status f64_dispatch(F64Args a, uint32_t key_bytes, uint32_t op, void* ws, cudaStream_t s) {

@@ -232,6 +232,58 @@ rfx_status rfx_total_i64_compat(const void* key_begin, const void* value_begin,
                                 void* result_key_begin, void* result_value_begin,
                                 uint64_t* key_size, uint64_t* value_size, uint32_t key_bytes);
 
+/* Packs an aggregate's key and value columns into tuples: out[i] = key[i] << value_bits |
+ * (value[i] & mask(value_bits)) -- the merge that closes the reference's aggregation
+ * (ra::cuda::merge, Split_Merge.h:442-495, as addAgg emits it,
+ * RelationalAlgebraCompiler.cpp:8536-8643).  Containers: out and keys 4/8/16 bytes, values
+ * 4/8 bytes (unused when value_bits is 0).  If d_n is not NULL the row count is
+ * min(n, *d_n), read on the device. */
+rfx_status rfx_merge_columns(void* out, uint32_t out_bytes, uint64_t n, const uint64_t* d_n,
+                             const void* keys, uint32_t key_bytes, const void* values,
+                             uint32_t value_bytes, uint32_t value_bits, void* stream);
+
+/* ---------------------------------------------------------------- plan builder */
+/* Lowers relational-algebra operators to an executor plan (rfx_exec_create), as the
+ * reference's RelationalAlgebraCompiler does to HIR kernel sequences (addJoin,
+ * RelationalAlgebraCompiler.cpp:4466-5227; addAgg, :7852-8643; select, project and set
+ * builders), without protobuf and without compiling kernels at run time.  Relations are
+ * packed tuples: field widths in bits, field 0 most significant.  Keys of a join are the
+ * first keycount fields of both inputs; an input not sorted on the fields an operator needs
+ * is sorted in place first (the builder tracks sortedness and sorts once).  A select read
+ * only by one project is fused into one select_project.  An aggregation over leading
+ * fields reads key and value from the rows directly; a COUNT over the same rows and
+ * domains as an earlier TOTAL shares its reduce.  Aggregation results are relations
+ * (domains..., value): TOTAL values are exact 64-bit sums, COUNT 32-bit counts.  Calls
+ * return RFX_ERR_INVALID / RFX_ERR_UNSUPPORTED with a message in rfx_plan_error. */
+enum { RFX_AGG_COUNT = 0, RFX_AGG_TOTAL = 1 };
+typedef struct rfx_plan rfx_plan;
+rfx_status rfx_plan_create(rfx_plan** out);
+void rfx_plan_destroy(rfx_plan* plan);
+const char* rfx_plan_error(const rfx_plan* plan);
+/* An input relation (bound or loaded by name on the executor) sorted on its first
+ * sorted_fields fields. */
+rfx_status rfx_plan_relation(rfx_plan* plan, const char* name, const uint32_t* widths,
+                             uint32_t nfields, uint32_t sorted_fields);
+rfx_status rfx_plan_select(rfx_plan* plan, const char* dest, const char* src,
+                           const rfx_cmp* cmps, uint32_t ncmp);
+rfx_status rfx_plan_project(rfx_plan* plan, const char* dest, const char* src,
+                            const uint32_t* fields, uint32_t nfields);
+rfx_status rfx_plan_join(rfx_plan* plan, const char* dest, const char* a, const char* b,
+                         uint32_t keycount);
+rfx_status rfx_plan_agg(rfx_plan* plan, const char* dest, const char* src,
+                        const uint32_t* domains, uint32_t ndomains, uint32_t tag,
+                        uint32_t field);
+/* kind: RFX_SET_UNION / RFX_SET_DIFFERENCE / RFX_SET_INTERSECTION. */
+rfx_status rfx_plan_set(rfx_plan* plan, const char* dest, const char* a, const char* b,
+                        uint32_t kind);
+/* Removes duplicate tuples of a relation in place. */
+rfx_status rfx_plan_unique(rfx_plan* plan, const char* name);
+rfx_status rfx_plan_output(rfx_plan* plan, const char* name);
+/* The executor plan as JSON into buf (cap bytes, NUL-terminated); returns the size needed. */
+size_t rfx_plan_json(rfx_plan* plan, char* buf, size_t cap);
+rfx_status rfx_plan_schema(const rfx_plan* plan, const char* name, uint32_t* widths,
+                           uint32_t* nfields, uint32_t* sorted_fields);
+
 /* ---------------------------------------------------------------- double values */
 /* Operations of rfx_reduce_f64. */
 enum { RFX_F64_SUM = 0, RFX_F64_MIN = 1 };

@@ -18,6 +18,8 @@
 //   reduce      {in, key_shift, value_shift, value_bits, keys, key_bytes, sums, counts}
 //   set         {kind: union|difference|intersection, a, b, out}
 //   unique      {rel}                                               in place
+//   merge       {keys, values, out, value_bits}   out = key << value_bits | value (values
+//               optional: then out = key); closes an aggregation as a relation
 // A comparison operand is {"field": i} or {"const": c}.  Every device buffer comes from
 // the stream-ordered allocator; the running total is held within the byte budget
 // (RFX_ERR_CAPACITY otherwise) and its peak is reported.
@@ -430,6 +432,19 @@ rfx_status op_unique(rfx_exec* x, const Op& o) {
   return read_count(x, (const uint64_t*)cnt.p, &v->rows);
 }
 
+rfx_status op_merge(rfx_exec* x, const Op& o) {
+  Var* k = var(x, jstr(o.j, "keys"));
+  Var* v = jstr(o.j, "values").empty() ? nullptr : var(x, jstr(o.j, "values"));
+  Var* out = var(x, jstr(o.j, "out"));
+  const uint32_t vb = v ? (uint32_t)jint(o.j, "value_bits", v->row_bytes * 8) : 0u;
+  if (v && v->rows != k->rows) return fail(x, RFX_ERR_INVALID, "merge: column lengths differ");
+  rfx_status st = dev_alloc(x, *out, k->rows * (uint64_t)out->row_bytes);
+  if (st != RFX_OK) return st;
+  out->rows = k->rows;
+  return rfx_merge_columns(out->ptr, out->row_bytes, k->rows, nullptr, k->ptr, k->row_bytes, v ? v->ptr : nullptr,
+                           v ? v->row_bytes : 4u, vb, x->stream);
+}
+
 // reads / writes of an op (names), for liveness
 bool op_operands(const Op& o, std::vector<std::string>& r, std::vector<std::string>& w) {
   const Json* j = o.j;
@@ -451,6 +466,10 @@ bool op_operands(const Op& o, std::vector<std::string>& r, std::vector<std::stri
   } else if (o.kind == "set") {
     r.push_back(jstr(j, "a"));
     r.push_back(jstr(j, "b"));
+    w.push_back(jstr(j, "out"));
+  } else if (o.kind == "merge") {
+    r.push_back(jstr(j, "keys"));
+    if (!jstr(j, "values").empty()) r.push_back(jstr(j, "values"));
     w.push_back(jstr(j, "out"));
   } else {
     return false;
@@ -605,6 +624,7 @@ extern "C" rfx_status rfx_exec_run(rfx_exec* x, void* stream) {
     else if (o.kind == "join") st = op_join(x, o);
     else if (o.kind == "reduce") st = op_reduce(x, o);
     else if (o.kind == "set") st = op_set(x, o);
+    else if (o.kind == "merge") st = op_merge(x, o);
     else st = op_unique(x, o);
     ++x->launches;
     if (st != RFX_OK) {

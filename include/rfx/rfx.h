@@ -493,7 +493,8 @@ rfx_status rfx_gen_uniform_rows(void* out, uint64_t n, const rfx_tuple* type, ui
 
 /* ---------------------------------------------------------------- autotuning
  * No counterpart in the reference (its kernels have fixed launch shapes).  Operators with
- * several compiled variants (the TMA-staged rfx_reduce_tuples: 256- or 128-line tiles; the
+ * several compiled variants (the TMA-staged rfx_reduce_tuples: chunked, or a look-back per
+ * 256- or 128-line tile; the
  * set filters behind rfx_set_op: 8 or 4 items per thread; the plan-specialised rfx_select /
  * rfx_select_project: items per thread; the plan-specialised rfx_filter_aggregate: rows per
  * thread per iteration) run their default unless tuning is on.  With
@@ -503,6 +504,9 @@ rfx_status rfx_gen_uniform_rows(void* out, uint64_t n, const rfx_tuple* type, ui
  * class run the fastest.  Do not enable it while capturing a stream into a graph. */
 void rfx_tune_set(int mode);
 void rfx_tune_reset(void);
+/* Pins an operator (1 reduce_tuples, 2 set filters, 3 select / project, 4 filter-aggregate)
+ * to one variant, ahead of tuning and of the default; a negative variant unpins it. */
+void rfx_tune_force(uint32_t op, int variant);
 /* The tuning table as text lines "op=.. shape=.. class=.. variant=.. ms=t0,t1,..";
  * returns the bytes needed (including the terminating 0); writes at most cap bytes. */
 size_t rfx_tune_dump(char* buf, size_t cap);

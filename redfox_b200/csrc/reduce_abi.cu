@@ -99,11 +99,45 @@ RowLayout row_layout(void* ws, uint64_t n, uint32_t row_bytes) {
   return L;
 }
 
+// The chunked staged reduce: one look-back record per chunk (at most one chunk per
+// resident block), and scratch for n / 16 groups (plus a floor for small inputs): a chunk
+// whose groups do not fit its share runs its rows a second time.
+constexpr uint64_t kMaxChunks = 4096;
+constexpr int kChunkStages = 3;
+constexpr uint64_t kChunkRowsPerSlot = 16;
+
+struct ChunkLayout {
+  SegRecord* records;
+  uint32_t* counter;
+  size_t clear;
+  uint8_t* keys;
+  int64_t* sums;
+  uint32_t* counts;
+  uint64_t slots;
+  size_t total;
+};
+
+ChunkLayout chunk_layout(void* ws, uint64_t n) {
+  Carver c(ws);
+  ChunkLayout L;
+  L.records = c.take<SegRecord>(kMaxChunks);
+  L.counter = c.take<uint32_t>(1);
+  L.clear = align_up(c.used, 256);
+  L.slots = n / kChunkRowsPerSlot + 65536;
+  L.keys = c.take<uint8_t>(L.slots * 16);
+  L.sums = c.take<int64_t>(L.slots);
+  L.counts = c.take<uint32_t>(L.slots);
+  L.total = align_up(c.used, 256);
+  return L;
+}
+
 }  // namespace
 
 size_t reduce_workspace_impl(uint64_t n) {
   const size_t a = red_layout(nullptr, n).total, b = row_layout(nullptr, n, 16).total;
-  return a > b ? a : b;
+  const size_t c = chunk_layout(nullptr, n).total;
+  const size_t ab = a > b ? a : b;
+  return ab > c ? ab : c;
 }
 
 rfx_status reduce_impl(const void* keys, uint64_t n, const uint64_t* d_n, uint32_t kb, const void* vals, uint32_t vk,
@@ -243,10 +277,84 @@ rfx_status launch_rows(const void* rows, uint64_t n, RowReduceArgs& a, cudaStrea
   return RFX_OK;
 }
 
-// Variant 0: 256-line tiles, 1: 128-line tiles.
+// The chunked form (256-line tiles): chunks of whole tiles, one per block.
 template <int RB, int SHAPE>
-rfx_status launch_rows_v(int v, const void* rows, uint64_t n, RowReduceArgs& a, cudaStream_t s) {
-  return v == 0 ? launch_rows<RB, SHAPE, 256>(rows, n, a, s) : launch_rows<RB, SHAPE, 128>(rows, n, a, s);
+rfx_status launch_chunks(const void* rows, uint64_t n, const RowReduceArgs& a, const ChunkLayout& L,
+                         cudaStream_t s) {
+  constexpr int NT = 256;
+  auto k = reduce_chunks_kernel<RB, SHAPE, kChunkStages, NT>;
+  const size_t smem = (size_t)kChunkStages * NT * kRingLineBytes + 1024;
+  RFX_CUDA_TRY(allow_smem((const void*)k, smem));
+  ChunkReduceArgs ca;
+  std::memset(&ca, 0, sizeof(ca));
+  ca.r = a;
+  ca.r.records = L.records;
+  ca.r.tile_counter = L.counter;
+  CUtensorMap map;
+  const uint64_t lines = n * RB / kRingLineBytes;
+  ca.r.full_lines = encode_line_map(&map, rows, lines, NT) ? lines : 0;
+  const uint64_t tiles = (n * RB + NT * kRingLineBytes - 1) / (NT * kRingLineBytes);
+  const uint64_t grid = (uint64_t)persistent_grid((const void*)k, NT, smem, tiles ? tiles : 1);
+  ca.tiles_per_chunk = tiles ? (tiles + grid - 1) / grid : 1;
+  const uint64_t chunks = tiles ? (tiles + ca.tiles_per_chunk - 1) / ca.tiles_per_chunk : 1;
+  if (chunks > kMaxChunks) return RFX_ERR_UNSUPPORTED;
+  const uint64_t cap = L.slots / chunks;
+  ca.cap = (uint32_t)(cap < 0xffffffffull ? cap : 0xffffffffull);
+  ca.s_keys = L.keys;
+  ca.s_sums = L.sums;
+  ca.s_counts = L.counts;
+  k<<<(int)chunks, NT, smem, s>>>(map, ca);
+  RFX_CUDA_TRY(cudaGetLastError());
+  return RFX_OK;
+}
+
+// The warp-chunked form: 4 KB tiles (32 lines), each warp of a block streams its own
+// sub-chunk of whole tiles.
+constexpr int kWarpChunkWarps = 8;
+constexpr int kWarpChunkStages = 3;
+
+template <int RB, int SHAPE>
+rfx_status launch_warps(const void* rows, uint64_t n, const RowReduceArgs& a, const ChunkLayout& L,
+                        cudaStream_t s) {
+  constexpr int W = kWarpChunkWarps, LINES = 32;
+  auto k = reduce_warps_kernel<RB, SHAPE, kWarpChunkStages, W>;
+  const size_t smem = (size_t)W * kWarpChunkStages * LINES * kRingLineBytes + 1024;
+  RFX_CUDA_TRY(allow_smem((const void*)k, smem));
+  ChunkReduceArgs ca;
+  std::memset(&ca, 0, sizeof(ca));
+  ca.r = a;
+  ca.r.records = L.records;
+  ca.r.tile_counter = L.counter;
+  CUtensorMap map;
+  const uint64_t lines = n * RB / kRingLineBytes;
+  ca.r.full_lines = encode_line_map(&map, rows, lines, LINES) ? lines : 0;
+  const uint64_t tiles = (n * RB + LINES * kRingLineBytes - 1) / (LINES * kRingLineBytes);
+  const uint64_t want = tiles ? (tiles + W - 1) / W : 1;
+  const uint64_t grid = (uint64_t)persistent_grid((const void*)k, W * 32, smem, want);
+  ca.tiles_per_chunk = tiles ? (tiles + grid * W - 1) / (grid * W) : 1;   // tiles per warp
+  const uint64_t blocks = tiles ? (tiles + ca.tiles_per_chunk * W - 1) / (ca.tiles_per_chunk * W) : 1;
+  if (blocks > kMaxChunks) return RFX_ERR_UNSUPPORTED;
+  const uint64_t cap = L.slots / (blocks * W);
+  ca.cap = (uint32_t)(cap < 0xffffffffull ? cap : 0xffffffffull);
+  ca.s_keys = L.keys;
+  ca.s_sums = L.sums;
+  ca.s_counts = L.counts;
+  k<<<(int)blocks, W * 32, smem, s>>>(map, ca);
+  RFX_CUDA_TRY(cudaGetLastError());
+  return RFX_OK;
+}
+
+// Variant 0: warp-chunked; 1: block-chunked, 256-line tiles; 2: look-back per tile,
+// 256-line tiles; 3: look-back per tile, 128-line tiles.
+template <int RB, int SHAPE>
+rfx_status launch_rows_v(int v, const void* rows, uint64_t n, RowReduceArgs& a, void* ws, cudaStream_t s) {
+  if (v <= 1) {
+    const ChunkLayout L = chunk_layout(ws, n);
+    RFX_CUDA_TRY(cudaMemsetAsync(ws, 0, L.clear, s));
+    return v == 0 ? launch_warps<RB, SHAPE>(rows, n, a, L, s) : launch_chunks<RB, SHAPE>(rows, n, a, L, s);
+  }
+  RFX_CUDA_TRY(cudaMemsetAsync(ws, 0, row_layout(ws, n, RB).total, s));
+  return v == 2 ? launch_rows<RB, SHAPE, 256>(rows, n, a, s) : launch_rows<RB, SHAPE, 128>(rows, n, a, s);
 }
 
 rfx_status reduce_rows_staged(const void* rows, uint64_t n, const uint64_t* d_n, uint32_t row_bytes,
@@ -274,17 +382,16 @@ rfx_status reduce_rows_staged(const void* rows, uint64_t n, const uint64_t* d_n,
                     : (row_bytes == 16 && value_shift == 0 && val_mask == ~0ull && key_shift == 64) ? 2
                                                                                                    : 0;
   auto run = [&](int v) -> rfx_status {
-    RFX_CUDA_TRY(cudaMemsetAsync(workspace, 0, L.total, s));
-    if (shape == 1) return launch_rows_v<16, ROW16_K32_V64>(v, rows, n, a, s);
-    if (shape == 2) return launch_rows_v<16, ROW16_K64_V64>(v, rows, n, a, s);
+    if (shape == 1) return launch_rows_v<16, ROW16_K32_V64>(v, rows, n, a, workspace, s);
+    if (shape == 2) return launch_rows_v<16, ROW16_K64_V64>(v, rows, n, a, workspace, s);
     switch (row_bytes) {
-      case 4: return launch_rows_v<4, ROW_GENERIC>(v, rows, n, a, s);
-      case 8: return launch_rows_v<8, ROW_GENERIC>(v, rows, n, a, s);
-      default: return launch_rows_v<16, ROW_GENERIC>(v, rows, n, a, s);
+      case 4: return launch_rows_v<4, ROW_GENERIC>(v, rows, n, a, workspace, s);
+      case 8: return launch_rows_v<8, ROW_GENERIC>(v, rows, n, a, workspace, s);
+      default: return launch_rows_v<16, ROW_GENERIC>(v, rows, n, a, workspace, s);
     }
   };
   const uint64_t shape_key = ((uint64_t)row_bytes << 32) | ((uint64_t)shape << 24) | (key_shift << 8) | value_shift;
-  return run(tune_pick(TUNE_REDUCE_ROWS, shape_key, n, 2, run, s));
+  return run(tune_pick(TUNE_REDUCE_ROWS, shape_key, n, 4, run, s));
 }
 }  // namespace
 }  // namespace rfx
@@ -307,7 +414,8 @@ extern "C" rfx_status rfx_reduce_tuples(const void* rows, uint64_t n, const uint
   if (!err) return RFX_ERR_CUDA;
   const uint64_t vmask = value_bits >= 64 ? ~0ull : ((1ull << value_bits) - 1);
   if ((reinterpret_cast<uintptr_t>(rows) & 15u) == 0 && std::getenv("RFX_REDUCE_REGS") == nullptr) {
-    if (workspace_bytes < row_layout(nullptr, n, row_bytes).total) return RFX_ERR_WORKSPACE;
+    if (workspace_bytes < row_layout(nullptr, n, row_bytes).total || workspace_bytes < chunk_layout(nullptr, n).total)
+      return RFX_ERR_WORKSPACE;
     return reduce_rows_staged(rows, n, d_n, row_bytes, key_shift, value_shift, vmask, out_keys, out_key_bytes,
                               out_sums, out_counts, d_groups, workspace, err, s);
   }

@@ -663,4 +663,581 @@ __global__ void __launch_bounds__(NT, 512 / NT) reduce_rows_kernel(const __grid_
   if (n == 0 && blockIdx.x == 0 && t == 0) *a.d_groups = 0;
 }
 
+// A key from lane `src` of the warp (32-, 64- or 128-bit keys).
+template <typename K>
+__device__ __forceinline__ K shfl_key(K k, uint32_t src) {
+  if constexpr (sizeof(K) <= 4) {
+    return (K)__shfl_sync(0xffffffffu, (uint32_t)k, src);
+  } else if constexpr (sizeof(K) == 8) {
+    return (K)__shfl_sync(0xffffffffu, (unsigned long long)k, src);
+  } else {
+    const unsigned long long lo = __shfl_sync(0xffffffffu, (unsigned long long)k, src);
+    const unsigned long long hi = __shfl_sync(0xffffffffu, (unsigned long long)(k >> 64), src);
+    return ((K)hi << 64) | (K)lo;
+  }
+}
+
+// ------------------------------------------------------------------ chunked variant
+// Each block claims a contiguous chunk of tiles and streams it through the three-stage
+// TMA ring, carrying the open run from tile to tile in registers, so no tile waits for
+// another block.  Runs that start and end inside the chunk are written to the chunk's
+// scratch area at their chunk-local index (the heads before them in the chunk).  After
+// its last tile the block publishes the chunk's aggregate and resolves the exclusive
+// prefix over chunks (one look-back per chunk): its f is the chunk's base group index and
+// (v, h) the run left open when the chunk began.  The block then closes that run (its end
+// lies in this chunk: total = carried v plus the chunk's first partial) and copies its
+// scratch groups to base + local index.  A chunk with more groups than its scratch holds
+// runs its tiles a second time, writing straight to base + local index.  Traffic: the
+// rows once, the groups twice (scratch and final) -- the groups are few where a reduce
+// follows a join.
+struct ChunkReduceArgs {
+  RowReduceArgs r;          // records: one per chunk; tile_counter: the chunk counter
+  uint64_t tiles_per_chunk;
+  uint32_t cap;             // scratch groups per chunk
+  uint8_t* s_keys;          // [chunks * cap] keys of out_key_bytes
+  int64_t* s_sums;          // [chunks * cap]
+  uint32_t* s_counts;       // [chunks * cap]
+};
+
+template <int RB, int SHAPE, int S, int NT>
+__global__ void __launch_bounds__(NT, (S <= 2 ? 768 : 512) / NT) reduce_chunks_kernel(const __grid_constant__ CUtensorMap map,
+                                                                       const ChunkReduceArgs ca) {
+  constexpr uint32_t TILE_BYTES = NT * kRingLineBytes;
+  constexpr uint32_t TR = TILE_BYTES / RB;
+  constexpr uint32_t IPT = TR / NT;
+  static_assert(IPT * RB == kRingLineBytes && IPT <= 32, "one 128-byte line per thread");
+  typedef RowAccess<RB, SHAPE> RA;
+  typedef typename RA::Key Key;
+  const RowReduceArgs& a = ca.r;
+  extern __shared__ uint8_t dyn_smem[];
+  uint8_t* stages = align1024(dyn_smem);
+  __shared__ TileRing<S> ring;
+  __shared__ SegPair s_warp[NT / 32];
+  __shared__ SegPair s_pre;
+  __shared__ uint32_t s_chunk, s_nlocal, s_overflow, s_has_first;
+  __shared__ uint64_t s_first_sum, s_first_tail;
+  __shared__ Key s_first_key;
+  const uint32_t t = threadIdx.x;
+  uint64_t n = a.n_max;
+  if (a.d_n) n = min(n, *a.d_n);
+  const uint64_t num_tiles = (n + TR - 1) / TR;
+  const uint64_t covered = a.full_lines * kRingLineBytes;
+  const uint32_t ks = a.key_shift, vs = a.val_shift;
+  const uint64_t vmask = a.val_mask;
+  const uint32_t tb = t * IPT;
+  if (t == 0) {
+    for (int s = 0; s < S; ++s) mbar_init(&ring.bar[s], 1);
+    mbar_fence_init();
+    if (a.full_lines) prefetch_map(&map);
+    s_chunk = atomicAdd(a.tile_counter, 1u);   // claim order = the look-back order
+    s_nlocal = 0;
+    s_overflow = 0;
+    s_has_first = 0;
+  }
+  __syncthreads();
+  const uint64_t c = s_chunk;
+  const uint64_t t0 = c * ca.tiles_per_chunk;
+  const uint64_t t1 = min(t0 + ca.tiles_per_chunk, num_tiles);
+  const uint64_t ntiles = t0 < t1 ? t1 - t0 : 0;
+  uint32_t uses[S];
+#pragma unroll
+  for (int s = 0; s < S; ++s) uses[s] = 0;
+  bool ok = true;
+
+  // start the copy of chunk tile i into its stage (thread 0)
+  auto issue = [&](uint64_t i) {
+    const int s = (int)(i % S);
+    const uint64_t tl = t0 + i;
+    const uint64_t line0 = tl * NT;
+    const bool copy = line0 < a.full_lines;
+    mbar_arrive_tx(&ring.bar[s], copy ? TILE_BYTES : 0u);
+    if (copy) tma_load_lines(stages + (size_t)s * TILE_BYTES, &map, (uint32_t)line0, &ring.bar[s]);
+  };
+
+  // one pass over the chunk's tiles; direct: write to base + local index, else scratch
+  auto run_chunk = [&](bool direct, uint64_t base) -> SegPair {
+    SegPair run{0, 0, 0};
+    if (t == 0) {
+      fence_proxy_async_smem();   // a second pass reuses stages the first one read
+      for (uint64_t i = 0; i < (uint64_t)S && i < ntiles; ++i) issue(i);
+    }
+    for (uint64_t i = 0; i < ntiles && ok; ++i) {
+      const int s = (int)(i % S);
+      const uint64_t tile = t0 + i;
+      uint8_t* st = stages + (size_t)s * TILE_BYTES;
+      bool w = true;
+      if (t == 0) w = mbar_wait(&ring.bar[s], uses[s] & 1u);
+      ++uses[s];
+      if (!__syncthreads_and(w)) {
+        ok = false;
+        break;
+      }
+      if ((tile + 1) * TILE_BYTES > covered) {
+        ring_fill_tail(st, a.rows, tile, covered, n * RB, TILE_BYTES);
+        __syncthreads();
+      }
+      // pass 1: this thread's rows into registers, heads, this thread's (f, v, h); the
+      // neighbouring keys come from the adjacent lanes
+      const uint64_t first = tile * TR + tb;
+      const uint32_t nvalid = first >= n ? 0u : (uint32_t)min((uint64_t)IPT, n - first);
+      Key key[IPT];
+      uint64_t val[IPT];
+#pragma unroll
+      for (uint32_t j = 0; j < IPT; ++j) {
+        key[j] = 0;
+        val[j] = 0;
+        if (j < nvalid) RA::read(st, tb + j, ks, vs, vmask, key[j], val[j]);
+      }
+      const uint32_t lane = t & 31;
+      Key pk = shfl_key(key[IPT - 1], lane ? lane - 1 : 0);
+      Key nk = shfl_key(key[0], lane < 31 ? lane + 1 : 31);
+      uint64_t v = 0;
+      if (lane == 0) {
+        if (t > 0) RA::read(st, tb - 1, ks, vs, vmask, pk, v);
+        else if (first > 0) pk = RA::global_key(a.rows, first - 1, ks);
+      }
+      const bool next_valid = first + IPT < n;
+      if (lane == 31 && next_valid) {
+        if (t + 1 < (uint32_t)NT) RA::read(st, tb + IPT, ks, vs, vmask, nk, v);
+        else nk = RA::global_key(a.rows, first + IPT, ks);
+      }
+      uint32_t heads = 0;
+      uint64_t acc = 0;
+#pragma unroll
+      for (uint32_t j = 0; j < IPT; ++j) {
+        if (j < nvalid) {
+          const bool h = key[j] != (j ? key[j - 1] : pk) || (j == 0 && first == 0);
+          heads |= (uint32_t)h << j;
+          acc = h ? val[j] : acc + val[j];
+        }
+      }
+      const SegPair tp{(uint64_t)__popc(heads), acc, heads ? first + (31u - __clz(heads)) : 0ull};
+      SegPair btot;
+      const SegPair ex = block_seg_exclusive_fast<NT>(tp, s_warp, &btot);
+      // pass 2: one output per run end; the carry is chunk-local
+      const SegPair carry = seg_op(run, ex);
+      uint64_t racc = carry.v, hpos = carry.h;
+#pragma unroll
+      for (uint32_t j = 0; j < IPT; ++j) {
+        if (j < nvalid) {
+          const bool h = (heads >> j) & 1u;
+          racc = h ? val[j] : racc + val[j];
+          if (h) hpos = first + j;
+          bool tail;
+          if (j + 1 < nvalid) tail = (heads >> (j + 1)) & 1u;
+          else if (j + 1 < IPT) tail = true;            // last row of the relation
+          else tail = !next_valid || key[j] != nk;
+          if (tail) {
+            const uint64_t lf = carry.f + (uint64_t)__popc(heads & ((2u << j) - 1u));
+            if (lf == 0) {
+              // the run that was open when the chunk began ends here
+              if (!direct) {
+                s_first_sum = racc;
+                s_first_tail = first + j;
+                s_first_key = key[j];
+                s_has_first = 1;
+              }
+            } else if (direct) {
+              const uint64_t g = base + lf - 1;
+              if (g < n) {
+                store_key(a.out_keys, g, a.out_key_bytes, key[j]);
+                if (a.out_sums) a.out_sums[g] = (int64_t)racc;
+                if (a.out_counts) a.out_counts[g] = (uint32_t)(first + j - hpos + 1);
+              }
+            } else if (lf - 1 < ca.cap) {
+              const uint64_t g = c * ca.cap + lf - 1;
+              store_key(ca.s_keys, g, a.out_key_bytes, key[j]);
+              ca.s_sums[g] = (int64_t)racc;
+              ca.s_counts[g] = (uint32_t)(first + j - hpos + 1);
+              atomicMax(&s_nlocal, (uint32_t)lf);
+            } else {
+              s_overflow = 1;
+            }
+          }
+        }
+      }
+      run = seg_op(run, btot);
+      __syncthreads();
+      if (t == 0 && i + S < ntiles) {
+        fence_proxy_async_smem();
+        issue(i + S);
+      }
+    }
+    return run;
+  };
+
+  const SegPair agg = run_chunk(false, 0);
+  // the chunk's base and the run open at its start (look-back over chunks)
+  lb_publish(a.records, c, agg);
+  if (t < 32) {
+    const SegPair p = warp_lookback_resolve<4>(a.records, c, agg, a.err);
+    if (t == 0) s_pre = p;
+  }
+  __syncthreads();
+  const SegPair pre = s_pre;
+  if (t == 0 && ntiles && t1 == num_tiles) *a.d_groups = pre.f + agg.f;
+  if (t == 0 && n == 0 && c == 0) *a.d_groups = 0;
+  if (t == 0 && s_has_first && pre.f > 0) {
+    const uint64_t g = pre.f - 1;
+    store_key(a.out_keys, g, a.out_key_bytes, s_first_key);
+    if (a.out_sums) a.out_sums[g] = (int64_t)(pre.v + s_first_sum);
+    if (a.out_counts) a.out_counts[g] = (uint32_t)(s_first_tail - pre.h + 1);
+  }
+  if (s_overflow) {
+    __syncthreads();
+    run_chunk(true, pre.f);
+  } else {
+    const uint32_t nl = s_nlocal;
+    for (uint32_t l = t; l < nl; l += NT) {
+      const uint64_t src = c * ca.cap + l, g = pre.f + l;
+      if (a.out_key_bytes == 4) reinterpret_cast<uint32_t*>(a.out_keys)[g] = reinterpret_cast<const uint32_t*>(ca.s_keys)[src];
+      else if (a.out_key_bytes == 8) reinterpret_cast<uint64_t*>(a.out_keys)[g] = reinterpret_cast<const uint64_t*>(ca.s_keys)[src];
+      else reinterpret_cast<uint4*>(a.out_keys)[g] = reinterpret_cast<const uint4*>(ca.s_keys)[src];
+      if (a.out_sums) a.out_sums[g] = ca.s_sums[src];
+      if (a.out_counts) a.out_counts[g] = ca.s_counts[src];
+    }
+  }
+  if (!ok && t == 0) raise_error(a.err, kErrTimeout);
+}
+
+// ------------------------------------------------------------------ warp-chunked variant
+// The chunked form with the block taken out of the per-tile path: a block claims a chunk,
+// and each of its warps streams its own contiguous sub-chunk through a private TMA ring
+// of 4 KB boxes (32 lines, one per lane), scans within the warp (shuffles only) and
+// carries the open run in registers.  No barrier and no look-back lies on the per-tile
+// path.  At the end the block folds its warps' aggregates in order, resolves one prefix
+// for the chunk, and each warp closes the run open at its sub-chunk's start and copies its
+// scratch groups (or runs its sub-chunk again, writing directly, if they overflowed).
+
+template <int WARPS>
+__device__ __forceinline__ void warp_fill_tail(uint8_t* stage, const uint8_t* src, uint64_t tile, uint64_t covered,
+                                               uint64_t limit, uint32_t tile_bytes, uint32_t lane) {
+  const uint64_t t0 = tile * tile_bytes;
+  const uint64_t lo = covered > t0 ? covered : t0;
+  const uint64_t hi = limit < t0 + tile_bytes ? limit : t0 + tile_bytes;
+  if (lo >= hi) return;
+  const uint64_t hi4 = lo + ((hi - lo) & ~3ull);
+  for (uint64_t b = lo + 4ull * lane; b < hi4; b += 128ull) {
+    const uint32_t w = *reinterpret_cast<const uint32_t*>(src + b);
+    *reinterpret_cast<uint32_t*>(stage + swz((uint32_t)(b - t0))) = w;
+  }
+  if (lane == 0)
+    for (uint64_t b = hi4; b < hi; ++b) stage[swz((uint32_t)(b - t0))] = src[b];
+}
+
+__device__ __forceinline__ SegPair shfl_seg(const SegPair& x, uint32_t src) {
+  return SegPair{__shfl_sync(0xffffffffu, x.f, src), __shfl_sync(0xffffffffu, x.v, src),
+                 __shfl_sync(0xffffffffu, x.h, src)};
+}
+
+template <int RB, int SHAPE, int S, int WARPS>
+__global__ void __launch_bounds__(WARPS * 32, 2) reduce_warps_kernel(const __grid_constant__ CUtensorMap map,
+                                                                       const ChunkReduceArgs ca) {
+  constexpr uint32_t LINES = 32;
+  constexpr uint32_t TILE_BYTES = LINES * kRingLineBytes;
+  constexpr uint32_t TR = TILE_BYTES / RB;
+  constexpr uint32_t IPT = TR / 32;
+  static_assert(IPT * RB == kRingLineBytes && IPT <= 32, "one 128-byte line per lane");
+  typedef RowAccess<RB, SHAPE> RA;
+  typedef typename RA::Key Key;
+  const RowReduceArgs& a = ca.r;
+  extern __shared__ uint8_t dyn_smem[];
+  uint8_t* stages = align1024(dyn_smem);
+  __shared__ uint64_t bars[WARPS][S];
+  __shared__ SegPair s_wagg[WARPS];
+  __shared__ SegPair s_pre;
+  __shared__ uint32_t s_chunk;
+  const uint32_t t = threadIdx.x, lane = t & 31, w = t >> 5;
+  uint64_t n = a.n_max;
+  if (a.d_n) n = min(n, *a.d_n);
+  const uint64_t num_tiles = (n + TR - 1) / TR;
+  const uint64_t covered = a.full_lines * kRingLineBytes;
+  const uint32_t ks = a.key_shift, vs = a.val_shift;
+  const uint64_t vmask = a.val_mask;
+  if (t == 0) {
+    s_chunk = atomicAdd(a.tile_counter, 1u);   // claim order = the look-back order
+    if (a.full_lines) prefetch_map(&map);
+  }
+  if (lane == 0) {
+    for (int s = 0; s < S; ++s) mbar_init(&bars[w][s], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  const uint64_t bc = s_chunk;
+  const uint64_t sub = bc * WARPS + w;
+  const uint64_t tpc = ca.tiles_per_chunk;     // tiles per warp sub-chunk
+  const uint64_t t0 = sub * tpc;
+  const uint64_t t1 = min(t0 + tpc, num_tiles);
+  const uint64_t ntiles = t0 < t1 ? t1 - t0 : 0;
+  uint8_t* wst = stages + (size_t)w * S * TILE_BYTES;
+  uint32_t uses[S];
+#pragma unroll
+  for (int s = 0; s < S; ++s) uses[s] = 0;
+  bool ok = true;
+  // this lane's record of the run open at the sub-chunk's start, if it ends here
+  bool has_first = false, overflow = false;
+  uint64_t first_sum = 0, first_tail = 0;
+  Key first_key = 0;
+  uint32_t max_lf = 0;
+
+  auto issue = [&](uint64_t i) {
+    const int s = (int)(i % S);
+    const uint64_t line0 = (t0 + i) * LINES;
+    const bool copy = line0 < a.full_lines;
+    mbar_arrive_tx(&bars[w][s], copy ? TILE_BYTES : 0u);
+    if (copy) tma_load_lines(wst + (size_t)s * TILE_BYTES, &map, (uint32_t)line0, &bars[w][s]);
+  };
+
+  // a group that ends at row `tail` with index lf (1-based, 0: the run open at the
+  // sub-chunk's start), total `sum`, head at `hpos`
+  auto emit = [&](bool direct, uint64_t base, uint64_t lf, Key key, uint64_t sum, uint64_t tail, uint64_t hpos) {
+    if (lf == 0) {
+      if (!direct) {
+        has_first = true;
+        first_sum = sum;
+        first_tail = tail;
+        first_key = key;
+      }
+    } else if (direct) {
+      const uint64_t g = base + lf - 1;
+      if (g < n) {
+        store_key(a.out_keys, g, a.out_key_bytes, key);
+        if (a.out_sums) a.out_sums[g] = (int64_t)sum;
+        if (a.out_counts) a.out_counts[g] = (uint32_t)(tail - hpos + 1);
+      }
+    } else if (lf - 1 < ca.cap) {
+      const uint64_t g = sub * ca.cap + lf - 1;
+      store_key(ca.s_keys, g, a.out_key_bytes, key);
+      ca.s_sums[g] = (int64_t)sum;
+      ca.s_counts[g] = (uint32_t)(tail - hpos + 1);
+      max_lf = max(max_lf, (uint32_t)lf);
+    } else {
+      overflow = true;
+    }
+  };
+
+  auto run_sub = [&](bool direct, uint64_t base) -> SegPair {
+    SegPair run{0, 0, 0};
+    if (lane == 0) {
+      fence_proxy_async_smem();   // a second pass reuses stages the first one read
+      for (uint64_t i = 0; i < (uint64_t)S && i < ntiles; ++i) issue(i);
+    }
+    __syncwarp();
+    // the key of the row before the current tile, and whether that row's run end is
+    // still undecided (it is the last row of the previous tile)
+    Key last_key = 0;
+    bool pending = false;
+    if (ntiles && t0 * TR > 0 && t0 * TR <= n) last_key = RA::global_key(a.rows, t0 * TR - 1, ks);
+    for (uint64_t i = 0; i < ntiles && ok; ++i) {
+      const int s = (int)(i % S);
+      const uint64_t tile = t0 + i;
+      uint8_t* st = wst + (size_t)s * TILE_BYTES;
+      const bool wok = mbar_wait(&bars[w][s], uses[s] & 1u);
+      ++uses[s];
+      if (!__all_sync(0xffffffffu, wok)) {
+        ok = false;
+        break;
+      }
+      if ((tile + 1) * TILE_BYTES > covered) {
+        warp_fill_tail<WARPS>(st, a.rows, tile, covered, n * RB, TILE_BYTES, lane);
+        __syncwarp();
+      }
+      const uint64_t first = tile * TR + lane * IPT;
+      if (IPT <= 16 && (tile + 1) * TR <= n) {
+        // a full tile: every lane holds IPT rows; the scan carries (heads << 16 | position
+        // of the last head within the tile) in one word and the sum in another
+        const uint64_t tile_row = tile * TR;
+        Key key[IPT];
+        uint64_t val[IPT], racc[IPT];
+#pragma unroll
+        for (uint32_t j = 0; j < IPT; ++j) RA::read(st, lane * IPT + j, ks, vs, vmask, key[j], val[j]);
+        Key pk = shfl_key(key[IPT - 1], lane ? lane - 1 : 0);
+        const Key nk = shfl_key(key[0], lane < 31 ? lane + 1 : 31);
+        if (lane == 0) pk = last_key;
+        uint32_t heads = 0;
+        uint64_t acc = 0;
+#pragma unroll
+        for (uint32_t j = 0; j < IPT; ++j) {
+          const bool h = key[j] != (j ? key[j - 1] : pk) || (j == 0 && first == 0);
+          heads |= (uint32_t)h << j;
+          acc = h ? val[j] : acc + val[j];
+          racc[j] = acc;
+        }
+        if (lane == 0 && pending && (heads & 1u)) emit(direct, base, run.f, last_key, run.v, first - 1, run.h);
+        uint32_t fh = heads ? ((uint32_t)__popc(heads) << 16) | (lane * IPT + 31u - __clz(heads)) : 0u;
+        uint64_t fv = acc;
+#pragma unroll
+        for (uint32_t o = 1; o < 32; o <<= 1) {
+          const uint32_t yfh = __shfl_up_sync(0xffffffffu, fh, o);
+          const uint64_t yv = __shfl_up_sync(0xffffffffu, fv, o);
+          if (lane >= o) {
+            if (fh >> 16) {
+              fh += yfh & 0xffff0000u;
+            } else {
+              fh = yfh;
+              fv += yv;
+            }
+          }
+        }
+        const uint32_t tfh = __shfl_sync(0xffffffffu, fh, 31);
+        const uint64_t tv = __shfl_sync(0xffffffffu, fv, 31);
+        uint32_t efh = __shfl_up_sync(0xffffffffu, fh, 1);
+        uint64_t ev = __shfl_up_sync(0xffffffffu, fv, 1);
+        if (lane == 0) {
+          efh = 0;
+          ev = 0;
+        }
+        const uint64_t cf = run.f + (efh >> 16);
+        const uint64_t cv = (efh >> 16) ? ev : run.v + ev;
+        const uint64_t ch = (efh >> 16) ? tile_row + (efh & 0xffffu) : run.h;
+        // run ends: the row before each head, and the last row when the next key differs
+        uint32_t tails = heads >> 1;
+        if (lane < 31) {
+          if (key[IPT - 1] != nk) tails |= 1u << (IPT - 1);
+        } else if ((tile + 1) * TR >= n) {
+          tails |= 1u << (IPT - 1);                      // the relation's last row
+        }
+        if (tails) {
+#pragma unroll
+          for (uint32_t j = 0; j < IPT; ++j) {
+            if ((tails >> j) & 1u) {
+              const uint32_t hb = heads & ((2u << j) - 1u);
+              emit(direct, base, cf + (uint64_t)__popc(hb), key[j], hb ? racc[j] : cv + racc[j], first + j,
+                   hb ? first + (31u - __clz(hb)) : ch);
+            }
+          }
+        }
+        run.f += tfh >> 16;
+        run.v = (tfh >> 16) ? tv : run.v + tv;
+        run.h = (tfh >> 16) ? tile_row + (tfh & 0xffffu) : run.h;
+        last_key = shfl_key(key[IPT - 1], 31);
+        pending = (tile + 1) * TR < n;
+        __syncwarp();
+        if (lane == 0 && i + S < ntiles) {
+          fence_proxy_async_smem();
+          issue(i + S);
+        }
+        continue;
+      }
+      const uint32_t nvalid = first >= n ? 0u : (uint32_t)min((uint64_t)IPT, n - first);
+      Key key[IPT];
+      uint64_t val[IPT];
+#pragma unroll
+      for (uint32_t j = 0; j < IPT; ++j) {
+        key[j] = 0;
+        val[j] = 0;
+        if (j < nvalid) RA::read(st, lane * IPT + j, ks, vs, vmask, key[j], val[j]);
+      }
+      Key pk = shfl_key(key[IPT - 1], lane ? lane - 1 : 0);
+      const Key nk = shfl_key(key[0], lane < 31 ? lane + 1 : 31);
+      if (lane == 0) pk = last_key;
+      const bool next_valid = first + IPT < n;
+      uint32_t heads = 0;
+      uint64_t acc = 0;
+#pragma unroll
+      for (uint32_t j = 0; j < IPT; ++j) {
+        if (j < nvalid) {
+          const bool h = key[j] != (j ? key[j - 1] : pk) || (j == 0 && first == 0);
+          heads |= (uint32_t)h << j;
+          acc = h ? val[j] : acc + val[j];
+        }
+      }
+      // the previous tile's last row ends its run when this tile starts a new one
+      if (lane == 0 && pending && (heads & 1u)) emit(direct, base, run.f, last_key, run.v, first - 1, run.h);
+      // warp segmented scan of (f, v, h)
+      SegPair incl{(uint64_t)__popc(heads), acc, heads ? first + (31u - __clz(heads)) : 0ull};
+#pragma unroll
+      for (uint32_t o = 1; o < 32; o <<= 1) {
+        SegPair y;
+        y.f = __shfl_up_sync(0xffffffffu, incl.f, o);
+        y.v = __shfl_up_sync(0xffffffffu, incl.v, o);
+        y.h = __shfl_up_sync(0xffffffffu, incl.h, o);
+        if (lane >= o) incl = seg_op(y, incl);
+      }
+      const SegPair wtot = shfl_seg(incl, 31);
+      SegPair ex;
+      ex.f = __shfl_up_sync(0xffffffffu, incl.f, 1);
+      ex.v = __shfl_up_sync(0xffffffffu, incl.v, 1);
+      ex.h = __shfl_up_sync(0xffffffffu, incl.h, 1);
+      if (lane == 0) ex = SegPair{0, 0, 0};
+      const SegPair carry = seg_op(run, ex);
+      uint64_t racc = carry.v, hpos = carry.h;
+#pragma unroll
+      for (uint32_t j = 0; j < IPT; ++j) {
+        if (j < nvalid) {
+          const bool h = (heads >> j) & 1u;
+          racc = h ? val[j] : racc + val[j];
+          if (h) hpos = first + j;
+          bool tail;
+          if (j + 1 < nvalid) tail = (heads >> (j + 1)) & 1u;
+          else if (j + 1 < IPT) tail = true;            // last row of the relation
+          else if (!next_valid) tail = true;
+          else if (lane < 31) tail = key[j] != nk;
+          else tail = false;                            // decided with the next tile
+          if (tail) emit(direct, base, carry.f + (uint64_t)__popc(heads & ((2u << j) - 1u)), key[j], racc, first + j, hpos);
+        }
+      }
+      run = seg_op(run, wtot);
+      last_key = shfl_key(key[IPT - 1], 31);
+      pending = __shfl_sync(0xffffffffu, (uint32_t)(nvalid == IPT && next_valid), 31) != 0;
+      __syncwarp();
+      if (lane == 0 && i + S < ntiles) {
+        fence_proxy_async_smem();
+        issue(i + S);
+      }
+    }
+    // the sub-chunk's last row: its run ends here unless the next row continues it
+    if (lane == 0 && pending && ok) {
+      const uint64_t nx = t1 * TR;   // first row after the sub-chunk (< n since pending)
+      if (RA::global_key(a.rows, nx, ks) != last_key) emit(direct, base, run.f, last_key, run.v, nx - 1, run.h);
+    }
+    return run;
+  };
+
+  const SegPair wagg = run_sub(false, 0);
+  const unsigned fb = __ballot_sync(0xffffffffu, has_first);
+  const uint32_t src = fb ? (uint32_t)(__ffs(fb) - 1) : 0u;
+  first_sum = __shfl_sync(0xffffffffu, first_sum, src);
+  first_tail = __shfl_sync(0xffffffffu, first_tail, src);
+  first_key = shfl_key(first_key, src);
+  const bool wover = __any_sync(0xffffffffu, overflow);
+  const uint32_t nloc = __reduce_max_sync(0xffffffffu, max_lf);
+  if (lane == 0) s_wagg[w] = wagg;
+  __syncthreads();
+  if (t < 32) {
+    SegPair bagg{0, 0, 0};
+    for (int v = 0; v < WARPS; ++v) bagg = seg_op(bagg, s_wagg[v]);
+    lb_publish(a.records, bc, bagg);
+    const SegPair p = warp_lookback_resolve<4>(a.records, bc, bagg, a.err);
+    if (t == 0) {
+      s_pre = p;
+      const uint64_t c0 = bc * WARPS * tpc;
+      if (c0 < num_tiles && num_tiles <= c0 + WARPS * tpc) *a.d_groups = p.f + bagg.f;
+      if (n == 0 && bc == 0) *a.d_groups = 0;
+    }
+  }
+  __syncthreads();
+  SegPair pw = s_pre;
+  for (uint32_t v = 0; v < w; ++v) pw = seg_op(pw, s_wagg[v]);
+  if (fb && pw.f > 0 && lane == 0) {
+    const uint64_t g = pw.f - 1;
+    store_key(a.out_keys, g, a.out_key_bytes, first_key);
+    if (a.out_sums) a.out_sums[g] = (int64_t)(pw.v + first_sum);
+    if (a.out_counts) a.out_counts[g] = (uint32_t)(first_tail - pw.h + 1);
+  }
+  if (wover) {
+    run_sub(true, pw.f);
+  } else {
+    for (uint32_t l = lane; l < nloc; l += 32) {
+      const uint64_t sidx = sub * ca.cap + l, g = pw.f + l;
+      if (a.out_key_bytes == 4) reinterpret_cast<uint32_t*>(a.out_keys)[g] = reinterpret_cast<const uint32_t*>(ca.s_keys)[sidx];
+      else if (a.out_key_bytes == 8) reinterpret_cast<uint64_t*>(a.out_keys)[g] = reinterpret_cast<const uint64_t*>(ca.s_keys)[sidx];
+      else reinterpret_cast<uint4*>(a.out_keys)[g] = reinterpret_cast<const uint4*>(ca.s_keys)[sidx];
+      if (a.out_sums) a.out_sums[g] = ca.s_sums[sidx];
+      if (a.out_counts) a.out_counts[g] = ca.s_counts[sidx];
+    }
+  }
+  if (!ok && lane == 0) raise_error(a.err, kErrTimeout);
+}
+
 }  // namespace rfx

@@ -20,6 +20,7 @@ struct Entry {
 
 std::mutex g_mu;
 int g_mode = -1;  // -1: not read from the environment yet
+std::map<uint32_t, int> g_force;  // op -> pinned variant
 std::map<std::tuple<int, uint32_t, uint64_t, uint32_t>, Entry> g_table;  // (device, op, shape, class)
 
 int mode_locked() {
@@ -49,6 +50,11 @@ bool tune_enabled() {
 int tune_pick(uint32_t op, uint64_t shape, uint64_t n, int ncand, const std::function<rfx_status(int)>& run,
               cudaStream_t stream) {
   if (ncand <= 1) return 0;
+  {
+    std::lock_guard<std::mutex> lk(g_mu);
+    auto f = g_force.find(op);
+    if (f != g_force.end() && f->second < ncand) return f->second;
+  }
   int dev = 0;
   cudaGetDevice(&dev);
   const auto key = std::make_tuple(dev, op, shape, size_class(n));
@@ -104,6 +110,15 @@ int tune_pick(uint32_t op, uint64_t shape, uint64_t n, int ncand, const std::fun
 extern "C" void rfx_tune_set(int mode) {
   std::lock_guard<std::mutex> lk(rfx::g_mu);
   rfx::g_mode = mode == 1 ? 1 : 0;
+}
+
+// Pins operator `op` to `variant` (ahead of tuning and the default); variant < 0 unpins.
+extern "C" void rfx_tune_force(uint32_t op, int variant) {
+  std::lock_guard<std::mutex> lk(rfx::g_mu);
+  if (variant < 0)
+    rfx::g_force.erase(op);
+  else
+    rfx::g_force[op] = variant;
 }
 
 extern "C" void rfx_tune_reset(void) {

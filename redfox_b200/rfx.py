@@ -530,6 +530,8 @@ def _declare_tune():
     LIB.rfx_tune_set.argtypes = [C.c_int]
     LIB.rfx_tune_reset.restype = None
     LIB.rfx_tune_reset.argtypes = []
+    LIB.rfx_tune_force.restype = None
+    LIB.rfx_tune_force.argtypes = [C.c_uint32, C.c_int]
     LIB.rfx_tune_dump.restype = C.c_size_t
     LIB.rfx_tune_dump.argtypes = [C.c_char_p, C.c_size_t]
 
@@ -543,6 +545,11 @@ def tune(mode=1):
     """1: time each operator variant on first use per (shape, size class) and keep the
     fastest; 0: run the defaults."""
     LIB.rfx_tune_set(int(mode))
+
+
+def tune_force(op, variant):
+    """Pin operator `op` (a TUNE_OPS key) to a variant; variant < 0 unpins it."""
+    LIB.rfx_tune_force(op, variant)
 
 
 def tune_reset():

@@ -94,3 +94,19 @@ def test_reduce_tuples_repeat_is_stable(cuda):
     b = _run(cuda, rows, 96, 0, 64, 4)
     for x, y in zip(a, b):
         assert np.array_equal(x, y)
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2, 3], ids=["warps", "chunked", "lookback256", "lookback128"])
+@pytest.mark.parametrize("n,distinct", [(5000, 3), (300001, 1), (1 << 20, 1 << 18), (3_000_000, 2_999_000),
+                                        (2_000_003, 40000)])
+def test_reduce_tuples_variants(cuda, variant, n, distinct):
+    """Every staged variant: long runs across chunks, groups over the chunked form's
+    scratch share (its second pass), and the join-output shape."""
+    rows = _rows(n, 16, 96, distinct, seed=n + 7)
+    R.tune_force(1, variant)
+    try:
+        k, s, c = _run(cuda, rows, 96, 0, 64, 4)
+    finally:
+        R.tune_force(1, -1)
+    ek, es, ec = _expect(rows, 96, 0, 64, 4)
+    assert np.array_equal(k, ek) and np.array_equal(s, es) and np.array_equal(c, ec)

@@ -1051,6 +1051,12 @@ __global__ void __launch_bounds__(WARPS * 32, 2) reduce_warps_kernel(const __gri
         uint64_t val[IPT], racc[IPT];
 #pragma unroll
         for (uint32_t j = 0; j < IPT; ++j) RA::read(st, lane * IPT + j, ks, vs, vmask, key[j], val[j]);
+        // the rows are in registers: refill the stage now
+        __syncwarp();
+        if (lane == 0 && i + S < ntiles) {
+          fence_proxy_async_smem();
+          issue(i + S);
+        }
         Key pk = shfl_key(key[IPT - 1], lane ? lane - 1 : 0);
         const Key nk = shfl_key(key[0], lane < 31 ? lane + 1 : 31);
         if (lane == 0) pk = last_key;
@@ -1097,14 +1103,23 @@ __global__ void __launch_bounds__(WARPS * 32, 2) reduce_warps_kernel(const __gri
         } else if ((tile + 1) * TR >= n) {
           tails |= 1u << (IPT - 1);                      // the relation's last row
         }
-        if (tails) {
+        // one round per run end of the lane with the most: each lane takes its lowest
+        // remaining end (the row's key and running sum picked by compare-select)
+        while (__any_sync(0xffffffffu, tails != 0)) {
+          if (tails) {
+            const uint32_t j = (uint32_t)__ffs(tails) - 1u;
+            tails &= tails - 1u;
+            Key kj = key[0];
+            uint64_t rj = racc[0];
 #pragma unroll
-          for (uint32_t j = 0; j < IPT; ++j) {
-            if ((tails >> j) & 1u) {
-              const uint32_t hb = heads & ((2u << j) - 1u);
-              emit(direct, base, cf + (uint64_t)__popc(hb), key[j], hb ? racc[j] : cv + racc[j], first + j,
-                   hb ? first + (31u - __clz(hb)) : ch);
-            }
+            for (uint32_t jj = 1; jj < IPT; ++jj)
+              if (jj == j) {
+                kj = key[jj];
+                rj = racc[jj];
+              }
+            const uint32_t hb = heads & ((2u << j) - 1u);
+            emit(direct, base, cf + (uint64_t)__popc(hb), kj, hb ? rj : cv + rj, first + j,
+                 hb ? first + (31u - __clz(hb)) : ch);
           }
         }
         run.f += tfh >> 16;
@@ -1112,11 +1127,6 @@ __global__ void __launch_bounds__(WARPS * 32, 2) reduce_warps_kernel(const __gri
         run.h = (tfh >> 16) ? tile_row + (tfh & 0xffffu) : run.h;
         last_key = shfl_key(key[IPT - 1], 31);
         pending = (tile + 1) * TR < n;
-        __syncwarp();
-        if (lane == 0 && i + S < ntiles) {
-          fence_proxy_async_smem();
-          issue(i + S);
-        }
         continue;
       }
       const uint32_t nvalid = first >= n ? 0u : (uint32_t)min((uint64_t)IPT, n - first);

@@ -50,7 +50,35 @@ def parse():
                     help="queries of the batched join+aggregate comparison (0: skip it)")
     ap.add_argument("--serving-queries", type=int, default=150,
                     help="queries per arrival rate of the serving comparison (0: skip it)")
+    ap.add_argument("--section", default=None, choices=["strings_f64", "batched", "serving"],
+                    help="run one secondary benchmark alone and print its JSON (used by the main run, "
+                         "which gives each secondary benchmark a fresh process and allocator)")
     return ap.parse_args()
+
+
+def run_section(name, args):
+    """A secondary benchmark in a fresh process: its timings then do not depend on the
+    allocator and memory state the earlier benchmarks left behind."""
+    cmd = [sys.executable, os.path.abspath(__file__), "--section", name,
+           "--batched-queries", str(args.batched_queries), "--serving-queries", str(args.serving_queries)]
+    p = subprocess.run(cmd, capture_output=True, text=True)
+    lines = [ln for ln in p.stdout.splitlines() if ln.startswith("{")]
+    if p.returncode != 0 or not lines:
+        return {"error": "section %s exited %d: %s" % (name, p.returncode, p.stderr.strip().splitlines()[-1:])}
+    return json.loads(lines[-1])
+
+
+def main_section(args):
+    import torch
+    dev = torch.device("cuda:0")
+    if args.section == "strings_f64":
+        out = string_f64_benchmarks(dev, measured_peak_hbm()[0])
+    elif args.section == "batched":
+        out = batched_benchmark(dev, args.batched_queries)
+    else:
+        out = serving_benchmark(dev, args.serving_queries)
+    print(json.dumps(out), flush=True)
+    return 0
 
 
 # ------------------------------------------------------------------------------ clocks
@@ -267,14 +295,25 @@ def main_reference(args):
 # ------------------------------------------------------------------------------ per operator
 def _time_ms(fn, reps, setup=None):
     """Mean device time of fn() over `reps` calls (CUDA events on the current stream)
-    after one untimed call (first-call host set-up: tensor maps, launch attributes);
-    setup() runs before each call outside the timed interval."""
+    after one untimed call (first-call host set-up: tensor maps, launch attributes).
+    Without setup the calls run back to back between one pair of events, so the host's
+    time to enqueue a call overlaps the previous call on the device; with setup(), which
+    runs before each call outside the timed interval, each call has its own events."""
     import torch
     stream = torch.cuda.current_stream()
     if setup is not None:
         setup()
     fn()
     torch.cuda.synchronize()
+    if setup is None:
+        a = torch.cuda.Event(enable_timing=True)
+        b = torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            fn()
+        b.record(stream)
+        b.synchronize()
+        return a.elapsed_time(b) / reps
     total = 0.0
     for _ in range(reps):
         if setup is not None:
@@ -806,15 +845,16 @@ def main_ours(args):
         if world == 1 and not args.no_operators:
             del dev_in_keep
             result["operators"] = operator_benchmarks(dev, rows, peak)
-            result["operators"].update(string_f64_benchmarks(dev, peak))
             result["tuning"] = tuning_benchmark(dev, rows)
-        if world == 1 and args.batched_queries > 0:
+        if world == 1:
             del rows
             torch.cuda.empty_cache()
-            result["batched"] = batched_benchmark(dev, args.batched_queries)
-        if world == 1 and args.serving_queries > 0:
-            torch.cuda.empty_cache()
-            result["serving"] = serving_benchmark(dev, args.serving_queries)
+            if not args.no_operators:
+                result["operators"].update(run_section("strings_f64", args))
+            if args.batched_queries > 0:
+                result["batched"] = run_section("batched", args)
+            if args.serving_queries > 0:
+                result["serving"] = run_section("serving", args)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -827,6 +867,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         return main_reference(args)
+    if args.section:
+        return main_section(args)
     return main_ours(args)
 
 

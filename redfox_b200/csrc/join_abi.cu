@@ -35,9 +35,10 @@ FbLayout fb_layout(void* ws, uint64_t nl, bool with_offsets) {
 template <int LE, int RE>
 rfx_status launch_fb(FindBoundsArgs& a, cudaStream_t s) {
   auto k = find_bounds_kernel<LE, RE>;
+  RFX_CUDA_TRY(allow_smem((const void*)k, kFbWindowBytes));
   const uint64_t tiles = (a.nl + kFbTile - 1) / kFbTile;
-  const int grid = persistent_grid((const void*)k, kJoinThreads, 0, tiles ? tiles : 1);
-  k<<<grid, kJoinThreads, 0, s>>>(a);
+  const int grid = persistent_grid((const void*)k, kJoinThreads, kFbWindowBytes, tiles ? tiles : 1);
+  k<<<grid, kJoinThreads, kFbWindowBytes, s>>>(a);
   RFX_CUDA_TRY(cudaGetLastError());
   return RFX_OK;
 }

@@ -58,13 +58,10 @@ __device__ __forceinline__ uint64_t block_exclusive_u64(uint64_t x, uint64_t* s_
   return wpre + incl - x;
 }
 
-// Right-side keys a block's left keys can match, staged in shared memory: u64 keys for
-// containers up to 8 bytes, u128 above.
-template <int RE>
-struct Window {
-  typedef typename std::conditional<(RE <= 8), uint64_t, u128>::type T;
-  static constexpr int CAP = RE <= 8 ? 4096 : 2048;
-};
+// Right-side keys a block's left keys can match, staged in dynamic shared memory
+// (kFbWindowBytes): u64 keys when the key (container >> shift) has at most 64 bits, u128
+// otherwise.  A window that does not fit falls back to searches in global memory.
+constexpr uint32_t kFbWindowBytes = 64 * 1024;
 
 template <typename T>
 __device__ __forceinline__ uint32_t smem_bound(const T* w, uint32_t n, u128 k, bool strict) {
@@ -80,13 +77,15 @@ __device__ __forceinline__ uint32_t smem_bound(const T* w, uint32_t n, u128 k, b
 
 template <int LE, int RE>
 __global__ void __launch_bounds__(kJoinThreads) find_bounds_kernel(const FindBoundsArgs a) {
-  typedef typename Window<RE>::T WT;
-  constexpr int CAP = Window<RE>::CAP;
+  extern __shared__ __align__(16) uint8_t fb_window[];
+  uint64_t* s_win64 = reinterpret_cast<uint64_t*>(fb_window);
+  u128* s_win128 = reinterpret_cast<u128*>(fb_window);
+  const bool key64 = RE <= 8 || (uint32_t)RE * 8u - a.rshift <= 64u;
+  const uint64_t CAP = key64 ? kFbWindowBytes / 8 : kFbWindowBytes / 16;
   __shared__ uint64_t s_warp[kJoinThreads / 32];
   __shared__ uint64_t s_prefix;
   __shared__ uint32_t s_tile;
   __shared__ uint64_t s_lo, s_hi;
-  __shared__ WT s_win[CAP];
   const uint32_t t = threadIdx.x;
   const uint64_t num_tiles = (a.nl + kFbTile - 1) / kFbTile;
   const KeyView<LE> L{a.left, a.nl, a.lshift};
@@ -99,13 +98,22 @@ __global__ void __launch_bounds__(kJoinThreads) find_bounds_kernel(const FindBou
     const uint64_t tfirst = tile * kFbTile;
     const uint64_t tlast = min(tfirst + kFbTile, a.nl) - 1;
     // the window of right keys between the tile's smallest and largest left key
-    if (t == 0) s_lo = bsearch<RE>(R, L.key(tfirst), 0, a.nr, false);
-    if (t == 32) s_hi = bsearch<RE>(R, L.key(tlast), 0, a.nr, true);
+    if (t < 32) {
+      const uint64_t lo = warp_search<RE>(R, L.key(tfirst), 0, a.nr, false);
+      if (t == 0) s_lo = lo;
+    } else if (t < 64) {
+      const uint64_t hi = warp_search<RE>(R, L.key(tlast), 0, a.nr, true);
+      if (t == 32) s_hi = hi;
+    }
     __syncthreads();
     const uint64_t wlo = s_lo, wn = s_hi > s_lo ? s_hi - s_lo : 0;
-    const bool staged = wn <= (uint64_t)CAP;
-    if (staged)
-      for (uint64_t x = t; x < wn; x += kJoinThreads) s_win[x] = (WT)R.key(wlo + x);
+    const bool staged = wn <= CAP;
+    if (staged) {
+      if (key64)
+        for (uint64_t x = t; x < wn; x += kJoinThreads) s_win64[x] = (uint64_t)R.key(wlo + x);
+      else
+        for (uint64_t x = t; x < wn; x += kJoinThreads) s_win128[x] = R.key(wlo + x);
+    }
     __syncthreads();
     const uint64_t first = tfirst + (uint64_t)t * kFbIPT;
     uint64_t lo[kFbIPT], cnt[kFbIPT];
@@ -124,9 +132,12 @@ __global__ void __launch_bounds__(kJoinThreads) find_bounds_kernel(const FindBou
         cnt[j] = phi - plo;
       } else {
         uint64_t l, h;
-        if (staged) {
-          l = wlo + smem_bound<WT>(s_win, (uint32_t)wn, k, false);
-          h = wlo + smem_bound<WT>(s_win, (uint32_t)wn, k, true);
+        if (staged && key64) {
+          l = wlo + smem_bound<uint64_t>(s_win64, (uint32_t)wn, k, false);
+          h = wlo + smem_bound<uint64_t>(s_win64, (uint32_t)wn, k, true);
+        } else if (staged) {
+          l = wlo + smem_bound<u128>(s_win128, (uint32_t)wn, k, false);
+          h = wlo + smem_bound<u128>(s_win128, (uint32_t)wn, k, true);
         } else {
           l = j == 0 ? bsearch<RE>(R, k, 0, a.nr, false) : gallop<RE>(R, k, phi, false);
           h = gallop<RE>(R, k, l, true);
@@ -186,6 +197,25 @@ __device__ __forceinline__ uint64_t owner_scan(const int32_t* scan, uint64_t n, 
   return lo - 1;
 }
 
+// owner_scan found by one warp in ~log32(nl) rounds (all lanes return it).
+__device__ __forceinline__ uint64_t owner_scan_warp(const int32_t* scan, uint64_t n, uint64_t k) {
+  const uint32_t lane = threadIdx.x & 31;
+  uint64_t lo = 0, hi = n;   // the first index with scan > k lies in [lo, hi]
+  while (hi - lo > 32) {
+    const uint64_t step = (hi - lo + 31) / 32;
+    const uint64_t p = lo + lane * step;
+    const bool le = p < hi && (uint64_t)(uint32_t)__ldg(scan + p) <= k;
+    const uint32_t cnt = __popc(__ballot_sync(0xffffffffu, le));
+    if (cnt == 0) return lo - 1;   // lo > 0 here: scan[lo - 1] <= k held on entry
+    const uint64_t nlo = lo + (uint64_t)(cnt - 1) * step + 1;
+    const uint64_t nhi = cnt < 32 ? min(hi, lo + (uint64_t)cnt * step) : hi;
+    lo = nlo;
+    hi = nhi;
+  }
+  const bool le = lo + lane < hi && (uint64_t)(uint32_t)__ldg(scan + lo + lane) <= k;
+  return lo + __popc(__ballot_sync(0xffffffffu, le)) - 1;
+}
+
 __global__ void __launch_bounds__(kJoinThreads)
 join_expand_kernel(int32_t* __restrict__ li, int32_t* __restrict__ ri, uint64_t nout_max, const uint64_t* d_nout,
                    const int32_t* __restrict__ lb, const int32_t* __restrict__ scan, uint64_t nl) {
@@ -197,8 +227,13 @@ join_expand_kernel(int32_t* __restrict__ li, int32_t* __restrict__ ri, uint64_t 
   if (d_nout) nout = min(nout, *d_nout);
   for (uint64_t k0 = (uint64_t)blockIdx.x * kExpTile; k0 < nout; k0 += (uint64_t)gridDim.x * kExpTile) {
     const uint64_t k1 = min(k0 + (uint64_t)kExpTile, nout);
-    if (t == 0) s_i0 = owner_scan(scan, nl, k0);
-    if (t == 32) s_i1 = owner_scan(scan, nl, k1 - 1);
+    if (t < 32) {
+      const uint64_t i0 = owner_scan_warp(scan, nl, k0);
+      if (t == 0) s_i0 = i0;
+    } else if (t < 64) {
+      const uint64_t i1 = owner_scan_warp(scan, nl, k1 - 1);
+      if (t == 32) s_i1 = i1;
+    }
     __syncthreads();
     const uint64_t i0 = s_i0, span = s_i1 - i0 + 1;
     const bool staged = span <= (uint64_t)kExpCap;
@@ -347,25 +382,82 @@ __device__ __forceinline__ uint64_t owner_global(const uint64_t* off, uint64_t n
   return lo - 1;
 }
 
+// The same index found by one warp in ~log32(n) rounds of 32 loads in flight each
+// (instead of ~log2(n) dependent loads); all lanes return it.
+__device__ __forceinline__ uint64_t owner_warp(const uint64_t* off, uint64_t n, uint64_t k) {
+  const uint32_t lane = threadIdx.x & 31;
+  uint64_t lo = 0, hi = n;   // the first index with off > k lies in [lo, hi]
+  while (hi - lo > 32) {
+    const uint64_t step = (hi - lo + 31) / 32;
+    const uint64_t p = lo + lane * step;
+    const bool le = p < hi && __ldg(off + p) <= k;
+    const uint32_t cnt = __popc(__ballot_sync(0xffffffffu, le));
+    if (cnt == 0) return lo - 1;   // lo > 0 here: off[lo - 1] <= k held on entry to this round
+    const uint64_t nlo = lo + (uint64_t)(cnt - 1) * step + 1;
+    const uint64_t nhi = cnt < 32 ? min(hi, lo + (uint64_t)cnt * step) : hi;
+    lo = nlo;
+    hi = nhi;
+  }
+  const bool le = lo + lane < hi && __ldg(off + lo + lane) <= k;
+  return lo + __popc(__ballot_sync(0xffffffffu, le)) - 1;
+}
+
 template <int LE, int RE, int OE>
 __global__ void __launch_bounds__(kJoinThreads) tuple_join_kernel(const TupleJoinArgs a) {
   __shared__ uint64_t s_off[kStageCap + 1];
   __shared__ uint64_t s_lb[kStageCap];
+  __shared__ uint32_t s_own[kExpTile];      // staged row owning each output of the tile
+  __shared__ uint32_t s_wmax[kJoinThreads / 32];
   __shared__ uint64_t s_i0, s_i1;
-  const uint32_t t = threadIdx.x;
+  const uint32_t t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const uint64_t total = a.off64[a.nl];
   const uint64_t nout = total < a.cap ? total : a.cap;
   const u128 rmask = a.rv_bits >= 128 ? ~(u128)0 : (((u128)1 << a.rv_bits) - 1);
   for (uint64_t k0 = (uint64_t)blockIdx.x * kExpTile; k0 < nout; k0 += (uint64_t)gridDim.x * kExpTile) {
     const uint64_t k1 = min(k0 + (uint64_t)kExpTile, nout);
-    if (t == 0) s_i0 = owner_global(a.off64, a.nl, k0);
-    if (t == 32) s_i1 = owner_global(a.off64, a.nl, k1 - 1);
+    if (t < 32) {
+      const uint64_t i0 = owner_warp(a.off64, a.nl, k0);
+      if (t == 0) s_i0 = i0;
+    } else if (t < 64) {
+      const uint64_t i1 = owner_warp(a.off64, a.nl, k1 - 1);
+      if (t == 32) s_i1 = i1;
+    }
     __syncthreads();
     const uint64_t i0 = s_i0, span = s_i1 - i0 + 1;
     const bool staged = span <= (uint64_t)kStageCap;
     if (staged) {
       for (uint64_t x = t; x <= span; x += kJoinThreads) s_off[x] = __ldg(a.off64 + i0 + x);
       for (uint64_t x = t; x < span; x += kJoinThreads) s_lb[x] = __ldg(a.lb64 + i0 + x);
+      for (uint32_t x = t; x < (uint32_t)kExpTile; x += kJoinThreads) s_own[x] = 0;
+    }
+    __syncthreads();
+    if (staged) {
+      // each staged row with outputs marks its first output in the tile (row 0 owns the
+      // tile's start); an inclusive max-scan then gives every output its row (the
+      // load-balancing search of a merge-path join, without a search per output)
+      for (uint64_t x = 1 + t; x < span; x += kJoinThreads)
+        if (s_off[x] < k1 && s_off[x + 1] > s_off[x]) s_own[s_off[x] - k0] = (uint32_t)x;
+      __syncthreads();
+      constexpr uint32_t PER = kExpTile / kJoinThreads;
+      uint32_t m = 0, v[PER];
+#pragma unroll
+      for (uint32_t j = 0; j < PER; ++j) {
+        m = max(m, s_own[t * PER + j]);
+        v[j] = m;
+      }
+      uint32_t inc = m;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= (uint32_t)o) inc = max(inc, y);
+      }
+      if (lane == 31) s_wmax[warp] = inc;
+      uint32_t ex = __shfl_up_sync(0xffffffffu, inc, 1);
+      if (lane == 0) ex = 0;
+      __syncthreads();
+      for (uint32_t w = 0; w < warp; ++w) ex = max(ex, s_wmax[w]);
+#pragma unroll
+      for (uint32_t j = 0; j < PER; ++j) s_own[t * PER + j] = max(v[j], ex);
     }
     __syncthreads();
     // outputs striped over the block: consecutive threads write consecutive rows
@@ -375,15 +467,10 @@ __global__ void __launch_bounds__(kJoinThreads) tuple_join_kernel(const TupleJoi
       if (k >= k1) break;
       uint64_t i, offi, lbi;
       if (staged) {
-        uint32_t lo = 0, hi = (uint32_t)span;
-        while (lo < hi) {
-          const uint32_t mid = (lo + hi) >> 1;
-          if (s_off[mid] <= k) lo = mid + 1;
-          else hi = mid;
-        }
-        i = i0 + lo - 1;
-        offi = s_off[lo - 1];
-        lbi = s_lb[lo - 1];
+        const uint32_t x = s_own[k - k0];
+        i = i0 + x;
+        offi = s_off[x];
+        lbi = s_lb[x];
       } else {
         i = owner_global(a.off64, a.nl, k);
         offi = __ldg(a.off64 + i);

@@ -221,35 +221,6 @@ __global__ void __launch_bounds__(kSetThreads) set_filter_kernel(const SetFilter
   if (p.na == 0 && blockIdx.x == 0 && t == 0) *p.d_count = 0;
 }
 
-// Warp-cooperative search: the first index in [lo, hi) whose key is >= k (> k when
-// strict), or hi.  Each round the 32 lanes probe 32 evenly spaced keys and the range
-// shrinks 32-fold, so a search over millions of keys costs ~5 dependent round trips
-// instead of ~22 for a one-thread binary search.  All lanes return the same index.
-template <int E>
-__device__ __forceinline__ uint64_t warp_search(const KeyView<E>& v, u128 k, uint64_t lo, uint64_t hi, bool strict) {
-  const uint32_t lane = threadIdx.x & 31;
-  while (hi - lo > 32) {
-    const uint64_t step = (hi - lo + 31) / 32;
-    const uint64_t p = lo + lane * step;
-    bool before = false;
-    if (p < hi) {
-      const u128 m = v.key(p);
-      before = strict ? (m <= k) : (m < k);
-    }
-    const uint32_t cnt = __popc(__ballot_sync(0xffffffffu, before));
-    if (cnt == 0) return lo;
-    const uint64_t nlo = lo + (uint64_t)(cnt - 1) * step + 1;
-    const uint64_t nhi = cnt < 32 ? min(hi, lo + (uint64_t)cnt * step) : hi;
-    lo = nlo;
-    hi = nhi;
-  }
-  bool before = false;
-  if (lo + lane < hi) {
-    const u128 m = v.key(lo + lane);
-    before = strict ? (m <= k) : (m < k);
-  }
-  return lo + __popc(__ballot_sync(0xffffffffu, before));
-}
 
 // Per tile of A (TILE elements): the start of the run of equal values containing the
 // tile's first element, and the window of B that can equal the tile's values -- one warp

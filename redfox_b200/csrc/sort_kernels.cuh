@@ -250,8 +250,15 @@ sort_pass_kernel(const SortPassArgs a) {
     for (int j = 0; j < IPT; ++j) {
       const uint32_t li = wbase + j * 32 + lane;
       const bool valid = li < tcount;
-      const uint32_t d = valid ? (elem_bits<K>(key[j], a.shift) & a.mask) : kRadix + 1;
-      const unsigned peers = __match_any_sync(0xffffffffu, d);
+      const uint32_t d = valid ? (elem_bits<K>(key[j], a.shift) & a.mask) : 0u;
+      // lanes with the same digit: the intersection of the 8 digit-bit ballots (valid
+      // lanes only)
+      unsigned peers = __ballot_sync(0xffffffffu, valid);
+#pragma unroll
+      for (int b = 0; b < 8; ++b) {
+        const unsigned bb = __ballot_sync(0xffffffffu, (d >> b) & 1u);
+        peers &= ((d >> b) & 1u) ? bb : ~bb;
+      }
       const unsigned lower = peers & ((1u << lane) - 1);
       uint32_t base = 0;
       if (valid) base = whist[warp][d];

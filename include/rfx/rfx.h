@@ -300,9 +300,9 @@ size_t rfx_reduce_f64_workspace(uint64_t n);
  * error).  NaN if a term is NaN or both infinities occur, an infinity if one occurs, -0
  * only when every term is -0.  RFX_F64_MIN is the reference's fold acc = acc < v ? acc : v
  * bit for bit (a later equal element replaces an earlier one; a NaN replaces the
- * accumulator and the next element replaces the NaN).  Sums return after `stream`
- * drains (a value far below the largest one triggers a second, full-range pass).
- * n < 2^30. */
+ * accumulator and the next element replaces the NaN).  Stream-ordered; a value whose bits
+ * fall more than 2^107 below the largest one makes a second, full-range pass do the work
+ * (decided on the device).  n < 2^30. */
 rfx_status rfx_reduce_f64(const void* keys, uint64_t n, uint32_t key_bytes, const double* values,
                           uint32_t op, void* out_keys, double* out_values, uint64_t* d_groups,
                           void* workspace, size_t workspace_bytes, void* stream);

@@ -9,8 +9,9 @@
 // floating-point tree, whose rounding follows its shape.  The fast window is W = 3 limbs
 // with L set from the largest exponent in the input (a pre-pass): exact for every value
 // within 2^107 of the largest, with room for 2^30 terms.  A value below that window with
-// bits that would be lost raises a flag and the reduction re-runs with W = 34 limbs and
-// L = -1074, which covers every finite double.  Specials
+// bits that would be lost raises a flag, and a second pass with W = 34 limbs and
+// L = -1074, which covers every finite double, runs -- its kernels are always enqueued and
+// return at once unless the flag is set, so no host round trip is needed.  Specials
 // follow IEEE addition: NaN if any NaN or both infinities, else the infinity, and an
 // exact zero is -0 only when every term is -0.
 //
@@ -20,11 +21,12 @@
 // combination of run summaries, so the parallel result equals the sequential one bit for
 // bit.
 //
-// Structure (three kernels plus a fix-up over tiles): tiles of 2048 elements, persistent
-// CTAs; the run index of every head comes from a decoupled look-back on head counts; each
-// tile reduces its runs in registers and a segmented scan over threads, writes every run
-// that starts and ends inside it, and leaves the partial before its first head and the
-// partial from its last head for the fix-up, which is a segmented scan over tiles.
+// Structure: units of 4096 elements, one warp per unit.  A pre-pass counts each unit's run
+// heads (taking the exponent maximum for sums) and one block scans the counts into each
+// unit's first run index; the main pass folds a unit in registers and warp shuffles,
+// writes every run that starts and ends inside it at its final index, and leaves the
+// partial before its first head and the partial from its last head for the fix-up, a
+// segmented scan over units that closes the runs crossing units.
 #include <cstring>
 
 #include "host_common.h"
@@ -297,6 +299,18 @@ __device__ __forceinline__ T shfl_up_any(const T& x, int delta) {
   return r;
 }
 
+template <typename T>
+__device__ __forceinline__ T shfl_any(const T& x, int src) {
+  constexpr int W = (int)((sizeof(T) + 3) / 4);
+  uint32_t w[W];
+  memcpy(w, &x, sizeof(T));
+#pragma unroll
+  for (int i = 0; i < W; ++i) w[i] = __shfl_sync(0xffffffffu, w[i], src);
+  T r;
+  memcpy(&r, w, sizeof(T));
+  return r;
+}
+
 // Exclusive segmented scan over the NT threads of a block (thread order); also returns the
 // block's inclusive total.  `warp_tot` holds NT / 32 entries.
 template <class Op, int NT>
@@ -349,8 +363,11 @@ struct F64Args {
   const int* d_emax;    // max biased exponent (sums with the narrow window)
   int fixed_L;          // used when d_emax is null
   uint32_t* inexact;
+  const uint32_t* gate;   // if set, the kernels do nothing unless *gate != 0
   uint32_t* err;
 };
+
+__device__ __forceinline__ bool gated_off(const F64Args& a) { return a.gate && *a.gate == 0u; }
 
 __device__ __forceinline__ int window_L(const F64Args& a) {
   if (!a.d_emax) return a.fixed_L;
@@ -358,128 +375,11 @@ __device__ __forceinline__ int window_L(const F64Args& a) {
   return (e > 1 ? e : 1) - 1182;
 }
 
-// Largest biased exponent of the finite values (1 for subnormals and zeros).
-__global__ void f64_emax_kernel(const double* vals, uint64_t n, int* emax) {
-  int m = 1;
-  for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
-    const int eb = (int)(((unsigned long long)__double_as_longlong(vals[i]) >> 52) & 0x7ffu);
-    if (eb != 0x7ff && eb > m) m = eb;
-  }
-  m = __reduce_max_sync(0xffffffffu, m);
-  if ((threadIdx.x & 31) == 0) atomicMax(emax, m);
-}
-
-template <int KB, class Op>
-__global__ void __launch_bounds__(kF64Threads) f64_tile_kernel(F64Args a) {
-  using P = typename Op::P;
-  using S = Seg<P>;
-  __shared__ uint32_t s_cnt[kF64Threads / 32];
-  __shared__ uint64_t s_base;
-  __shared__ uint32_t s_tile;
-  __shared__ S s_warp[kF64Threads / 32];
-  const uint32_t t = threadIdx.x, lane = t & 31, warp = t >> 5;
-  const uint64_t tiles = (a.n + kF64Tile - 1) / kF64Tile;
-  const int L = window_L(a);
-  while (true) {
-    if (t == 0) s_tile = atomicAdd(a.counter, 1u);
-    __syncthreads();
-    const uint64_t tile = s_tile;
-    if (tile >= tiles) break;
-    const uint64_t first = tile * kF64Tile + (uint64_t)t * kF64Items;
-    // heads
-    uint32_t head = 0, cnt = 0;
-    Key prev = first > 0 && first < a.n ? load_key<KB>(a.keys, first - 1) : Key{0ull, 0ull};
-    Key keys[kF64Items];
-#pragma unroll
-    for (int j = 0; j < kF64Items; ++j) {
-      const uint64_t i = first + j;
-      if (i < a.n) {
-        keys[j] = load_key<KB>(a.keys, i);
-        const bool h = i == 0 || keys[j].lo != prev.lo || keys[j].hi != prev.hi;
-        head |= (uint32_t)h << j;
-        cnt += h;
-        prev = keys[j];
-      }
-    }
-    uint32_t incl = cnt;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
-      if (lane >= (uint32_t)o) incl += v;
-    }
-    if (lane == 31) s_cnt[warp] = incl;
-    __syncthreads();
-    uint32_t wpre = 0, tot = 0;
-#pragma unroll
-    for (int w = 0; w < kF64Threads / 32; ++w) {
-      if (w < (int)warp) wpre += s_cnt[w];
-      tot += s_cnt[w];
-    }
-    if (warp == 0) {
-      const uint64_t pre = lookback_exclusive(a.status, (uint32_t)tile, tot, a.err);
-      if (t == 0) {
-        s_base = pre;
-        a.tile_heads[tile] = tot;
-        a.tile_base[tile] = (uint32_t)pre;
-        if (tile == tiles - 1) *a.d_groups = pre + tot;
-      }
-    }
-    __syncthreads();
-    const uint32_t before = wpre + incl - cnt;  // heads in earlier threads of this tile
-    uint64_t run = s_base + before;             // index of the next head's run
-    // walk: runs wholly inside this thread are final here
-    P cur = Op::identity(), pfirst = Op::identity();
-    bool seen = false;
-#pragma unroll
-    for (int j = 0; j < kF64Items; ++j) {
-      const uint64_t i = first + j;
-      if (i < a.n) {
-        if ((head >> j) & 1u) {
-          if (seen) {
-            a.out_vals[run - 1] = __longlong_as_double((long long)Op::finalize(cur, L));
-          } else {
-            pfirst = cur;
-          }
-          if (a.emit)
-            reinterpret_cast<unsigned long long*>(a.out_keys)[run] = a.emit[i];
-          else
-            store_key<KB>(a.out_keys, run, keys[j]);
-          cur = Op::identity();
-          seen = true;
-          ++run;
-        }
-        Op::add(cur, a.vals[i], L, a.inexact);
-      }
-    }
-    if (!seen) pfirst = cur;
-    S x;
-    x.v = seen ? cur : pfirst;
-    x.f = seen;
-    x.pad = 0;
-    S total;
-    const S exc = block_seg_scan<Op, kF64Threads>(x, s_warp, total);
-    if (seen) {
-      // the run that ends just before this thread's first head
-      const P y = Op::combine(exc.v, pfirst);
-      if (before > 0)
-        a.out_vals[s_base + before - 1] = __longlong_as_double((long long)Op::finalize(y, L));
-      else
-        reinterpret_cast<P*>(a.tile_first)[tile] = y;  // started in an earlier tile
-    }
-    if (t == kF64Threads - 1) {
-      if (tot > 0)
-        reinterpret_cast<P*>(a.tile_last)[tile] = total.v;
-      else
-        reinterpret_cast<P*>(a.tile_first)[tile] = total.v;
-    }
-    __syncthreads();
-  }
-}
-
 // Fix-up, step 1: per chunk of kFixThreads tiles, the exclusive segmented scan of the
 // tile summaries (a tile with a head contributes its last partial, else its whole sum).
 template <class Op>
 __global__ void __launch_bounds__(kFixThreads) f64_fix_scan(F64Args a, uint64_t tiles) {
+  if (gated_off(a)) return;
   using P = typename Op::P;
   using S = Seg<P>;
   __shared__ S s_warp[kFixThreads / 32];
@@ -502,6 +402,7 @@ __global__ void __launch_bounds__(kFixThreads) f64_fix_scan(F64Args a, uint64_t 
 // Step 2: exclusive segmented scan over the chunk aggregates (one block, in order).
 template <class Op>
 __global__ void __launch_bounds__(kFixThreads) f64_fix_chunks(F64Args a, uint64_t chunks) {
+  if (gated_off(a)) return;
   using S = Seg<typename Op::P>;
   __shared__ S s_warp[kFixThreads / 32];
   __shared__ S s_carry;
@@ -536,6 +437,7 @@ __global__ void __launch_bounds__(kFixThreads) f64_fix_chunks(F64Args a, uint64_
 // previous head (the last head of an earlier tile); the last tile also closes the last run.
 template <class Op>
 __global__ void __launch_bounds__(kFixThreads) f64_fix_apply(F64Args a, uint64_t tiles) {
+  if (gated_off(a)) return;
   using P = typename Op::P;
   using S = Seg<P>;
   const uint64_t u = (uint64_t)blockIdx.x * kFixThreads + threadIdx.x;
@@ -555,6 +457,199 @@ __global__ void __launch_bounds__(kFixThreads) f64_fix_apply(F64Args a, uint64_t
     self.pad = 0;
     const S y = seg_combine<Op>(x, self);
     a.out_vals[a.tile_base[u] + a.tile_heads[u] - 1] = __longlong_as_double((long long)Op::finalize(y.v, L));
+  }
+}
+
+// ------------------------------------------------------------------ warp units
+// The default path: units of kF64UnitItems elements, one warp per unit.  A pre-pass counts
+// every unit's run heads (and takes the exponent maximum for sums); one block scans the
+// counts into each unit's first run index.  The main pass then needs nothing from other
+// units: a warp folds its unit in 256-element steps (8 per lane) with shuffles only,
+// writes every run that starts and ends inside the unit at its final index, and leaves the
+// partial before the unit's first head and the partial from its last head for the fix-up
+// above, which treats units as tiles.
+constexpr int kF64UnitItems = 4096;
+constexpr int kF64WarpIPT = 8;
+
+template <int KB>
+__global__ void __launch_bounds__(256) f64_unit_count(F64Args a, uint64_t units, int* emax) {
+  if (gated_off(a)) return;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t gw = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  int m = 1;
+  for (uint64_t u = gw; u < units; u += nw) {
+    const uint64_t e0 = u * kF64UnitItems, e1 = min(e0 + (uint64_t)kF64UnitItems, a.n);
+    uint32_t c = 0;
+    for (uint64_t e = e0 + lane; e < e1; e += 32) {
+      bool h = e == 0;
+      if constexpr (KB > 0) {
+        if (!h) {
+          const Key k = load_key<KB>(a.keys, e), pk = load_key<KB>(a.keys, e - 1);
+          h = k.lo != pk.lo || k.hi != pk.hi;
+        }
+      }
+      c += h;
+      if (emax) {
+        const int eb = (int)(((unsigned long long)__double_as_longlong(a.vals[e]) >> 52) & 0x7ffu);
+        if (eb != 0x7ff && eb > m) m = eb;
+      }
+    }
+    c = __reduce_add_sync(0xffffffffu, c);
+    if (lane == 0) a.tile_heads[u] = c;
+  }
+  if (emax) {
+    m = __reduce_max_sync(0xffffffffu, m);
+    if (lane == 0) atomicMax(emax, m);
+  }
+}
+
+// Exclusive scan of the unit head counts (one block, in order) and the number of runs.
+__global__ void __launch_bounds__(1024) f64_unit_scan(F64Args a, uint64_t units) {
+  if (gated_off(a)) return;
+  __shared__ uint32_t s_warp[32];
+  __shared__ uint64_t s_carry;
+  const uint32_t t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  if (t == 0) s_carry = 0;
+  __syncthreads();
+  for (uint64_t b = 0; b < units; b += 1024) {
+    const uint64_t u = b + t;
+    const uint32_t x = u < units ? a.tile_heads[u] : 0u;
+    uint32_t inc = x;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= (uint32_t)o) inc += y;
+    }
+    if (lane == 31) s_warp[warp] = inc;
+    __syncthreads();
+    uint32_t wpre = 0, tot = 0;
+    for (uint32_t w = 0; w < 32; ++w) {
+      if (w < warp) wpre += s_warp[w];
+      tot += s_warp[w];
+    }
+    const uint64_t carry = s_carry;
+    if (u < units) a.tile_base[u] = (uint32_t)(carry + wpre + inc - x);
+    __syncthreads();
+    if (t == 0) s_carry = carry + tot;
+    __syncthreads();
+  }
+  if (t == 0) *a.d_groups = s_carry;
+}
+
+template <int KB, class Op>
+__global__ void __launch_bounds__(256) f64_unit_kernel(F64Args a, uint64_t units) {
+  if (gated_off(a)) return;
+  using P = typename Op::P;
+  using S = Seg<P>;
+  constexpr int V = kF64WarpIPT;
+  const uint32_t lane = threadIdx.x & 31;
+  const uint64_t gw = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+  const int L = window_L(a);
+  for (uint64_t u = gw; u < units; u += nw) {
+    const uint64_t e0 = u * kF64UnitItems, e1 = min(e0 + (uint64_t)kF64UnitItems, a.n);
+    const uint64_t ubase = a.tile_base[u];
+    S carry;
+    carry.v = Op::identity();
+    carry.f = 0;
+    carry.pad = 0;
+    uint64_t heads_so_far = 0;
+    for (uint64_t tb = e0; tb < e1; tb += 32 * V) {
+      const uint64_t first = tb + (uint64_t)lane * V;
+      Key keys[V];
+      double vals[V];
+      uint32_t hm = 0;
+#pragma unroll
+      for (int j = 0; j < V; ++j) {
+        keys[j] = Key{0ull, 0ull};
+        vals[j] = 0.0;
+        if (first + j < e1) {
+          keys[j] = load_key<KB>(a.keys, first + j);
+          vals[j] = a.vals[first + j];
+        }
+      }
+      Key pk;
+      pk.lo = __shfl_sync(0xffffffffu, keys[V - 1].lo, lane ? lane - 1 : 0);
+      pk.hi = __shfl_sync(0xffffffffu, keys[V - 1].hi, lane ? lane - 1 : 0);
+      if (lane == 0 && first > 0 && first < e1) pk = load_key<KB>(a.keys, first - 1);
+#pragma unroll
+      for (int j = 0; j < V; ++j) {
+        if (first + j < e1) {
+          const Key q = j ? keys[j - 1] : pk;
+          const bool h = first + j == 0 || (KB > 0 && (keys[j].lo != q.lo || keys[j].hi != q.hi));
+          hm |= (uint32_t)h << j;
+        }
+      }
+      // run index of this lane's first head
+      const uint32_t cnt = (uint32_t)__popc(hm);
+      uint32_t inc = cnt;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= (uint32_t)o) inc += y;
+      }
+      const uint32_t ttot = __shfl_sync(0xffffffffu, inc, 31);
+      const uint64_t run_base = ubase + heads_so_far + (inc - cnt);
+      // keys at heads; runs that end inside this lane
+      P cur = Op::identity(), pfirst = Op::identity();
+      bool seen = false;
+      uint32_t r = 0;
+#pragma unroll
+      for (int j = 0; j < V; ++j) {
+        if (first + j < e1) {
+          if ((hm >> j) & 1u) {
+            if (a.emit)
+              reinterpret_cast<unsigned long long*>(a.out_keys)[run_base + r] = a.emit[first + j];
+            else
+              store_key<KB>(a.out_keys, run_base + r, keys[j]);
+            if (seen)
+              a.out_vals[run_base + r - 1] = __longlong_as_double((long long)Op::finalize(cur, L));
+            else
+              pfirst = cur;
+            cur = Op::identity();
+            seen = true;
+            ++r;
+          }
+          Op::add(cur, vals[j], L, a.inexact);
+        }
+      }
+      if (!seen) pfirst = cur;
+      // everything before this lane in the unit, then the run that ends before its first head
+      S x;
+      x.v = seen ? cur : pfirst;
+      x.f = seen;
+      x.pad = 0;
+      S incl = x;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const S y = shfl_up_any(incl, o);
+        if (lane >= (uint32_t)o) incl = seg_combine<Op>(y, incl);
+      }
+      S ex = shfl_up_any(incl, 1);
+      if (lane == 0) {
+        ex.v = Op::identity();
+        ex.f = 0;
+        ex.pad = 0;
+      }
+      const S X = seg_combine<Op>(carry, ex);
+      if (seen) {
+        const P y = Op::combine(X.v, pfirst);
+        if (X.f)
+          a.out_vals[run_base - 1] = __longlong_as_double((long long)Op::finalize(y, L));
+        else
+          reinterpret_cast<P*>(a.tile_first)[u] = y;   // the run began before this unit
+      }
+      const S tt = shfl_any(incl, 31);
+      carry = seg_combine<Op>(carry, tt);
+      heads_so_far += ttot;
+    }
+    if (lane == 0) {
+      if (carry.f)
+        reinterpret_cast<P*>(a.tile_last)[u] = carry.v;
+      else
+        reinterpret_cast<P*>(a.tile_first)[u] = carry.v;
+    }
   }
 }
 
@@ -596,9 +691,9 @@ struct F64Layout {
 };
 
 template <class Op>
-F64Layout f64_layout(void* ws, uint64_t n) {
+F64Layout f64_layout(void* ws, uint64_t n, uint64_t tile_items = kF64Tile) {
   using P = typename Op::P;
-  const uint64_t tiles = (n + kF64Tile - 1) / kF64Tile;
+  const uint64_t tiles = (n + tile_items - 1) / tile_items;
   const uint64_t chunks = (tiles + kFixThreads - 1) / kFixThreads;
   F64Layout l;
   Carver c(ws);
@@ -617,16 +712,21 @@ F64Layout f64_layout(void* ws, uint64_t n) {
   return l;
 }
 
-size_t f64_workspace(uint64_t n) {
+size_t f64_core(uint64_t n) {
   const size_t a = f64_layout<SumOp<kNarrowLimbs>>(nullptr, n).total;
   const size_t b = f64_layout<SumOp<kWideLimbs>>(nullptr, n).total;
   const size_t c = f64_layout<MinOp>(nullptr, n).total;
-  return a > b ? (a > c ? a : c) : (b > c ? b : c);
+  return align_up(a > b ? (a > c ? a : c) : (b > c ? b : c), 256);
 }
 
+// The layouts, then one word past them: the narrow pass's inexact flag, which gates the
+// full-range pass.
+size_t f64_workspace(uint64_t n) { return f64_core(n) + 256; }
+
+// The unit path: count + scan, one warp per unit, then the tile fix-up over units.
 template <int KB, class Op>
-rfx_status f64_run(F64Args a, void* ws, bool narrow_sum, int fixed_L, cudaStream_t s) {
-  const F64Layout l = f64_layout<Op>(ws, a.n);
+rfx_status f64_run_units(F64Args a, void* ws, bool narrow_sum, int fixed_L, cudaStream_t s) {
+  const F64Layout l = f64_layout<Op>(ws, a.n, kF64UnitItems);
   RFX_CUDA_TRY(cudaMemsetAsync(ws, 0, l.clear, s));
   a.status = l.status;
   a.counter = l.counter;
@@ -637,40 +737,39 @@ rfx_status f64_run(F64Args a, void* ws, bool narrow_sum, int fixed_L, cudaStream
   a.exc = l.exc;
   a.chunk_agg = l.chunk_agg;
   a.inexact = l.inexact;
-  a.d_emax = nullptr;
+  a.d_emax = narrow_sum ? l.emax : nullptr;
   a.fixed_L = fixed_L;
-  const uint64_t tiles = (a.n + kF64Tile - 1) / kF64Tile;
-  const uint64_t chunks = (tiles + kFixThreads - 1) / kFixThreads;
-  if (narrow_sum) {
-    a.d_emax = l.emax;
-    const uint64_t blocks = (a.n + 255) / 256;
-    const uint64_t cap = (uint64_t)device_sms() * 8;
-    f64_emax_kernel<<<(int)(blocks < cap ? blocks : cap), 256, 0, s>>>(a.vals, a.n, l.emax);
-    RFX_CUDA_TRY(cudaGetLastError());
-  }
-  const int grid = persistent_grid((const void*)f64_tile_kernel<KB, Op>, kF64Threads, 0, tiles);
-  f64_tile_kernel<KB, Op><<<grid, kF64Threads, 0, s>>>(a);
+  const uint64_t units = (a.n + kF64UnitItems - 1) / kF64UnitItems;
+  const uint64_t chunks = (units + kFixThreads - 1) / kFixThreads;
+  const uint64_t want = (units + 7) / 8;
+  const int gc = persistent_grid((const void*)f64_unit_count<KB>, 256, 0, want);
+  f64_unit_count<KB><<<gc, 256, 0, s>>>(a, units, narrow_sum ? l.emax : nullptr);
   RFX_CUDA_TRY(cudaGetLastError());
-  f64_fix_scan<Op><<<(int)chunks, kFixThreads, 0, s>>>(a, tiles);
+  f64_unit_scan<<<1, 1024, 0, s>>>(a, units);
+  RFX_CUDA_TRY(cudaGetLastError());
+  const int gm = persistent_grid((const void*)f64_unit_kernel<KB, Op>, 256, 0, want);
+  f64_unit_kernel<KB, Op><<<gm, 256, 0, s>>>(a, units);
+  RFX_CUDA_TRY(cudaGetLastError());
+  f64_fix_scan<Op><<<(int)chunks, kFixThreads, 0, s>>>(a, units);
   RFX_CUDA_TRY(cudaGetLastError());
   f64_fix_chunks<Op><<<1, kFixThreads, 0, s>>>(a, chunks);
   RFX_CUDA_TRY(cudaGetLastError());
-  f64_fix_apply<Op><<<(int)chunks, kFixThreads, 0, s>>>(a, tiles);
+  f64_fix_apply<Op><<<(int)chunks, kFixThreads, 0, s>>>(a, units);
   RFX_CUDA_TRY(cudaGetLastError());
   return RFX_OK;
 }
 
 template <int KB>
 rfx_status f64_dispatch_op(F64Args a, uint32_t op, void* ws, cudaStream_t s) {
-  if (op == RFX_F64_MIN) return f64_run<KB, MinOp>(a, ws, false, 0, s);
-  rfx_status st = f64_run<KB, SumOp<kNarrowLimbs>>(a, ws, true, 0, s);
+  if (op == RFX_F64_MIN) return f64_run_units<KB, MinOp>(a, ws, false, 0, s);
+  rfx_status st = f64_run_units<KB, SumOp<kNarrowLimbs>>(a, ws, true, 0, s);
   if (st != RFX_OK) return st;
-  const F64Layout l = f64_layout<SumOp<kNarrowLimbs>>(ws, a.n);
-  uint32_t inexact = 0;
-  RFX_CUDA_TRY(cudaMemcpyAsync(&inexact, l.inexact, sizeof(inexact), cudaMemcpyDeviceToHost, s));
-  RFX_CUDA_TRY(cudaStreamSynchronize(s));
-  if (!inexact) return RFX_OK;
-  return f64_run<KB, SumOp<kWideLimbs>>(a, ws, false, kWideL, s);  // values span beyond the window
+  // the full-range pass runs on the device only if the narrow window lost bits
+  const F64Layout l = f64_layout<SumOp<kNarrowLimbs>>(ws, a.n, kF64UnitItems);
+  uint32_t* gate = reinterpret_cast<uint32_t*>(static_cast<uint8_t*>(ws) + f64_core(a.n));
+  RFX_CUDA_TRY(cudaMemcpyAsync(gate, l.inexact, sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
+  a.gate = gate;
+  return f64_run_units<KB, SumOp<kWideLimbs>>(a, ws, false, kWideL, s);
 }
 
 rfx_status f64_dispatch(F64Args a, uint32_t key_bytes, uint32_t op, void* ws, cudaStream_t s) {

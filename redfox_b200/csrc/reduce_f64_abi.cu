@@ -35,9 +35,6 @@
 namespace rfx {
 namespace {
 
-constexpr int kF64Threads = 256;
-constexpr int kF64Items = 8;
-constexpr int kF64Tile = kF64Threads * kF64Items;
 constexpr int kFixThreads = 256;
 constexpr int kNarrowLimbs = 3;   // 192 bits: every value within 2^107 of the largest
 constexpr int kWideLimbs = 34;    // 2176 bits: every finite double
@@ -691,7 +688,7 @@ struct F64Layout {
 };
 
 template <class Op>
-F64Layout f64_layout(void* ws, uint64_t n, uint64_t tile_items = kF64Tile) {
+F64Layout f64_layout(void* ws, uint64_t n, uint64_t tile_items) {
   using P = typename Op::P;
   const uint64_t tiles = (n + tile_items - 1) / tile_items;
   const uint64_t chunks = (tiles + kFixThreads - 1) / kFixThreads;
@@ -713,9 +710,9 @@ F64Layout f64_layout(void* ws, uint64_t n, uint64_t tile_items = kF64Tile) {
 }
 
 size_t f64_core(uint64_t n) {
-  const size_t a = f64_layout<SumOp<kNarrowLimbs>>(nullptr, n).total;
-  const size_t b = f64_layout<SumOp<kWideLimbs>>(nullptr, n).total;
-  const size_t c = f64_layout<MinOp>(nullptr, n).total;
+  const size_t a = f64_layout<SumOp<kNarrowLimbs>>(nullptr, n, kF64UnitItems).total;
+  const size_t b = f64_layout<SumOp<kWideLimbs>>(nullptr, n, kF64UnitItems).total;
+  const size_t c = f64_layout<MinOp>(nullptr, n, kF64UnitItems).total;
   return align_up(a > b ? (a > c ? a : c) : (b > c ? b : c), 256);
 }
 

@@ -31,8 +31,6 @@ REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REPO)
 
 ROWS = 60_000_000
-WORKLOAD = ("filter-project-aggregate: 60M rows Tuple<32,64,64,64,64,8,8> (64 B), "
-            "select date<=2475 (~98%), 2 int64 products, group by (flag1,flag2) -> 6 groups SUM/COUNT")
 METRIC = "tuples/s"
 
 
@@ -160,6 +158,8 @@ def profiled_traffic(rows):
 
 
 # ------------------------------------------------------------------------------ CPU legs
+# The CPU legs import only the oracle package and redfox_b200.shapes (plain constants), so
+# the process that times the reference's CPU code never maps librfx.so.
 def cpu_threads():
     try:
         return len(os.sched_getaffinity(0))
@@ -168,124 +168,166 @@ def cpu_threads():
 
 
 def fact_oracle_descriptors():
+    """The plan's predicate and the two products as oracle descriptors:
+    date <= cutoff; price*(100-discount); price*(100-discount)*(100+tax)."""
     import oracle as O
-    from redfox_b200 import workloads as WL
+    from redfox_b200 import shapes as SH
+    cmps = [{"op": O.LE, "a": (O.OPND_VAR, SH.F_DATE), "b": (O.OPND_CONST, SH.FACT_CUTOFF), "type": O.I32}]
+    p1 = O.make_arith([(O.NODE_OP, O.MUL, O.I64, 1, 2, 0), (O.NODE_INDEX, 0, O.I64, -1, -1, SH.F_PRICE),
+                       (O.NODE_OP, O.SUB, O.I64, 3, 4, 0), (O.NODE_CONST, 0, O.I64, -1, -1, 100),
+                       (O.NODE_INDEX, 0, O.I64, -1, -1, SH.F_DISC)], 0, O.I64, 64)
+    p2 = O.make_arith([(O.NODE_OP, O.MUL, O.I64, 1, 6, 0), (O.NODE_OP, O.MUL, O.I64, 2, 3, 0),
+                       (O.NODE_INDEX, 0, O.I64, -1, -1, SH.F_PRICE), (O.NODE_OP, O.SUB, O.I64, 4, 5, 0),
+                       (O.NODE_CONST, 0, O.I64, -1, -1, 100), (O.NODE_INDEX, 0, O.I64, -1, -1, SH.F_DISC),
+                       (O.NODE_OP, O.ADD, O.I64, 7, 8, 0), (O.NODE_CONST, 0, O.I64, -1, -1, 100),
+                       (O.NODE_INDEX, 0, O.I64, -1, -1, SH.F_TAX)], 0, O.I64, 64)
+    return cmps, [p1, p2]
 
-    def oarith(e):
-        return O.make_arith([(e.nodes[i].kind, e.nodes[i].op, e.nodes[i].type, e.nodes[i].left, e.nodes[i].right,
-                              e.nodes[i].value) for i in range(e.nnodes)], e.root, e.dest_type, e.dest_bits)
-    cmps = [{"op": op, "a": a, "b": b, "type": vt} for (op, a, b, vt) in WL.fact_predicate()]
-    return cmps, [oarith(a) for a in WL.fact_ariths()]
 
-
-def cpu_rows_sample(n):
+def fact_rows_host(n):
+    """The first n rows of the seeded fact table, packed on the host (same bytes as the
+    device generator)."""
     import oracle as O
-    from redfox_b200 import workloads as WL
-    cols = [O.uniform(n, WL.FACT_SEED, f, WL.FACT_LO[f], WL.FACT_HI[f]) for f in range(7)]
-    return O.pack(WL.FACT_WIDTHS, cols)
+    from redfox_b200 import shapes as SH
+    cols = [O.uniform(n, SH.FACT_SEED, f, SH.FACT_LO[f], SH.FACT_HI[f]) for f in range(7)]
+    return O.pack(SH.FACT_WIDTHS, cols)
 
 
-def time_oracle_port(rows, threads, reps=3):
+def oracle_port_fn(threads):
+    """One run of the C oracle's filter-aggregate (OpenMP) over `rows` -> (keys, sums, counts)."""
     import oracle as O
-    from redfox_b200 import workloads as WL
+    from redfox_b200 import shapes as SH
     cmps, ariths = fact_oracle_descriptors()
-    ts = []
-    for _ in range(reps):
-        t0 = time.perf_counter()
-        O.filter_aggregate(rows, WL.FACT_WIDTHS, cmps, ariths, WL.FACT_GROUP_FIELDS, WL.FACT_SUM_FIELDS,
-                           threads=threads)
-        ts.append(time.perf_counter() - t0)
-    return len(rows) / statistics.median(ts)
+
+    def run(rows):
+        return O.filter_aggregate(rows, SH.FACT_WIDTHS, cmps, ariths, SH.FACT_GROUP_FIELDS, SH.FACT_SUM_FIELDS,
+                                  threads=threads)
+    return run
 
 
-def reference_plan_fn():
-    """ref_fact_plan from oracle/_ref (the reference's code built for the host), or None."""
+def reference_plan_fn(threads):
+    """ref_fact_plan from oracle/_ref -- the reference's Select.h / Project.h / arith device
+    code and thrust reduce_by_key compiled for the host -- over `threads` row partitions
+    in parallel, partial groups summed; None where oracle/_ref is not built."""
     import ctypes as C
+    from concurrent.futures import ThreadPoolExecutor
+
+    import numpy as np
     import oracle as O
+    from redfox_b200 import shapes as SH
     ref = O.ref_lib()
     if ref is None:
         return None
     fn = ref.ref_fact_plan
     fn.restype = C.c_int64
     fn.argtypes = [C.c_void_p, C.c_size_t, C.c_uint, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
-    return fn
+    pool = ThreadPoolExecutor(max_workers=threads)
+
+    def run(rows):
+        n = rows.shape[0]
+        cuts = [n * i // threads for i in range(threads + 1)]
+
+        def one(i):
+            sub = rows[cuts[i]:cuts[i + 1]]
+            ok = np.zeros(16, np.uint64)
+            s1 = np.zeros(16, np.int64)
+            s2 = np.zeros(16, np.int64)
+            cnt = np.zeros(16, np.uint64)
+            g = fn(sub.ctypes.data_as(C.c_void_p), sub.shape[0], SH.FACT_CUTOFF, ok.ctypes.data_as(C.c_void_p),
+                   s1.ctypes.data_as(C.c_void_p), s2.ctypes.data_as(C.c_void_p), cnt.ctypes.data_as(C.c_void_p))
+            return ok[:g], s1[:g], s2[:g], cnt[:g]
+
+        merged = {}
+        for ok, s1, s2, cnt in pool.map(one, range(threads)):   # ctypes releases the GIL
+            for k, a, b, c in zip(ok, s1, s2, cnt):
+                x = merged.get(int(k), (0, 0, 0))
+                merged[int(k)] = (x[0] + int(a), x[1] + int(b), x[2] + int(c))
+        keys = sorted(merged)
+        return (np.array(keys, np.uint64), np.array([[merged[k][0], merged[k][1]] for k in keys], np.int64),
+                np.array([merged[k][2] for k in keys], np.uint64))
+    return run
 
 
-def run_reference_plan(fn, rows, threads):
-    """The reference plan over `threads` row partitions in parallel, partial groups summed."""
-    import ctypes as C
-    from concurrent.futures import ThreadPoolExecutor
-
-    import numpy as np
-    from redfox_b200 import workloads as WL
-    parts = np.array_split(np.arange(len(rows)), threads)
-
-    def one(idx):
-        sub = np.ascontiguousarray(rows[idx[0]:idx[-1] + 1]) if len(idx) else rows[:0]
-        ok = np.zeros(16, np.uint64)
-        s1 = np.zeros(16, np.int64)
-        s2 = np.zeros(16, np.int64)
-        cnt = np.zeros(16, np.uint64)
-        g = fn(sub.ctypes.data_as(C.c_void_p), len(sub), WL.FACT_CUTOFF, ok.ctypes.data_as(C.c_void_p),
-               s1.ctypes.data_as(C.c_void_p), s2.ctypes.data_as(C.c_void_p), cnt.ctypes.data_as(C.c_void_p))
-        return {int(k): (int(a), int(b), int(c)) for k, a, b, c in zip(ok[:g], s1[:g], s2[:g], cnt[:g])}
-
-    merged = {}
-    with ThreadPoolExecutor(max_workers=threads) as ex:
-        for part in ex.map(one, parts):
-            for k, (a, b, c) in part.items():
-                x = merged.get(k, (0, 0, 0))
-                merged[k] = (x[0] + a, x[1] + b, x[2] + c)
-    return merged
+def time_steps(run, rows, steps, warmup):
+    """`warmup` untimed runs, then `steps` timed runs; returns the per-run seconds."""
+    for _ in range(warmup):
+        run(rows)
+    ts = []
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        run(rows)
+        ts.append(time.perf_counter() - t0)
+    return ts
 
 
-def cpu_baseline_line(budget_s=12.0):
-    """The oracle port on a bounded sample of the same table, all host threads."""
+def cpu_legs(rows, kind, steps=5, warmup=1, one_core=True):
+    """All-host-thread and 1-thread timings of the CPU implementation of the plan over the
+    whole table: median of `steps` runs after `warmup`, and one 1-thread run."""
     threads = cpu_threads()
-    probe = cpu_rows_sample(200_000)
-    rate = time_oracle_port(probe, threads, reps=1)
-    n = int(min(max(rate * budget_s / 3.0, 200_000), 16_000_000))
-    rows = cpu_rows_sample(n)
-    v = time_oracle_port(rows, threads, reps=3)
-    return {"value": v, "unit": "tuples/s", "cores": threads, "kind": "port",
-            "sample": "first %d rows of the same seeded table, C oracle (OpenMP), median of 3" % n}
+    make = reference_plan_fn if kind == "reference" else oracle_port_fn
+    run = make(threads)
+    if run is None:
+        return None
+    ts = time_steps(run, rows, steps, warmup)
+    n = rows.shape[0]
+    out = {"threads": threads, "seconds": ts, "median_s": statistics.median(ts), "value": n / statistics.median(ts)}
+    if one_core:
+        t1 = time_steps(make(1), rows, 1, 0)[0]
+        out["one_core"] = {"value": n / t1, "seconds": t1, "cores": 1}
+    return out
+
+
+def cpu_baseline_line(rows):
+    """The oracle port (C, OpenMP) over the whole seeded table on the host: median of 5
+    after 1 warm-up with all host threads, plus one 1-thread run."""
+    leg = cpu_legs(rows, "port")
+    return {"value": leg["value"], "unit": "tuples/s", "cores": leg["threads"], "kind": "port",
+            "sample": "the whole %d-row table (host copy of the timed input), C oracle (OpenMP), median of 5 "
+                      "after 1 warm-up" % rows.shape[0],
+            "one_core": {"value": leg["one_core"]["value"], "unit": "tuples/s", "cores": 1,
+                         "sample": "one run over the whole table"}}
+
+
+def bench_config(n, world):
+    from redfox_b200 import shapes as SH
+    return {"workload": SH.FACT_WORKLOAD, "rows_per_gpu": n, "row_bytes": SH.FACT_ROW_BYTES,
+            "l2": "inputs larger than L2 (%.2f GB per GPU), no flush" % (n * SH.FACT_ROW_BYTES / 1e9),
+            "parallelism": "dp%d (row partitions, 6-group all-reduce)" % world if world > 1 else "1 GPU"}
 
 
 # ------------------------------------------------------------------------------ reference arm
 def main_reference(args):
+    """The reference's CPU code for the plan (oracle/_ref's ref_fact_plan, or the C oracle
+    where the reference did not build) over the same 60M-row table as our arm, every host
+    thread; value = rows / median step time over the timed steps."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
     threads = cpu_threads()
-    fn = reference_plan_fn()
-    kind = "reference" if fn is not None else "port"
-    sample = 4_000_000 if fn is not None else 8_000_000
-    rows = cpu_rows_sample(sample)
-
-    def step():
-        if fn is not None:
-            run_reference_plan(fn, rows, threads)
-        else:
-            time_oracle_port(rows, threads, reps=1)
-
-    for _ in range(max(args.warmup, 1)):
-        step()
-    ts = []
-    for _ in range(args.steps):
-        t0 = time.perf_counter()
-        step()
-        ts.append(time.perf_counter() - t0)
-    sec = sum(ts) / len(ts)
-    value = sample / sec
-    what = ("reference Tuple.h/Comparisons.h/Project.h device code + thrust reduce_by_key built for the host "
-            "(oracle/_ref), %d row partitions in parallel" % threads) if fn is not None else "C oracle (OpenMP)"
+    n = args.rows
+    rows = fact_rows_host(n)
+    run = reference_plan_fn(threads)
+    kind = "reference" if run is not None else "port"
+    if run is None:
+        run = oracle_port_fn(threads)
+    ts = time_steps(run, rows, args.steps, max(args.warmup, 1))
+    med = statistics.median(ts)
+    value = n / med
+    one = time_steps((reference_plan_fn if kind == "reference" else oracle_port_fn)(1), rows, 1, 0)[0]
+    what = ("the reference's Select.h / Project.h / Tuple.h device code and thrust reduce_by_key built for the "
+            "host (oracle/_ref ref_fact_plan), %d row partitions in parallel" % threads) if kind == "reference" \
+        else "C oracle (OpenMP)"
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "tuples/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3, "higher_is_better": True,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": med * 1e3, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "rows_per_step": sample, "parallelism": "host threads"},
+        "config": bench_config(n, 1),
         "cpu_baseline": {"value": value, "unit": "tuples/s", "cores": threads, "kind": kind,
-                         "sample": "%d rows of the seeded table per step; %s" % (sample, what)},
+                         "sample": "the whole %d-row table every step; %s; median of %d steps after %d warm-up"
+                                   % (n, what, args.steps, max(args.warmup, 1)),
+                         "mean_ms_per_step": statistics.mean(ts) * 1e3,
+                         "one_core": {"value": n / one, "unit": "tuples/s", "cores": 1,
+                                      "sample": "one run over the whole table"}},
         "e2e": {"value": value, "unit": "tuples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -811,16 +853,25 @@ def main_ours(args):
         achieved = bytes_alg / (kms / 1e3) / 1e9
         traffic = profiled_traffic(n)
         cpu = None
+        parity_rows = 0
+        import numpy as np
+        import oracle as O
+        cmps, ariths = fact_oracle_descriptors()
+        sub = rows[:check_n].cpu().numpy()
+        ek, es, ec = O.filter_aggregate(sub, WL.FACT_WIDTHS, cmps, ariths, WL.FACT_GROUP_FIELDS, WL.FACT_SUM_FIELDS)
+        ok = ok and np.array_equal(keys, ek) and np.array_equal(sums, es) and np.array_equal(counts, ec)
+        parity_rows = check_n
         if not args.no_cpu_baseline and world == 1:
             try:
-                import numpy as np
-                import oracle as O
-                cmps, ariths = fact_oracle_descriptors()
-                sub = rows[:check_n].cpu().numpy()
-                ek, es, ec = O.filter_aggregate(sub, WL.FACT_WIDTHS, cmps, ariths, WL.FACT_GROUP_FIELDS,
-                                                WL.FACT_SUM_FIELDS)
-                ok = ok and np.array_equal(keys, ek) and np.array_equal(sums, es) and np.array_equal(counts, ec)
-                cpu = cpu_baseline_line()
+                host_rows = rows.cpu().numpy()
+                cpu = cpu_baseline_line(host_rows)
+                # whole-table parity: the plan's last result (the e2e steps ran it over a copy
+                # of this table) against the oracle over the same 60M rows
+                fk, fs, fc = plan.result()
+                ek, es, ec = oracle_port_fn(cpu_threads())(host_rows)
+                ok = ok and np.array_equal(fk, ek) and np.array_equal(fs, es) and np.array_equal(fc, ec)
+                parity_rows = n
+                del host_rows
             except Exception as e:  # the baseline is reported, never required
                 cpu = {"value": None, "unit": "tuples/s", "cores": cpu_threads(), "kind": "port",
                        "sample": "failed: %s" % e}
@@ -828,9 +879,7 @@ def main_ours(args):
             "metric": METRIC, "value": value, "unit": "tuples/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "int64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "rows_per_gpu": n, "row_bytes": WL.fact_row_bytes(),
-                       "l2": "inputs larger than L2 (%.2f GB per GPU), no flush" % (bytes_alg / 1e9),
-                       "parallelism": "dp%d (row partitions, 6-group all-reduce)" % world if world > 1 else "1 GPU"},
+            "config": bench_config(n, world),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
                          "kernel": "rfx_plan_aggregate (plan-specialised scan_aggregate_kernel<64>)", "kernel_ms": kms,
@@ -840,7 +889,8 @@ def main_ours(args):
                     "h2d_bytes_per_step": n * WL.fact_row_bytes(), "d2h_bytes_per_step": d2h},
             "gpu_launches": args.steps,
             "clocks": clocks,
-            "parity": "ok" if ok else "MISMATCH",
+            "parity": ("ok" if ok else "MISMATCH"),
+            "parity_rows": parity_rows,
         }
         if world == 1 and not args.no_operators:
             del dev_in_keep

@@ -466,17 +466,20 @@ rfx_status rfx_count_string_compat(const void* key_begin, const void* value_begi
                                    uint64_t* key_size, uint64_t* value_size);
 
 /* rfx_filter_aggregate for callers that cannot allocate device memory when they call it:
- * a runtime that has already handed all device memory out by liveness, code recording a
- * stream capture, or a request path that must not touch the allocator.  It has no
- * counterpart in the reference.  The arguments and outputs are rfx_filter_aggregate's
- * minus the workspace; its scratch is a fixed array inside the library (about 160 KiB,
- * held by every GPU that loads the library until exit), so it allocates nothing.
- * Limits: at most 4096 groups x (nsum + 1) <= 20480 accumulators -- a larger plan gets
- * RFX_ERR_CAPACITY.  The first call on a device looks the array's address up; make it
- * before any stream capture.  All calls share the array: calls whose kernels overlap on
- * the GPU race (order them on one stream).  A row outside the declared group domains is
- * recorded as RFX_ERR_CAPACITY in *d_error (a device word the caller zeroes; may be
- * NULL), not in the library's error word. */
+ * a runtime that has already handed all device memory out by liveness, or a request path
+ * that must not touch the allocator.  It has no counterpart in the reference.  The
+ * arguments and outputs are rfx_filter_aggregate's minus the workspace; its scratch is a
+ * fixed array inside the library (about 160 KiB, held by every GPU that loads the library
+ * until exit), so it allocates nothing.
+ * Limits: the array holds 4096 groups x (4 sums + a count), the largest plan
+ * rfx_filter_aggregate accepts; plans are validated as that entry validates them and a
+ * plan beyond its limits gets the same status (RFX_ERR_UNSUPPORTED).  The first call on a
+ * device looks the array's address up; make it before any stream capture.  No call may
+ * follow a cudaDeviceReset of that device (the address looked up before it is stale).
+ * All calls share the array: calls whose kernels overlap on the GPU race (order them on
+ * one stream).  A row outside the declared group domains is recorded as
+ * RFX_ERR_CAPACITY in *d_error (a device word the caller zeroes; may be NULL), not in
+ * the library's error word. */
 rfx_status rfx_filter_aggregate_noalloc(const void* in, uint64_t n, const rfx_tuple* in_type,
                                         const rfx_cmp* cmps, uint32_t ncmp,
                                         const rfx_arith_expr* ariths, uint32_t narith,

@@ -30,7 +30,17 @@ struct OccHash {
   }
 };
 std::unordered_map<OccKey, int, OccHash> g_occ;
-std::unordered_map<const void*, size_t> g_smem_set;
+// cudaFuncSetAttribute applies to the current device only: the opt-in is remembered per
+// (device, kernel)
+struct SmemKey {
+  int dev;
+  const void* k;
+  bool operator==(const SmemKey& o) const { return dev == o.dev && k == o.k; }
+};
+struct SmemHash {
+  size_t operator()(const SmemKey& o) const { return std::hash<const void*>()(o.k) ^ ((size_t)o.dev << 40); }
+};
+std::unordered_map<SmemKey, size_t, SmemHash> g_smem_set;
 }  // namespace
 
 int device_sms() {
@@ -60,11 +70,15 @@ uint32_t* device_error_word() {
 }
 
 cudaError_t allow_smem(const void* kernel, size_t bytes) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
   std::lock_guard<std::mutex> lk(g_mu);
-  auto it = g_smem_set.find(kernel);
+  const SmemKey key{dev, kernel};
+  auto it = g_smem_set.find(key);
   if (it != g_smem_set.end() && it->second >= bytes) return cudaSuccess;
-  cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-  if (e == cudaSuccess) g_smem_set[kernel] = bytes;
+  e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) g_smem_set[key] = bytes;
   return e;
 }
 

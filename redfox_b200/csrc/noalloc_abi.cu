@@ -3,12 +3,12 @@
 //
 // Who needs it: callers that cannot allocate device memory at call time -- a host runtime
 // that has already handed all device memory out by liveness (as the reference's Harmony
-// runtime plans its variables), code recording into a stream capture where allocation is
-// not allowed, or a serving loop that must not touch the allocator on its request path.
+// runtime plans its variables), or a serving loop that must not touch the allocator on its
+// request path.
 //
-// The scratch is g_scratch below: kScratchWords 64-bit accumulators (room for 4096 groups
-// x 4 sums + a count) plus a completion counter, about 160 KiB, held by every GPU that
-// loads the library until the process exits.  Every call uses the same array, so two
+// The scratch is g_scratch below: kScratchWords 64-bit accumulators (room for the largest
+// plan the aggregate accepts: 4096 groups x (4 sums + a count)) plus a completion counter,
+// about 160 KiB, held by every GPU that loads the library until the process exits.  Every call uses the same array, so two
 // calls whose kernels overlap on the GPU (different streams without ordering between
 // them) race and produce wrong sums; calls on one stream are ordered and safe.  The array
 // keeps the last call's contents; each call clears what must start at zero.
@@ -77,20 +77,16 @@ extern "C" rfx_status rfx_filter_aggregate_noalloc(const void* in, uint64_t n, c
                                                    uint64_t* out_keys, int64_t* out_sums, uint64_t* out_counts,
                                                    uint64_t* d_groups, uint32_t* d_error, void* stream) {
   if ((!in && n) || !out_keys || !out_counts || !d_groups || (nsum && !out_sums)) return RFX_ERR_INVALID;
-  if (!group_domain || ngroup == 0) return RFX_ERR_INVALID;
-  // the plan's accumulator table must fit the fixed scratch
-  uint64_t table = (uint64_t)nsum + 1;
-  for (uint32_t k = 0; k < ngroup; ++k) {
-    table *= group_domain[k] ? group_domain[k] : 1;
-    if (table > kScratchWords) return RFX_ERR_CAPACITY;
-  }
+  // the plan is validated exactly as rfx_filter_aggregate validates it (same statuses);
+  // every plan it accepts fits the fixed scratch, and the check below keeps that true
   ScanProgram p;
   rfx_status st = compile_scan(&p, in_type, cmps, ncmp, ariths, narith);
   if (st != RFX_OK) return st;
   st = compile_aggregate(&p, group_fields, group_domain, ngroup, sum_fields, nsum);
   if (st != RFX_OK) return st;
   const size_t nacc = (size_t)p.ngroups_total * (nsum + 1);
-  if (nacc > kScratchWords) return RFX_ERR_CAPACITY;  // larger than the fixed scratch
+  if (nacc > kScratchWords) return RFX_ERR_CAPACITY;  // larger than the fixed scratch (not reachable
+                                                      // while compile_aggregate caps the table)
   if (n && (reinterpret_cast<uintptr_t>(in) % (p.in_bytes < 16 ? p.in_bytes : 16)) != 0) return RFX_ERR_INVALID;
   unsigned long long* base = nullptr;
   st = scratch_address(&base);

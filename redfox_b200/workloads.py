@@ -3,20 +3,12 @@ and the RA plans run over them.  Inputs are seeded synthetic data of the named s
 (SplitMix64 streams, one per column; seed 0x5EED0000 + workload index).
 """
 from . import rfx as R
-
-SEED_BASE = 0x5EED0000
+from .shapes import (FACT_CUTOFF, FACT_GROUP_DOMAIN, FACT_GROUP_FIELDS, FACT_HI, FACT_LO,  # noqa: F401
+                     FACT_ROWS, FACT_SEED, FACT_SUM_FIELDS, FACT_WIDTHS, FACT_WORKLOAD, F_DATE, F_DISC,
+                     F_FLAG1, F_FLAG2, F_PRICE, F_QTY, F_TAX, SEED_BASE)
 
 # ---------------------------------------------------------------- filter-project-aggregate
-# A fact table of Tuple<32,64,64,64,64,8,8> = (date, quantity, price, discount, tax,
-# flag1, flag2) in a 64-byte container; price in fixed-point cents, discount and tax in
-# hundredths.
-FACT_WIDTHS = [32, 64, 64, 64, 64, 8, 8]
-FACT_LO = [0, 1, 90000, 0, 0, 0, 0]
-FACT_HI = [2526, 51, 10500001, 11, 9, 3, 2]
-FACT_ROWS = 60_000_000
-FACT_CUTOFF = 2475          # date <= cutoff keeps ~98% of the rows
-FACT_SEED = SEED_BASE + 1
-F_DATE, F_QTY, F_PRICE, F_DISC, F_TAX, F_FLAG1, F_FLAG2 = range(7)
+# The fact table's shape and value ranges are in shapes.py; the plan over it is here.
 
 
 def fact_predicate():
@@ -47,11 +39,6 @@ def fact_ariths():
         (R.NODE_INDEX, 0, R.I64, -1, -1, F_TAX),
     ], 0, R.I64, 64)
     return [p1, p2]
-
-
-FACT_GROUP_FIELDS = [F_FLAG1, F_FLAG2]
-FACT_GROUP_DOMAIN = [3, 2]
-FACT_SUM_FIELDS = [7, 8]   # the two appended products
 
 
 def gen_fact(n, device="cuda", stream=None):

@@ -1,4 +1,6 @@
 """Shared test helpers: the oracle form of the workloads and small utilities."""
+import os
+
 import numpy as np
 
 import oracle as O
@@ -27,6 +29,10 @@ def fact_oracle(rows):
                               WL.FACT_SUM_FIELDS)
 
 
+# host threads for the oracle's parallel sort (its order does not depend on the count)
+THREADS = os.cpu_count() or 1
+
+
 def to_np(t):
     return t.detach().cpu().numpy()
 
@@ -42,8 +48,8 @@ def join_aggregate_oracle_data(nr, ns, key_domain):
 
 
 def join_aggregate_oracle(r, s):
-    rs = O.sort_pairs(r, begin_bit=32, end_bit=64)
-    ss = O.sort_pairs(s, begin_bit=64, end_bit=96)
+    rs = O.sort_pairs(r, begin_bit=32, end_bit=64, threads=THREADS)
+    ss = O.sort_pairs(s, begin_bit=64, end_bit=96, threads=THREADS)
     out = O.join_tuples(rs, 32, ss, 64, 16)
     limbs = out.view(np.uint64)
     key = (limbs[:, 1] >> np.uint64(32)).astype(np.uint32)
@@ -65,7 +71,7 @@ def three_relation_oracle_data(n1, n2, n3, l5, l2):
     lists = []
     for cnt, seed in ((l5, PL.C2_SEED + 3), (l2, PL.C2_SEED + 4)):
         raw = O.uniform(cnt, seed, 0, 0, n2).astype(np.uint32)
-        lists.append(O.unique(O.sort_pairs(raw)))
+        lists.append(O.unique(O.sort_pairs(raw, threads=THREADS)))
     return d1, d2, f, lists[0], lists[1]
 
 
@@ -75,12 +81,12 @@ def three_relation_oracle(d1, d2, f, list_in, list_out):
     d2f = O.select(d2, [32, 32, 32], oracle_cmps([(O.GE, (O.OPND_VAR, 2), (O.OPND_CONST, PL.C2_DATE_LO), O.I32),
                                                   (O.LT, (O.OPND_VAR, 2), (O.OPND_CONST, PL.C2_DATE_HI), O.I32)]))
     d2s = O.project(d2f, [32, 32, 32], [32, 32], [1, 0])
-    d2s = O.sort_pairs(d2s, begin_bit=32, end_bit=64)
+    d2s = O.sort_pairs(d2s, begin_bit=32, end_bit=64, threads=THREADS)
     j1 = O.join_tuples(d1s, 8, d2s, 32, 16)
     keys = O.project(j1, [32, 8, 32], [32], [2]).view(np.uint32).ravel()
-    keys = O.sort_pairs(keys)
+    keys = O.sort_pairs(keys, threads=THREADS)
     keys = O.set_difference(O.set_intersection(keys, list_in), list_out)
-    fs = O.sort_pairs(f, begin_bit=64, end_bit=96)
+    fs = O.sort_pairs(f, begin_bit=64, end_bit=96, threads=THREADS)
     j2 = O.join_tuples(keys.view(np.uint8).reshape(-1, 4), 0, fs, 64, 16)
     limbs = j2.view(np.uint64)
     key = limbs[:, 1].astype(np.uint32)
@@ -96,13 +102,13 @@ def serving_query_oracle(d1, d2, f, segment, date_lo, date_hi, keys_list=None):
     d2f = O.select(d2, [32, 32, 32], oracle_cmps([(O.GE, (O.OPND_VAR, 2), (O.OPND_CONST, date_lo), O.I32),
                                                   (O.LT, (O.OPND_VAR, 2), (O.OPND_CONST, date_hi), O.I32)]))
     d2s = O.project(d2f, [32, 32, 32], [32, 32], [1, 0])
-    d2s = O.sort_pairs(d2s, begin_bit=32, end_bit=64)
+    d2s = O.sort_pairs(d2s, begin_bit=32, end_bit=64, threads=THREADS)
     j1 = O.join_tuples(d1s, 8, d2s, 32, 16)
     keys = O.project(j1, [32, 8, 32], [32], [2]).view(np.uint32).ravel()
-    keys = O.sort_pairs(keys)
+    keys = O.sort_pairs(keys, threads=THREADS)
     if keys_list is not None:
         keys = O.set_intersection(keys, keys_list)
-    fs = O.sort_pairs(f, begin_bit=64, end_bit=96)
+    fs = O.sort_pairs(f, begin_bit=64, end_bit=96, threads=THREADS)
     j2 = O.join_tuples(keys.view(np.uint8).reshape(-1, 4), 0, fs, 64, 16)
     limbs = j2.view(np.uint64)
     key = limbs[:, 1].astype(np.uint32)

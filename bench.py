@@ -46,8 +46,14 @@ def parse():
     ap.add_argument("--no-operators", action="store_true")
     ap.add_argument("--batched-queries", type=int, default=512,
                     help="queries of the batched join+aggregate comparison (0: skip it)")
-    ap.add_argument("--serving-queries", type=int, default=150,
+    ap.add_argument("--serving-queries", type=int, default=300,
                     help="queries per arrival rate of the serving comparison (0: skip it)")
+    ap.add_argument("--only", default=None,
+                    help="comma-separated operator groups (%s): run only those operator benchmarks on one GPU "
+                         "and print their JSON (no headline step)" % ",".join(["select", "sort_c0", "join",
+                                                                                "sort_large", "setops", "pipelines",
+                                                                                "strings_f64"]))
+    ap.add_argument("--reps", type=int, default=5, help="timed calls per operator with --only")
     ap.add_argument("--section", default=None, choices=["strings_f64", "batched", "serving"],
                     help="run one secondary benchmark alone and print its JSON (used by the main run, "
                          "which gives each secondary benchmark a fresh process and allocator)")
@@ -378,123 +384,213 @@ def _op_line(n, nbytes, ms, peak, **extra):
     return d
 
 
-def operator_benchmarks(dev, fact_rows, peak, reps=5):
-    """tuples/s and fraction of the measured HBM bandwidth per operator, on the workload
-    shapes (data resident in HBM; inputs larger than L2 except where noted)."""
+class OpContext:
+    """Inputs of the operator benchmarks, generated on first use and kept resident."""
+
+    def __init__(self, dev, fact_rows):
+        self.dev = dev
+        self.fact_rows = fact_rows
+        self._c0 = None
+        self._c2 = None
+
+    def c0(self):
+        """(R, S) of the join + aggregate workload, unsorted and sorted on their keys."""
+        if self._c0 is None:
+            from redfox_b200 import plans as PL
+            from redfox_b200 import rfx as R
+            r, s = PL.gen_join_aggregate(device=self.dev)
+            rs, ss = r.clone(), s.clone()
+            R.sort_pairs(rs, begin_bit=32, end_bit=64)
+            R.sort_pairs(ss, begin_bit=64, end_bit=96)
+            self._c0 = (r, s, rs, ss)
+        return self._c0
+
+    def c2(self):
+        if self._c2 is None:
+            from redfox_b200 import plans as PL
+            self._c2 = PL.gen_three_relation(device=self.dev)
+        return self._c2
+
+
+def _op_select(ctx, peak, reps):
     import torch
 
-    from redfox_b200 import plans as PL
     from redfox_b200 import rfx as R
     from redfox_b200 import workloads as WL
-
-    ops = {}
-    # select on the 60M-row fact table (64 B rows, ~98% kept)
-    n = fact_rows.shape[0]
-    out = torch.empty_like(fact_rows)
-    cnt = torch.zeros(1, dtype=torch.int64, device=dev)
+    rows = ctx.fact_rows
+    n = rows.shape[0]
+    out = torch.empty_like(rows)
+    cnt = torch.zeros(1, dtype=torch.int64, device=ctx.dev)
     t = R.Tuple.of(WL.FACT_WIDTHS)
     cm = R.make_cmps(WL.fact_predicate())
     wsb = R.LIB.rfx_select_workspace(n, R.C.byref(t))
-    ws = R._empty_bytes(wsb, dev)
+    ws = R._empty_bytes(wsb, ctx.dev)
 
     def sel():
-        R.check("rfx_select", R.LIB.rfx_select(R._ptr(out), R._ptr(cnt), R._ptr(fact_rows), n, R.C.byref(t), cm, 1,
+        R.check("rfx_select", R.LIB.rfx_select(R._ptr(out), R._ptr(cnt), R._ptr(rows), n, R.C.byref(t), cm, 1,
                                                R._ptr(ws), wsb, R._stream()))
     sel()
     ms = _time_ms(sel, reps)
     k = int(cnt.item())
-    ops["select_fact_60M"] = _op_line(n, n * 64 + k * 64, ms, peak, kept=k)
-    del out
+    return {"select_fact_60M": _op_line(n, n * 64 + k * 64, ms, peak, kept=k)}
 
-    # join + aggregate inputs (1M x 4M)
-    r, s = PL.gen_join_aggregate(device=dev)
-    # sort pairs: S rows (16 B) on the 32-bit key field (= b40c sort_pair of u32 key / u64 value)
-    ss = torch.empty_like(s)
-    srt = R.Sorter(s.shape[0], 16, 0, 64, 96, device=dev)
-    ms = _time_ms(lambda: srt(ss), reps, setup=lambda: ss.copy_(s))
-    ns = s.shape[0]
-    ops["sort_pairs_4M_u32key_u64val"] = _op_line(ns, ns * 16 + 4 * 2 * ns * 16, ms, peak, passes=4,
-                                                  note="input 64 MB (fits L2)")
-    rs = r.clone()
-    R.sort_pairs(rs, begin_bit=32, end_bit=64)
-    srt(ss)
-    # fused tuple join (count + emit), 19.3M output rows
-    tj = R.TupleJoin(rs.shape[0], device=dev)
-    dummy = torch.empty((1, 16), dtype=torch.uint8, device=dev)
+
+def _sort_line(src, kb, begin, end, reps, peak, flags=0, note=None, passes=None):
+    """Device time of sorting a copy of `src` (n x kb bytes) on bits [begin, end); the
+    copy is restored before each call outside the timed interval."""
+    import torch
+
+    from redfox_b200 import rfx as R
+    n = src.shape[0]
+    work = torch.empty_like(src)
+    srt = R.Sorter(n, kb, 0, begin, end, device=src.device)
+    ms = _time_ms(lambda: srt(work, flags=flags), reps, setup=lambda: work.copy_(src))
+    p = passes if passes is not None else (end - begin + 7) // 8
+    extra = {"passes": p}
+    if note:
+        extra["note"] = note
+    return _op_line(n, n * kb + p * 2 * n * kb, ms, peak, **extra)
+
+
+def _op_sort_c0(ctx, peak, reps):
+    r, s, _, _ = ctx.c0()
+    return {"sort_pairs_4M_u32key_u64val": _sort_line(s, 16, 64, 96, reps, peak, note="S rows (fk, amount); 64 MB, fits L2"),
+            "sort_tuples_1M_8B_on_key": _sort_line(r, 8, 32, 64, reps, peak, note="R rows (key, payload); fits L2")}
+
+
+def _op_sort_large(ctx, peak, reps):
+    import torch
+
+    from redfox_b200 import rfx as R
+    _, _, f, _, _ = ctx.c2()
+    out = {"sort_tuples_60M_16B_on_fk": _sort_line(f, 16, 64, 96, 3, peak, flags=R.SORT_SKIP_TRIVIAL, passes=3,
+                                                   note="fk < 2^24: the top digit is constant and skipped")}
+    n = 60_000_000
+    keys = R.gen_uniform_rows(n, [32], 0x5EED0101, [0], [1 << 32], device=ctx.dev)
+    out["sort_keys_60M_u32"] = _sort_line(keys.view(torch.uint8).view(n, 4), 4, 0, 32, 3, peak,
+                                          note="uniform 32-bit keys, 4 passes")
+    rows8 = R.gen_uniform_rows(n, [32, 32], 0x5EED0102, [0, 0], [1 << 32, 1 << 32], device=ctx.dev)
+    out["sort_tuples_60M_8B_on_key"] = _sort_line(rows8, 8, 32, 64, 3, peak, note="Tuple<32,32> rows on the key")
+    return out
+
+
+def _op_join(ctx, peak, reps):
+    import torch
+
+    from redfox_b200 import rfx as R
+    _, _, rs, ss = ctx.c0()
+    ops = {}
+    nl, nr = rs.shape[0], ss.shape[0]
+    tj = R.TupleJoin(nl, device=ctx.dev)
+    dummy = torch.empty((1, 16), dtype=torch.uint8, device=ctx.dev)
     tj(dummy, 0, rs, 32, ss, 64)
     total = int(tj.count.item())
-    jout = torch.empty((total, 16), dtype=torch.uint8, device=dev)
+    jout = torch.empty((total, 16), dtype=torch.uint8, device=ctx.dev)
     ms = _time_ms(lambda: tj(jout, total, rs, 32, ss, 64), reps)
-    nl, nr = rs.shape[0], ss.shape[0]
-    ops["join_fused_1Mx4M"] = _op_line(total, total * 16 + nl * 8 + nr * 16 + nl * 16, ms, peak,
-                                       inputs=nl + nr)
+    ops["join_fused_1Mx4M"] = _op_line(total, total * 16 + nl * 8 + nr * 16 + nl * 16, ms, peak, inputs=nl + nr)
     # find_bounds alone on the split u32 keys
     lk = ((rs.view(torch.int64).view(-1) >> 32) & 0xFFFFFFFF).to(torch.int32)
     rk = (ss.view(torch.int64).view(-1, 2)[:, 1] & 0xFFFFFFFF).to(torch.int32)
-    lb = torch.empty(nl, dtype=torch.int32, device=dev)
-    sc = torch.empty(nl, dtype=torch.int32, device=dev)
-    tot = torch.zeros(1, dtype=torch.int64, device=dev)
+    lb = torch.empty(nl, dtype=torch.int32, device=ctx.dev)
+    sc = torch.empty(nl, dtype=torch.int32, device=ctx.dev)
+    tot = torch.zeros(1, dtype=torch.int64, device=ctx.dev)
     fwsb = R.LIB.rfx_join_find_bounds_workspace(nl)
-    fws = R._empty_bytes(fwsb, dev)
+    fws = R._empty_bytes(fwsb, ctx.dev)
     ms = _time_ms(lambda: R.check("fb", R.LIB.rfx_join_find_bounds(R._ptr(lb), R._ptr(sc), R._ptr(tot), R._ptr(lk), nl,
                                                                    R._ptr(rk), nr, 4, R._ptr(fws), fwsb, R._stream())),
                   reps)
     ops["find_bounds_1Mx4M_u32"] = _op_line(nl, (nl + nr) * 4 + 8 * nl, ms, peak, note="inputs fit L2")
     # reduce-by-key over the 19.3M-row join output (16 B rows, key = high 32 bits)
-    g = torch.zeros(1, dtype=torch.int64, device=dev)
-    okeys = torch.empty(total, dtype=torch.int32, device=dev)
-    osum = torch.empty(total, dtype=torch.int64, device=dev)
-    ocnt = torch.empty(total, dtype=torch.int32, device=dev)
+    g = torch.zeros(1, dtype=torch.int64, device=ctx.dev)
+    okeys = torch.empty(total, dtype=torch.int32, device=ctx.dev)
+    osum = torch.empty(total, dtype=torch.int64, device=ctx.dev)
+    ocnt = torch.empty(total, dtype=torch.int32, device=ctx.dev)
     rwsb = R.LIB.rfx_reduce_by_key_workspace(total)
-    rws = R._empty_bytes(rwsb, dev)
+    rws = R._empty_bytes(rwsb, ctx.dev)
     ms = _time_ms(lambda: R.check("rt", R.LIB.rfx_reduce_tuples(R._ptr(jout), total, None, 16, 96, 0, 64, R._ptr(okeys),
                                                                 4, R._ptr(osum), R._ptr(ocnt), R._ptr(g), R._ptr(rws),
                                                                 rwsb, R._stream())), reps)
     groups = int(g.item())
     ops["reduce_by_key_19M_rows"] = _op_line(total, total * 16 + groups * 16, ms, peak, groups=groups)
-    del jout, okeys, osum, ocnt
+    # join + aggregate on the key as one operator (no join rows)
+    ja = R.JoinAggregate(nr, 4, device=ctx.dev)
+    ms = _time_ms(lambda: ja(rs, 32, ss, 64, 0, 64), reps)
+    gj = int(ja.groups.item())
+    ops["join_aggregate_1Mx4M"] = _op_line(nl + nr, nl * 8 + nr * 16 + gj * 16, ms, peak, groups=gj,
+                                           note="S reduced to its groups, then matched against R; inputs fit L2")
+    return ops
 
-    # three-relation inputs: sort of F (60M x 16 B) on fk, set ops on the key lists
-    d1, d2, f, l5, l2 = PL.gen_three_relation(device=dev)
-    fs = torch.empty_like(f)
-    fsort = R.Sorter(f.shape[0], 16, 0, 64, 96, device=dev)
-    ms = _time_ms(lambda: fsort(fs, flags=R.SORT_SKIP_TRIVIAL), 3, setup=lambda: fs.copy_(f))
-    nf = f.shape[0]
-    ops["sort_tuples_60M_16B_on_fk"] = _op_line(nf, nf * 16 + 3 * 2 * nf * 16, ms, peak, passes=3,
-                                               note="fk < 2^24: the top digit is constant and skipped")
-    for name, op, a, b in (("intersect_5M_2M_u32", R.SET_INTERSECTION, l5, l2),
-                           ("difference_5M_2M_u32", R.SET_DIFFERENCE, l5, l2),
-                           ("union_5M_2M_u32", R.SET_UNION, l5, l2)):
-        outp = torch.empty(a.shape[0] + b.shape[0], dtype=torch.int32, device=dev)
-        c = torch.zeros(1, dtype=torch.int64, device=dev)
-        swsb = R.LIB.rfx_set_op_workspace(op, a.shape[0], b.shape[0], 4)
-        sws = R._empty_bytes(swsb, dev)
 
-        def run(op=op, a=a, b=b, outp=outp, c=c, sws=sws, swsb=swsb):
-            R.check("set", R.LIB.rfx_set_op(op, R._ptr(outp), R._ptr(c), R._ptr(a), a.shape[0], R._ptr(b), b.shape[0],
-                                            4, R._ptr(sws), swsb, R._stream()))
-        ms = _time_ms(run, reps)
-        no = int(c.item())
-        ops[name] = _op_line(a.shape[0] + b.shape[0], (a.shape[0] + b.shape[0] + no) * 4, ms, peak, out=no,
-                             note="inputs fit L2")
-    # the two pipelines end to end (host reads sizes back between steps, as the reference);
-    # one untimed run first compiles the plan-specialised kernels
-    PL.join_aggregate(r, s)
-    PL.three_relation(d1, d2, f, l5, l2)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    PL.join_aggregate(r, s)
-    torch.cuda.synchronize()
-    ms = (time.perf_counter() - t0) * 1e3
-    ops["pipeline_join_aggregate_1Mx4M"] = {"tuples": nl + nr, "ms": ms, "tuples_per_s": (nl + nr) / (ms / 1e3),
-                                            "note": "sort R, sort S, join, reduce; wall clock incl. size reads"}
-    t0 = time.perf_counter()
-    PL.three_relation(d1, d2, f, l5, l2)
-    torch.cuda.synchronize()
-    ms = (time.perf_counter() - t0) * 1e3
-    nin = d1.shape[0] + d2.shape[0] + f.shape[0]
-    ops["pipeline_three_relation_76M"] = {"tuples": nin, "ms": ms, "tuples_per_s": nin / (ms / 1e3),
-                                          "note": "selects, sort, 2 joins, set ops, sort of F, reduce; wall clock"}
+def _op_setops(ctx, peak, reps):
+    import torch
+
+    from redfox_b200 import rfx as R
+    _, _, _, l5, l2 = ctx.c2()
+    ops = {}
+    lists = [("5M_2M_u32", l5, l2, "inputs fit L2")]
+    big_a = R.gen_uniform_rows(60_000_000, [32], 0x5EED0201, [0], [1 << 30], device=ctx.dev).view(torch.int32).view(-1)
+    big_b = R.gen_uniform_rows(15_000_000, [32], 0x5EED0202, [0], [1 << 30], device=ctx.dev).view(torch.int32).view(-1)
+    R.sort_pairs(big_a)
+    R.sort_pairs(big_b)
+    lists.append(("60M_15M_u32", big_a, big_b, "sorted u32 lists with duplicates, larger than L2"))
+    for tag, a, b, note in lists:
+        for name, op in (("intersect", R.SET_INTERSECTION), ("difference", R.SET_DIFFERENCE), ("union", R.SET_UNION)):
+            outp = torch.empty(a.shape[0] + b.shape[0], dtype=torch.int32, device=ctx.dev)
+            c = torch.zeros(1, dtype=torch.int64, device=ctx.dev)
+            swsb = R.LIB.rfx_set_op_workspace(op, a.shape[0], b.shape[0], 4)
+            sws = R._empty_bytes(swsb, ctx.dev)
+
+            def run(op=op, a=a, b=b, outp=outp, c=c, sws=sws, swsb=swsb):
+                R.check("set", R.LIB.rfx_set_op(op, R._ptr(outp), R._ptr(c), R._ptr(a), a.shape[0], R._ptr(b),
+                                                b.shape[0], 4, R._ptr(sws), swsb, R._stream()))
+            ms = _time_ms(run, reps)
+            no = int(c.item())
+            ops["%s_%s" % (name, tag)] = _op_line(a.shape[0] + b.shape[0], (a.shape[0] + b.shape[0] + no) * 4, ms,
+                                                  peak, out=no, note=note)
+    return ops
+
+
+def _op_pipelines(ctx, peak, reps):
+    """The plans end to end (host reads sizes back between steps, as the reference); one
+    untimed run first compiles the plan-specialised kernels."""
+    import torch
+
+    from redfox_b200 import plans as PL
+    r, s, _, _ = ctx.c0()
+    d1, d2, f, l5, l2 = ctx.c2()
+    ops = {}
+    nin0 = r.shape[0] + s.shape[0]
+    nin2 = d1.shape[0] + d2.shape[0] + f.shape[0]
+    for name, fn, nin, note in (
+            ("pipeline_join_aggregate_1Mx4M", lambda: PL.join_aggregate(r, s), nin0,
+             "sort R, sort S, join (19.3M rows written), reduce; wall clock incl. size reads"),
+            ("pipeline_join_aggregate_fused_1Mx4M", lambda: PL.join_aggregate_fused(r, s), nin0,
+             "sort R, sort S, join-aggregate on the key (no join rows); wall clock incl. the group count read"),
+            ("pipeline_three_relation_76M", lambda: PL.three_relation(d1, d2, f, l5, l2), nin2,
+             "selects, sort, 2 joins, set ops, sort of F, reduce; wall clock")):
+        fn()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        fn()
+        torch.cuda.synchronize()
+        ms = (time.perf_counter() - t0) * 1e3
+        ops[name] = {"tuples": nin, "ms": ms, "tuples_per_s": nin / (ms / 1e3), "note": note}
+    return ops
+
+
+OPERATORS = {"select": _op_select, "sort_c0": _op_sort_c0, "join": _op_join, "sort_large": _op_sort_large,
+             "setops": _op_setops, "pipelines": _op_pipelines}
+
+
+def operator_benchmarks(dev, fact_rows, peak, reps=5, only=None):
+    """tuples/s and fraction of the measured HBM bandwidth per operator, on the workload
+    shapes (data resident in HBM; inputs larger than L2 except where noted).  `only`: a
+    list of OPERATORS keys to run (all when None)."""
+    ctx = OpContext(dev, fact_rows)
+    ops = {}
+    for name, fn in OPERATORS.items():
+        if only is None or name in only:
+            ops.update(fn(ctx, peak, reps))
     return ops
 
 
@@ -679,7 +775,7 @@ def batched_benchmark(dev, nq, reps=3):
     per = B.split_by_query(keys, sums, counts, min(nq, 8))
     ok = all(torch.equal(per[q][0], plain[q][0] & B.QUERY_KEY_MASK) and torch.equal(per[q][1], plain[q][1])
              and torch.equal(per[q][2], plain[q][2]) for q in range(len(plain)))
-    nbytes = sum(t.numel() * t.element_size() for t in (plan.r, plan.s, plan.out, plan.keys, plan.sums, plan.counts))
+    nbytes = plan.nbytes()
     del plan
     torch.cuda.empty_cache()
 
@@ -697,36 +793,43 @@ def batched_benchmark(dev, nq, reps=3):
                           "plan_buffers_gb": nbytes / 1e9},
         "speedup_queries_per_s": plain_ms / batch_ms,
         "parity_first_8_queries": "ok" if ok else "MISMATCH",
-        "note": "same kernels both ways; plain reads each query's join and group counts back to size its "
-                "outputs, batched sizes them once and replays the captured plan",
+        "note": "same kernels both ways (sort R, sort S, join-aggregate on the key); plain runs one launch "
+                "sequence per query and reads its group count back, batched sorts and aggregates all queries "
+                "folded by query id in one captured plan",
     }
 
 
-def serving_benchmark(dev, nq, rates=(100.0, 1000.0, 5000.0), slots=8):
+def serving_benchmark(dev, nq, rates=(100.0, 300.0, 1000.0, 3000.0, 5000.0), slots=2):
     """Parameterised select-join-aggregate queries over the resident three-relation data
     (D1 1.5M, D2 15M, F 60M sorted on fk), Poisson arrivals at each rate: the serving loop
-    (admission against a 40 GB intermediate budget, `slots` queries in flight on their own
-    streams) against serial plain execution of the same trace (one query at a time, FIFO).
-    Latency = host time from a query's arrival to its result on the host."""
+    (admission against a 40 GB intermediate budget; the queries admitted since the last
+    round started packed into one batched plan; `slots` rounds in flight on their own
+    streams) against serial plain execution of the same trace (one query at a time,
+    FIFO).  Latency = host time from a query's arrival to its result on the host."""
     import torch
 
     from redfox_b200 import serving as S
 
     res = S.Resident(device=dev)
-    for q in S.gen_requests(6, 1e6, seed=S.SERVING_SEED + 99):       # untimed warm-up
+    warm = S.gen_requests(6, 1e6, seed=S.SERVING_SEED + 99)
+    for q in warm:                                              # untimed warm-up
         S.run_alone(res, q, device=dev)
+    S.run_round_host(res, warm, dev)
     out = {"resident_gb": res.nbytes() / 1e9, "slots": slots, "budget_gb": S.BUDGET_BYTES / 1e9,
            "queries_per_rate": nq, "rates": {}}
     for rate in rates:
         line = {}
-        for name, k in (("serial", 1), ("serving", slots)):
+        for name, srv in (("serial", S.Server(res, slots=1, device=dev, plain=True)),
+                          ("serving", S.Server(res, slots=slots, device=dev))):
             reqs = S.gen_requests(nq, rate)
             torch.cuda.synchronize()
             torch.cuda.reset_peak_memory_stats(dev)
             base = torch.cuda.memory_allocated(dev)
-            sch = S.Server(res, slots=k, device=dev).serve(reqs)
+            sch = srv.serve(reqs)
             line[name] = S.latency_summary(reqs)
             line[name]["peak_in_flight"] = sch.peak_queries
+            line[name]["rounds"] = len(srv.rounds)
+            line[name]["mean_round"] = sum(srv.rounds) / max(1, len(srv.rounds))
             line[name]["peak_intermediate_gb"] = (torch.cuda.max_memory_allocated(dev) - base) / 1e9
         line["speedup_queries_per_s"] = line["serving"]["queries_per_s"] / line["serial"]["queries_per_s"]
         out["rates"][str(int(rate))] = line
@@ -913,12 +1016,33 @@ def main_ours(args):
     return 0 if ok else 1
 
 
+def main_only(args):
+    """Selected operator benchmarks alone (profiling and quick measurements)."""
+    import torch
+
+    from redfox_b200 import rfx as R
+    from redfox_b200 import workloads as WL
+    dev = torch.device("cuda:0")
+    peak = measured_peak_hbm()[0]
+    only = [x for x in args.only.split(",") if x]
+    rows = WL.gen_fact(args.rows, device=dev) if "select" in only else None
+    out = operator_benchmarks(dev, rows, peak, reps=args.reps, only=only)
+    if "strings_f64" in only:
+        out.update(string_f64_benchmarks(dev, peak, reps=args.reps))
+    torch.cuda.synchronize()
+    out["device_status"] = R.device_status()
+    print(json.dumps(out), flush=True)
+    return 0 if out["device_status"] == R.OK else 1
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return main_reference(args)
     if args.section:
         return main_section(args)
+    if args.only:
+        return main_only(args)
     return main_ours(args)
 
 

@@ -386,6 +386,42 @@ rfx_status rfx_join_tuples_emit(void* out, uint32_t out_bytes, uint64_t capacity
                                 uint32_t right_bytes, uint32_t right_value_bits, void* workspace,
                                 size_t workspace_bytes, void* stream);
 
+/* addJoin followed by addAgg on the join key (RelationalAlgebraCompiler.cpp:4466-5227,
+ * :7852-8643: join, then reduce_by_key SUM / count over the join output) in one operator
+ * that never writes the join rows.  left / right are packed tuples sorted on their keys
+ * (key = tuple >> value bits, as rfx_join_tuples); the value is the value_bits-wide field
+ * of the right tuple at value_shift.  Per key present on both sides, in key order:
+ * out_keys (out_key_bytes = 4 or 8; the key fields must fit it, higher bits of the right
+ * key are dropped as rfx_reduce_tuples drops them), out_sums = the exact
+ * int64 sum of the value over that key's join rows, out_counts = the number of join rows
+ * (u32); *d_groups = keys written.  The bytes equal rfx_join_tuples + rfx_reduce_tuples
+ * over the join output.  Capacity of the outputs: nr.  Workspace:
+ * rfx_join_aggregate_workspace(nr, out_key_bytes). */
+size_t rfx_join_aggregate_workspace(uint64_t nr, uint32_t out_key_bytes);
+rfx_status rfx_join_aggregate(const void* left, uint64_t nl, uint32_t left_bytes,
+                              uint32_t left_value_bits, const void* right, uint64_t nr,
+                              uint32_t right_bytes, uint32_t right_value_bits, uint32_t value_shift,
+                              uint32_t value_bits, void* out_keys, uint32_t out_key_bytes,
+                              int64_t* out_sums, uint32_t* out_counts, uint64_t* d_groups,
+                              void* workspace, size_t workspace_bytes, void* stream);
+
+/* Range selection of one relation for up to 256 queries in one scan (no counterpart in
+ * the reference, which runs one select per query: Select.h:30-114).  For each row in
+ * order and each query q < nq in order, if lo[q] <= field < hi[q] (field = bits
+ * [field_shift, field_shift + field_width) of the row, width <= 32) the 8-byte row
+ * ((key << 8 | q) << val_width) | val is written, key and val being the bit fields
+ * (key_shift, key_width) and (val_shift, val_width) of the input row; key_width + 8 +
+ * val_width <= 64.  Input rows of 4/8/16 bytes.  Writes the first `capacity` rows and
+ * *d_count = all matches.  lo / hi are host arrays of nq bounds.  Workspace:
+ * rfx_multi_select_workspace(n). */
+size_t rfx_multi_select_workspace(uint64_t n);
+rfx_status rfx_multi_select(void* out, uint64_t capacity, uint64_t* d_count, const void* in,
+                            uint64_t n, uint32_t in_bytes, uint32_t field_shift,
+                            uint32_t field_width, const uint32_t* lo, const uint32_t* hi,
+                            uint32_t nq, uint32_t key_shift, uint32_t key_width,
+                            uint32_t val_shift, uint32_t val_width, void* workspace,
+                            size_t workspace_bytes, void* stream);
+
 /* redfox::find_bounds_* and redfox::join with the reference's argument meaning (element
  * counts; *result_size on the device).  Own their scratch, synchronous (default
  * stream), as the reference. */
@@ -537,6 +573,19 @@ rfx_status rfx_exec_stats(rfx_exec* exec, uint64_t* in_use, uint64_t* peak, uint
                           size_t err_cap);
 /* Copies a variable's rows (after a run) to caller device memory of cap_bytes. */
 rfx_status rfx_exec_copy_out(rfx_exec* exec, const char* name, void* dst, uint64_t cap_bytes, void* stream);
+
+/* The plan as a CUDA graph (Harmony runs a plan's kernels one launch at a time,
+ * Runtime.cpp:304-445; here the whole sequence is one graph launch).  rfx_exec_capture
+ * runs the plan once eagerly on `stream` (a non-default stream) to learn every size it
+ * reads back and every allocation, allocates one arena of that total (against the
+ * budget) and captures the op sequence with its memory taken from the arena and the
+ * learnt sizes in place of the read-backs.  rfx_exec_replay launches the graph and checks
+ * that each intermediate size the graph produced equals the captured one: RFX_OK means
+ * the outputs (rfx_exec_output) equal an eager run's; RFX_ERR_CAPACITY means the inputs'
+ * contents changed the plan's shape and the plan must run eagerly or be captured again.
+ * Inputs must stay bound to the same memory; tuning must be off. */
+rfx_status rfx_exec_capture(rfx_exec* exec, void* stream);
+rfx_status rfx_exec_replay(rfx_exec* exec, void* stream);
 
 #ifdef __cplusplus
 }

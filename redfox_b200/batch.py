@@ -4,7 +4,9 @@ operator, and the whole batched plan captured as a CUDA graph.
 The queries are folded into one relation by putting the query id above each query's key
 (key' = q << 21 | key, the per-query key domains |R|/4 being below 2^21): sorting on the
 composite key sorts every query, the sort-merge join on it joins every query with itself
-only, and the reduce-by-key groups per (query, key).  Tiles of all queries then share the
+only, and the aggregate groups per (query, key).  The join and the aggregate on its key run
+as one operator (rfx_join_aggregate: per key, the join's SUM and COUNT from the two sides'
+sorted runs, no join rows written) in both forms, batched and plain.  Tiles of all queries then share the
 persistent kernels' dynamic tile queues (the device work queue), so a 10^4-row query and an
 8 * 10^6-row query occupy the GPU alike, and per-query launch and read-back costs vanish.
 
@@ -74,8 +76,8 @@ def gen_batch(sizes, device="cuda"):
 
 class BatchedPlan:
     """The join + aggregate plan over the folded relations, with every buffer allocated up
-    front so that the plan can be captured in a CUDA graph and replayed.  The join output
-    capacity comes from one eager count of the same inputs."""
+    front (outputs sized by |S|, every count on the device) so that the plan can be
+    captured in a CUDA graph and replayed."""
 
     def __init__(self, r_all, s_all):
         import torch
@@ -86,25 +88,24 @@ class BatchedPlan:
         self.s = torch.empty_like(s_all)
         self.rsort = R.Sorter(self.nr, 8, 0, 32, 64, device=dev)
         self.ssort = R.Sorter(self.ns, 16, 0, 64, 96, device=dev)
-        self.tj = R.TupleJoin(self.nr, device=dev)
-        # size the join output with one eager pass
-        self.r.copy_(r_all)
-        self.s.copy_(s_all)
-        self.rsort(self.r)
-        self.ssort(self.s)
-        dummy = torch.empty((1, 16), dtype=torch.uint8, device=dev)
-        self.tj(dummy, 0, self.r, 32, self.s, 64)
-        self.cap = int(self.tj.count.item())
-        self.out = torch.empty((max(1, self.cap), 16), dtype=torch.uint8, device=dev)
-        # one group per distinct (query, key) of R at most
-        g = max(1, self.nr)
-        self.keys = torch.empty(g, dtype=torch.int32, device=dev)
-        self.sums = torch.empty(g, dtype=torch.int64, device=dev)
-        self.counts = torch.empty(g, dtype=torch.int32, device=dev)
-        self.groups = torch.zeros(1, dtype=torch.int64, device=dev)
-        self.rwsb = R.LIB.rfx_reduce_by_key_workspace(self.cap)
-        self.rws = R._empty_bytes(self.rwsb, dev)
+        self.ja = R.JoinAggregate(self.ns, 4, device=dev)
         self.graph = None
+
+    @property
+    def keys(self):
+        return self.ja.keys
+
+    @property
+    def sums(self):
+        return self.ja.sums
+
+    @property
+    def counts(self):
+        return self.ja.counts
+
+    def nbytes(self):
+        return sum(t.numel() * t.element_size() for t in (self.r, self.s, self.ja.keys, self.ja.sums,
+                                                          self.ja.counts, self.ja.ws, self.rsort.ws, self.ssort.ws))
 
     def run(self, stream=None):
         """Enqueue the whole plan (no host synchronisation)."""
@@ -112,11 +113,7 @@ class BatchedPlan:
         self.s.copy_(self.s_in)
         self.rsort(self.r, stream=stream)
         self.ssort(self.s, stream=stream)
-        self.tj(self.out, self.cap, self.r, 32, self.s, 64, stream=stream)
-        R.check("rfx_reduce_tuples", R.LIB.rfx_reduce_tuples(
-            R._ptr(self.out), self.cap, R._ptr(self.tj.count), 16, 96, 0, 64, R._ptr(self.keys), 4,
-            R._ptr(self.sums), R._ptr(self.counts), R._ptr(self.groups), R._ptr(self.rws), self.rwsb,
-            R._stream(stream)))
+        self.ja(self.r, 32, self.s, 64, 0, 64, stream=stream)
 
     def capture(self):
         """Capture run() in a CUDA graph (after one eager run has warmed every kernel up)."""
@@ -134,8 +131,10 @@ class BatchedPlan:
         self.graph.replay()
 
     def result(self):
-        g = int(self.groups.item())
-        return self.keys[:g], self.sums[:g], self.counts[:g], int(self.tj.count.item())
+        """(keys, sums, counts, join rows): the join's row count is the sum of the counts."""
+        import torch
+        keys, sums, counts = self.ja.result()
+        return keys, sums, counts, int(counts.to(torch.int64).sum())
 
 
 def split_by_query(keys, sums, counts, nq):
@@ -151,5 +150,9 @@ def split_by_query(keys, sums, counts, nq):
 
 
 def plain_query(r_all, s_all, r_off, s_off, q, stream=None):
-    """Query q alone through the plain plan (one launch sequence, sizes read back)."""
-    return PL.join_aggregate(r_all[r_off[q]:r_off[q + 1]], s_all[s_off[q]:s_off[q + 1]], stream=stream)
+    """Query q alone through the plain plan (one launch sequence, the group count read
+    back).  Returns (keys, sums, counts, join rows)."""
+    import torch
+    keys, sums, counts = PL.join_aggregate_fused(r_all[r_off[q]:r_off[q + 1]], s_all[s_off[q]:s_off[q + 1]],
+                                                 stream=stream)
+    return keys, sums, counts, int(counts.to(torch.int64).sum())

@@ -155,6 +155,7 @@ struct Var {
   bool input = false;       // defined by no op
   bool bound = false;       // caller memory
   bool output = false;
+  bool in_arena = false;    // memory of the graph form's arena (never freed by itself)
   int last_use = -1;
   int def = -1;
 };
@@ -178,6 +179,22 @@ struct rfx_exec {
   uint64_t launches = 0;   // operator calls
   std::string err;
   cudaStream_t stream = 0;
+  // CUDA-graph form (rfx_exec_capture / rfx_exec_replay): an eager run records every
+  // size read back and every allocation; the capture then takes its memory from one arena
+  // in the same order and, where the eager run read a size back, copies the device count
+  // into `observed` and uses the recorded size.  A replay is valid when every observed
+  // size equals the recorded one.
+  bool recording = false;
+  bool capturing = false;
+  std::vector<uint64_t> rec_sizes;
+  std::vector<uint64_t> rec_allocs;
+  size_t size_pos = 0;
+  uint64_t arena_used = 0;
+  void* arena = nullptr;
+  uint64_t arena_bytes = 0;
+  uint64_t* d_observed = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t gexec = nullptr;
 };
 
 namespace rfx {
@@ -197,11 +214,33 @@ rfx_status fail(rfx_exec* x, rfx_status st, const std::string& m) {
   return st;
 }
 
+// One allocation: from the stream-ordered allocator, or while capturing, the next block
+// of the arena (allocations replay in the recorded order and are never freed inside
+// the graph).
+rfx_status raw_alloc(rfx_exec* x, void** p, uint64_t b) {
+  if (x->capturing) {
+    const uint64_t off = align_up(x->arena_used, 256);
+    if (off + b > x->arena_bytes) return fail(x, RFX_ERR_CAPACITY, "capture: arena exhausted");
+    *p = static_cast<uint8_t*>(x->arena) + off;
+    x->arena_used = off + b;
+    return RFX_OK;
+  }
+  if (x->recording) x->rec_allocs.push_back(b);
+  RFX_CUDA_TRY(cudaMallocAsync(p, b, x->stream));
+  return RFX_OK;
+}
+
+void raw_free(rfx_exec* x, void* p) {
+  if (!x->capturing) cudaFreeAsync(p, x->stream);
+}
+
 rfx_status dev_alloc(rfx_exec* x, Var& v, uint64_t bytes) {
   const uint64_t b = bytes ? bytes : 16;
   if (x->budget && x->in_use + b > x->budget)
     return fail(x, RFX_ERR_CAPACITY, "memory budget exceeded allocating '" + v.name + "'");
-  RFX_CUDA_TRY(cudaMallocAsync(&v.ptr, b, x->stream));
+  rfx_status st = raw_alloc(x, &v.ptr, b);
+  if (st != RFX_OK) return st;
+  v.in_arena = x->capturing;
   v.bytes = b;
   x->in_use += b;
   if (x->in_use > x->peak) x->peak = x->in_use;
@@ -210,12 +249,13 @@ rfx_status dev_alloc(rfx_exec* x, Var& v, uint64_t bytes) {
 
 void dev_free(rfx_exec* x, Var& v) {
   if (v.ptr && !v.bound) {
-    cudaFreeAsync(v.ptr, x->stream);
+    if (!v.in_arena) raw_free(x, v.ptr);
     x->in_use -= v.bytes;
   }
   if (!v.bound) {
     v.ptr = nullptr;
     v.bytes = 0;
+    v.in_arena = false;
   }
 }
 
@@ -225,7 +265,7 @@ struct Scratch {  // temporary device memory counted against the budget
   uint64_t bytes = 0;
   ~Scratch() {
     if (p) {
-      cudaFreeAsync(p, x->stream);
+      raw_free(x, p);
       x->in_use -= bytes;
     }
   }
@@ -235,7 +275,12 @@ struct Scratch {  // temporary device memory counted against the budget
       bytes = 0;
       return fail(x, RFX_ERR_CAPACITY, "memory budget exceeded allocating a workspace");
     }
-    RFX_CUDA_TRY(cudaMallocAsync(&p, bytes, x->stream));
+    rfx_status st = raw_alloc(x, &p, bytes);
+    if (st != RFX_OK) {
+      p = nullptr;
+      bytes = 0;
+      return st;
+    }
     x->in_use += bytes;
     if (x->in_use > x->peak) x->peak = x->in_use;
     return RFX_OK;
@@ -243,8 +288,17 @@ struct Scratch {  // temporary device memory counted against the budget
 };
 
 rfx_status read_count(rfx_exec* x, const uint64_t* d, uint64_t* h) {
+  if (x->capturing) {
+    // the size the eager run read here; the replay's own count is kept for the check
+    if (x->size_pos >= x->rec_sizes.size()) return fail(x, RFX_ERR_INVALID, "capture: plan diverged");
+    RFX_CUDA_TRY(cudaMemcpyAsync(x->d_observed + x->size_pos, d, sizeof(uint64_t), cudaMemcpyDeviceToDevice,
+                                 x->stream));
+    *h = x->rec_sizes[x->size_pos++];
+    return RFX_OK;
+  }
   RFX_CUDA_TRY(cudaMemcpyAsync(h, d, sizeof(uint64_t), cudaMemcpyDeviceToHost, x->stream));
   RFX_CUDA_TRY(cudaStreamSynchronize(x->stream));
+  if (x->recording) x->rec_sizes.push_back(*h);
   return RFX_OK;
 }
 
@@ -445,6 +499,13 @@ rfx_status op_merge(rfx_exec* x, const Op& o) {
                            v ? v->row_bytes : 4u, vb, x->stream);
 }
 
+void drop_graph(rfx_exec* x) {
+  if (x->gexec) cudaGraphExecDestroy(x->gexec);
+  if (x->graph) cudaGraphDestroy(x->graph);
+  x->gexec = nullptr;
+  x->graph = nullptr;
+}
+
 // reads / writes of an op (names), for liveness
 bool op_operands(const Op& o, std::vector<std::string>& r, std::vector<std::string>& w) {
   const Json* j = o.j;
@@ -562,6 +623,9 @@ extern "C" void rfx_exec_destroy(rfx_exec* x) {
   if (!x) return;
   for (auto& kv : x->vars) dev_free(x, kv.second);
   cudaStreamSynchronize(x->stream);
+  drop_graph(x);
+  if (x->arena) cudaFree(x->arena);
+  if (x->d_observed) cudaFree(x->d_observed);
   delete x;
 }
 
@@ -599,12 +663,12 @@ extern "C" rfx_status rfx_exec_load(rfx_exec* x, const char* name, const char* p
   return RFX_OK;
 }
 
-// Runs the plan on `stream`: each defined variable is allocated at its op, every variable
-// that is neither an input nor an output is freed after its last use.  Synchronises where
-// an op's output size is needed (as the reference's GetSize / Resize kernels do).
-extern "C" rfx_status rfx_exec_run(rfx_exec* x, void* stream) {
-  if (!x) return RFX_ERR_INVALID;
-  x->stream = as_stream(stream);
+namespace rfx {
+namespace {
+
+// The op sequence: each defined variable is allocated at its op, every variable that is
+// neither an input nor an output is freed after its last use.
+rfx_status run_ops(rfx_exec* x) {
   for (auto& kv : x->vars) {
     Var& v = kv.second;
     if (v.input && !v.ptr && v.rows) return fail(x, RFX_ERR_INVALID, "input '" + v.name + "' not bound");
@@ -637,7 +701,109 @@ extern "C" rfx_status rfx_exec_run(rfx_exec* x, void* stream) {
       if (!v.input && !v.output && v.last_use == (int)i) dev_free(x, v);
     }
   }
+  return RFX_OK;
+}
+
+}  // namespace
+}  // namespace rfx
+
+// Runs the plan on `stream`.  Synchronises where an op's output size is needed (as the
+// reference's GetSize / Resize kernels do).
+extern "C" rfx_status rfx_exec_run(rfx_exec* x, void* stream) {
+  if (!x) return RFX_ERR_INVALID;
+  x->stream = as_stream(stream);
+  rfx_status st = run_ops(x);
+  if (st != RFX_OK) return st;
   RFX_CUDA_TRY(cudaStreamSynchronize(x->stream));
+  return RFX_OK;
+}
+
+// Captures the plan as a CUDA graph on `stream` (not the legacy default stream): one eager
+// run records the sizes it reads back and the allocations it makes; one arena of their
+// total size is allocated (counted against the budget); the op sequence is then captured
+// with its memory taken from the arena in the same order and the recorded sizes in place
+// of the read-backs.  Inputs stay bound to the same memory; outputs live in the arena
+// until the next capture or destroy.  Tuning (rfx_tune_set) must be off.
+extern "C" rfx_status rfx_exec_capture(rfx_exec* x, void* stream) {
+  if (!x) return RFX_ERR_INVALID;
+  if (!stream) return fail(x, RFX_ERR_INVALID, "capture: needs a non-default stream");
+  x->stream = as_stream(stream);
+  drop_graph(x);
+  x->rec_sizes.clear();
+  x->rec_allocs.clear();
+  x->recording = true;
+  rfx_status st = run_ops(x);
+  x->recording = false;
+  if (st != RFX_OK) return st;
+  RFX_CUDA_TRY(cudaStreamSynchronize(x->stream));
+  for (auto& kv : x->vars)
+    if (!kv.second.input) dev_free(x, kv.second);
+  RFX_CUDA_TRY(cudaStreamSynchronize(x->stream));
+  uint64_t need = 0;
+  for (uint64_t b : x->rec_allocs) need = align_up(need, 256) + b;
+  need = align_up(need, 256);
+  if (x->arena) {
+    x->in_use -= x->arena_bytes;
+    cudaFree(x->arena);
+    x->arena = nullptr;
+    x->arena_bytes = 0;
+  }
+  if (x->d_observed) {
+    cudaFree(x->d_observed);
+    x->d_observed = nullptr;
+  }
+  if (x->budget && x->in_use + need > x->budget) return fail(x, RFX_ERR_CAPACITY, "capture: arena over the budget");
+  RFX_CUDA_TRY(cudaMalloc(&x->arena, need ? need : 256));
+  x->arena_bytes = need ? need : 256;
+  x->in_use += x->arena_bytes;
+  if (x->in_use > x->peak) x->peak = x->in_use;
+  RFX_CUDA_TRY(cudaMalloc(&x->d_observed, (x->rec_sizes.size() + 1) * sizeof(uint64_t)));
+  x->capturing = true;
+  x->arena_used = 0;
+  x->size_pos = 0;
+  const uint64_t in_use0 = x->in_use;
+  cudaError_t e = cudaStreamBeginCapture(x->stream, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    st = run_ops(x);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e2 = cudaStreamEndCapture(x->stream, &g);
+    if (st == RFX_OK && e2 != cudaSuccess) st = cuda_fail(e2);
+    if (st == RFX_OK) {
+      x->graph = g;
+      const cudaError_t e3 = cudaGraphInstantiate(&x->gexec, g, 0);
+      if (e3 != cudaSuccess) {
+        st = cuda_fail(e3);
+        drop_graph(x);
+      }
+    } else if (g) {
+      cudaGraphDestroy(g);
+    }
+  } else {
+    st = cuda_fail(e);
+  }
+  x->capturing = false;
+  x->in_use = in_use0;   // the arena holds everything; nothing else stays allocated
+  return st;
+}
+
+// Replays the captured plan on `stream` and waits for it.  RFX_ERR_CAPACITY when an
+// intermediate size differs from the captured one (the inputs' contents changed the
+// plan's shape): the outputs are then invalid and the plan must run eagerly or be
+// captured again.
+extern "C" rfx_status rfx_exec_replay(rfx_exec* x, void* stream) {
+  if (!x || !x->gexec) return RFX_ERR_INVALID;
+  cudaStream_t s = as_stream(stream);
+  RFX_CUDA_TRY(cudaGraphLaunch(x->gexec, s));
+  std::vector<uint64_t> seen(x->rec_sizes.size());
+  if (!seen.empty())
+    RFX_CUDA_TRY(cudaMemcpyAsync(seen.data(), x->d_observed, seen.size() * sizeof(uint64_t), cudaMemcpyDeviceToHost,
+                                 s));
+  RFX_CUDA_TRY(cudaStreamSynchronize(s));
+  for (size_t i = 0; i < seen.size(); ++i)
+    if (seen[i] != x->rec_sizes[i])
+      return fail(x, RFX_ERR_CAPACITY, "replay: size " + std::to_string(i) + " is " + std::to_string(seen[i]) +
+                                           ", captured " + std::to_string(x->rec_sizes[i]));
+  ++x->launches;
   return RFX_OK;
 }
 

@@ -52,6 +52,58 @@ rfx_status dispatch_fb(uint32_t le, uint32_t re, FindBoundsArgs& a, cudaStream_t
   return RFX_ERR_UNSUPPORTED;
 }
 
+template <int LE, int RE>
+rfx_status launch_group(FindBoundsArgs& a, cudaStream_t s) {
+  auto k = find_bounds_kernel<LE, RE, true>;
+  RFX_CUDA_TRY(allow_smem((const void*)k, kFbWindowBytes));
+  const uint64_t tiles = (a.nl + kFbTile - 1) / kFbTile;
+  const int grid = persistent_grid((const void*)k, kJoinThreads, kFbWindowBytes, tiles ? tiles : 1);
+  k<<<grid, kJoinThreads, kFbWindowBytes, s>>>(a);
+  RFX_CUDA_TRY(cudaGetLastError());
+  return RFX_OK;
+}
+
+rfx_status dispatch_group(uint32_t ke, uint32_t re, FindBoundsArgs& a, cudaStream_t s) {
+#define RFX_GJ(L, R) \
+  if (ke == L && re == R) return launch_group<L, R>(a, s);
+  RFX_GJ(4, 4) RFX_GJ(4, 8) RFX_GJ(4, 16) RFX_GJ(8, 4) RFX_GJ(8, 8) RFX_GJ(8, 16)
+#undef RFX_GJ
+  return RFX_ERR_UNSUPPORTED;
+}
+
+// Workspace of rfx_join_aggregate: the right side's groups (keys, sums, counts, their
+// number), the group join's tile status, then the reduce's own workspace.
+struct JaLayout {
+  uint8_t* gkeys;
+  int64_t* gsum;
+  uint32_t* gcnt;
+  uint64_t* ngroups;
+  uint64_t* status;
+  uint32_t* counter;
+  size_t clear_off, clear;   // status + counter
+  void* rws;
+  size_t rws_bytes;
+  size_t total;
+};
+
+JaLayout ja_layout(void* ws, uint64_t nr, uint32_t kb) {
+  JaLayout L;
+  Carver c(ws);
+  L.gkeys = c.take<uint8_t>(nr * kb);
+  L.gsum = c.take<int64_t>(nr);
+  L.gcnt = c.take<uint32_t>(nr);
+  L.ngroups = c.take<uint64_t>(1);
+  c.used = align_up(c.used, 256);
+  L.clear_off = c.used;
+  L.status = c.take<uint64_t>((nr + kFbTile - 1) / kFbTile + 1);
+  L.counter = c.take<uint32_t>(1);
+  L.clear = c.used - L.clear_off;
+  L.rws_bytes = rfx_reduce_by_key_workspace(nr);
+  L.rws = c.take<uint8_t>(L.rws_bytes);
+  L.total = align_up(c.used, 256);
+  return L;
+}
+
 template <int LE, int RE, int OE>
 rfx_status launch_tj(TupleJoinArgs& a, cudaStream_t s) {
   auto k = tuple_join_kernel<LE, RE, OE>;
@@ -221,6 +273,66 @@ extern "C" rfx_status rfx_join_tuples(void* out, uint32_t out_bytes, uint64_t ca
   j.out = static_cast<uint8_t*>(out);
   j.cap = capacity;
   return dispatch_tj(left_bytes, right_bytes, out_bytes, j, s);
+}
+
+extern "C" size_t rfx_join_aggregate_workspace(uint64_t nr, uint32_t out_key_bytes) {
+  return ja_layout(nullptr, nr, out_key_bytes).total;
+}
+
+// The join of left and right on their keys followed by SUM(right value) and COUNT per key,
+// without the join rows: the right side is reduced to its groups, then each group whose
+// key occurs on the left is kept with its sum and count multiplied by the number of left
+// rows that carry the key -- per key the join has n_left(k) x n_right(k) rows whose values
+// sum to n_left(k) x (sum of the right values), and the products wrap modulo 2^64 / 2^32
+// exactly as the sums over the join rows do.
+extern "C" rfx_status rfx_join_aggregate(const void* left, uint64_t nl, uint32_t left_bytes, uint32_t left_value_bits,
+                                         const void* right, uint64_t nr, uint32_t right_bytes,
+                                         uint32_t right_value_bits, uint32_t value_shift, uint32_t value_bits,
+                                         void* out_keys, uint32_t out_key_bytes, int64_t* out_sums,
+                                         uint32_t* out_counts, uint64_t* d_groups, void* workspace,
+                                         size_t workspace_bytes, void* stream) {
+  const bool w_ok = (left_bytes == 4 || left_bytes == 8 || left_bytes == 16) &&
+                    (right_bytes == 4 || right_bytes == 8 || right_bytes == 16) &&
+                    (out_key_bytes == 4 || out_key_bytes == 8);
+  if (!w_ok || left_value_bits >= left_bytes * 8u || right_value_bits >= right_bytes * 8u || value_bits > 64 ||
+      value_shift + value_bits > right_bytes * 8u)
+    return RFX_ERR_UNSUPPORTED;
+  // the right key is stored in out_key_bytes (bits above are dropped, as
+  // rfx_reduce_tuples drops them): the caller's key fields must fit that width
+  if (!d_groups || (nl && !left) || (nr && !right) || (nr && (!out_keys || !out_sums || !out_counts)))
+    return RFX_ERR_INVALID;
+  if ((nl && !aligned_to(left, left_bytes)) || (nr && !aligned_to(right, right_bytes)) ||
+      (nr && !aligned_to(out_keys, out_key_bytes)))
+    return RFX_ERR_INVALID;
+  cudaStream_t s = as_stream(stream);
+  JaLayout L = ja_layout(workspace, nr, out_key_bytes);
+  if (!workspace || workspace_bytes < L.total) return RFX_ERR_WORKSPACE;
+  if (nr == 0) return cuda_fail(cudaMemsetAsync(d_groups, 0, sizeof(uint64_t), s));
+  uint32_t* err = device_error_word();
+  if (!err) return RFX_ERR_CUDA;
+  rfx_status st = rfx_reduce_tuples(right, nr, nullptr, right_bytes, right_value_bits, value_shift, value_bits,
+                                    L.gkeys, out_key_bytes, L.gsum, L.gcnt, L.ngroups, L.rws, L.rws_bytes, stream);
+  if (st != RFX_OK) return st;
+  RFX_CUDA_TRY(cudaMemsetAsync(static_cast<uint8_t*>(workspace) + L.clear_off, 0, L.clear, s));
+  FindBoundsArgs a;
+  std::memset(&a, 0, sizeof(a));
+  a.left = L.gkeys;
+  a.nl = nr;
+  a.d_nl = L.ngroups;
+  a.right = static_cast<const uint8_t*>(left);
+  a.nr = nl;
+  a.lshift = 0;
+  a.rshift = left_value_bits;
+  a.d_total = d_groups;
+  a.status = L.status;
+  a.tile_counter = L.counter;
+  a.err = err;
+  a.gsum = L.gsum;
+  a.gcnt = L.gcnt;
+  a.okey = static_cast<uint8_t*>(out_keys);
+  a.osum = out_sums;
+  a.ocnt = out_counts;
+  return dispatch_group(out_key_bytes, left_bytes, a, s);
 }
 
 // ---- reference-compatible entries (synchronous, own their scratch) ----

@@ -36,6 +36,15 @@ struct FindBoundsArgs {
   uint64_t* status;
   uint32_t* tile_counter;
   uint32_t* err;
+  // join-aggregate mode: the left side is a table of groups (one row per distinct key,
+  // with its SUM and COUNT); a group is kept when its key occurs on the right, with its
+  // SUM and COUNT multiplied by the number of right rows that carry the key
+  const uint64_t* d_nl;      // device-resident left size (<= nl), or null
+  const int64_t* gsum;
+  const uint32_t* gcnt;
+  uint8_t* okey;             // kept keys, LE bytes each
+  int64_t* osum;
+  uint32_t* ocnt;
 };
 
 // Block-wide exclusive sum of one 64-bit value per thread.
@@ -75,7 +84,10 @@ __device__ __forceinline__ uint32_t smem_bound(const T* w, uint32_t n, u128 k, b
   return lo;
 }
 
-template <int LE, int RE>
+// GROUP = false: find_bounds (lower bounds, equality counts, their exclusive scan, total).
+// GROUP = true: the join-aggregate (see FindBoundsArgs): the block scan counts kept groups
+// instead of matches and *d_total receives the number of kept groups.
+template <int LE, int RE, bool GROUP = false>
 __global__ void __launch_bounds__(kJoinThreads) find_bounds_kernel(const FindBoundsArgs a) {
   extern __shared__ __align__(16) uint8_t fb_window[];
   uint64_t* s_win64 = reinterpret_cast<uint64_t*>(fb_window);
@@ -87,8 +99,9 @@ __global__ void __launch_bounds__(kJoinThreads) find_bounds_kernel(const FindBou
   __shared__ uint32_t s_tile;
   __shared__ uint64_t s_lo, s_hi;
   const uint32_t t = threadIdx.x;
-  const uint64_t num_tiles = (a.nl + kFbTile - 1) / kFbTile;
-  const KeyView<LE> L{a.left, a.nl, a.lshift};
+  const uint64_t nl = a.d_nl ? min(a.nl, *a.d_nl) : a.nl;
+  const uint64_t num_tiles = (nl + kFbTile - 1) / kFbTile;
+  const KeyView<LE> L{a.left, nl, a.lshift};
   const KeyView<RE> R{a.right, a.nr, a.rshift};
   while (true) {
     if (t == 0) s_tile = atomicAdd(a.tile_counter, 1u);
@@ -96,7 +109,7 @@ __global__ void __launch_bounds__(kJoinThreads) find_bounds_kernel(const FindBou
     const uint64_t tile = s_tile;
     if (tile >= num_tiles) break;
     const uint64_t tfirst = tile * kFbTile;
-    const uint64_t tlast = min(tfirst + kFbTile, a.nl) - 1;
+    const uint64_t tlast = min(tfirst + kFbTile, nl) - 1;
     // the window of right keys between the tile's smallest and largest left key
     if (t < 32) {
       const uint64_t lo = warp_search<RE>(R, L.key(tfirst), 0, a.nr, false);
@@ -125,7 +138,7 @@ __global__ void __launch_bounds__(kJoinThreads) find_bounds_kernel(const FindBou
       const uint64_t i = first + j;
       lo[j] = 0;
       cnt[j] = 0;
-      if (i >= a.nl) continue;
+      if (i >= nl) continue;
       const u128 k = L.key(i);
       if (j > 0 && k == prevk) {
         lo[j] = plo;
@@ -148,7 +161,7 @@ __global__ void __launch_bounds__(kJoinThreads) find_bounds_kernel(const FindBou
         phi = h;
         prevk = k;
       }
-      tsum += cnt[j];
+      tsum += GROUP ? (cnt[j] != 0) : cnt[j];
     }
     uint64_t btot;
     const uint64_t ex = block_exclusive_u64(tsum, s_warp, &btot);
@@ -158,16 +171,30 @@ __global__ void __launch_bounds__(kJoinThreads) find_bounds_kernel(const FindBou
         s_prefix = pre;
         if (tile == num_tiles - 1) {
           *a.d_total = pre + btot;
-          if (a.off64) a.off64[a.nl] = pre + btot;
+          if (a.off64) a.off64[nl] = pre + btot;
         }
       }
     }
     __syncthreads();
     uint64_t run = s_prefix + ex;
+    if constexpr (GROUP) {
+      // kept groups in left order; products wrap like the sums of the join rows would
+#pragma unroll
+      for (int j = 0; j < kFbIPT; ++j) {
+        const uint64_t i = first + j;
+        if (i >= nl || cnt[j] == 0) continue;
+        store_u128<LE>(a.okey, run, load_u128<LE>(a.left, i));
+        a.osum[run] = (int64_t)((uint64_t)a.gsum[i] * cnt[j]);
+        a.ocnt[run] = a.gcnt[i] * (uint32_t)cnt[j];
+        ++run;
+      }
+      __syncthreads();
+      continue;
+    }
 #pragma unroll
     for (int j = 0; j < kFbIPT; ++j) {
       const uint64_t i = first + j;
-      if (i >= a.nl) continue;
+      if (i >= nl) continue;
       if (a.lb32) a.lb32[i] = (int32_t)lo[j];
       if (a.scan32) a.scan32[i] = (int32_t)(uint32_t)run;
       if (a.lb64) a.lb64[i] = lo[j];
@@ -176,7 +203,7 @@ __global__ void __launch_bounds__(kJoinThreads) find_bounds_kernel(const FindBou
     }
     __syncthreads();
   }
-  if (a.nl == 0 && blockIdx.x == 0 && t == 0) {
+  if (nl == 0 && blockIdx.x == 0 && t == 0) {
     *a.d_total = 0;
     if (a.off64) a.off64[0] = 0;
   }

@@ -4,6 +4,8 @@
 
 #include "host_common.h"
 #include "sort_kernels.cuh"
+#include "sort_onesweep.cuh"
+#include "tune.h"
 
 namespace rfx {
 
@@ -52,11 +54,36 @@ rfx_status run_sort_kv(SortPlan& s) {
     RFX_CUDA_TRY(cudaStreamSynchronize(s.stream));
     for (uint32_t p = 0; p < s.passes; ++p) triv[p] = s.host_trivial[p];
   }
+  // Pass variants: 0 = the pipelined onesweep pass (TMA stages + look-back warp) where it
+  // applies -- keys without values in 4/8/16-byte containers on 16-byte aligned buffers --
+  // 1 = the per-tile pass (every width, values too), 2 / 3 = the onesweep pass with fewer
+  // / other numbers of items per thread.  The autotuner may pick per size class.
   constexpr size_t ek = sizeof(Elem<K>), ev = V > 0 ? sizeof(Elem<V>) : 0;
-  const size_t smem = (size_t)T::TILE * (ek > ev ? ek : ev);
-  auto pk = sort_pass_kernel<K, V>;
-  RFX_CUDA_TRY(allow_smem((const void*)pk, smem));
-  const int grid = persistent_grid((const void*)pk, kSortThreads, smem, s.tiles ? s.tiles : 1);
+  const size_t tile_smem = (size_t)T::TILE * (ek > ev ? ek : ev);
+  RFX_CUDA_TRY(allow_smem((const void*)sort_pass_kernel<K, V>, tile_smem));
+  const int tile_grid = persistent_grid((const void*)sort_pass_kernel<K, V>, kSortThreads, tile_smem,
+                                        s.tiles ? s.tiles : 1);
+  constexpr bool kOnesweep = V == 0 && (K == 4 || K == 8 || K == 16);
+  bool os_ok = false;
+  int os_grid[3] = {0, 0, 0};   // default, small, alternative tiles
+  if constexpr (kOnesweep) {
+    os_ok = ((reinterpret_cast<uintptr_t>(s.keys) | reinterpret_cast<uintptr_t>(s.alt_keys)) & 15u) == 0;
+    if (os_ok) {
+      auto prep = [&](const void* k, size_t smem, int tile, int* grid) -> rfx_status {
+        RFX_CUDA_TRY(allow_smem(k, smem));
+        const uint64_t ot = (s.n + tile - 1) / tile;
+        *grid = persistent_grid(k, kOsThreads, smem, ot ? ot : 1);
+        return RFX_OK;
+      };
+      using TD = OsTuning<K, OsIpt<K>::DEF>;
+      using TS = OsTuning<K, OsIpt<K>::SMALL>;
+      using TL = OsTuning<K, OsIpt<K>::ALT>;
+      rfx_status st = prep((const void*)sort_onesweep_kernel<K, TD::IPT>, TD::SMEM, TD::TILE, &os_grid[0]);
+      if (st == RFX_OK) st = prep((const void*)sort_onesweep_kernel<K, TS::IPT>, TS::SMEM, TS::TILE, &os_grid[1]);
+      if (st == RFX_OK) st = prep((const void*)sort_onesweep_kernel<K, TL::IPT>, TL::SMEM, TL::TILE, &os_grid[2]);
+      if (st != RFX_OK) return st;
+    }
+  }
   const uint8_t* kin = s.keys;
   const uint8_t* vin = s.vals;
   uint8_t* kout = s.alt_keys;
@@ -78,8 +105,36 @@ rfx_status run_sort_kv(SortPlan& s) {
     a.status = s.status + (uint64_t)p * s.tiles * kRadix;
     a.tile_counter = s.counters + p;
     a.err = s.err;
-    pk<<<grid, kSortThreads, smem, s.stream>>>(a);
-    RFX_CUDA_TRY(cudaGetLastError());
+    // a pass reads kin and writes kout only, so a candidate can run again (the tuner
+    // times each one); the look-back words and the tile counter are cleared between runs
+    bool fresh = true;
+    auto launch = [&](int v) -> rfx_status {
+      if (!fresh) {
+        RFX_CUDA_TRY(cudaMemsetAsync(a.status, 0, (size_t)s.tiles * kRadix * sizeof(uint32_t), s.stream));
+        RFX_CUDA_TRY(cudaMemsetAsync(a.tile_counter, 0, sizeof(uint32_t), s.stream));
+      }
+      fresh = false;
+      if constexpr (kOnesweep) {
+        using TD = OsTuning<K, OsIpt<K>::DEF>;
+        using TS = OsTuning<K, OsIpt<K>::SMALL>;
+        using TL = OsTuning<K, OsIpt<K>::ALT>;
+        if (os_ok && v == 0)
+          sort_onesweep_kernel<K, TD::IPT><<<os_grid[0], kOsThreads, TD::SMEM, s.stream>>>(a);
+        else if (os_ok && v == 2)
+          sort_onesweep_kernel<K, TS::IPT><<<os_grid[1], kOsThreads, TS::SMEM, s.stream>>>(a);
+        else if (os_ok && v == 3)
+          sort_onesweep_kernel<K, TL::IPT><<<os_grid[2], kOsThreads, TL::SMEM, s.stream>>>(a);
+        else
+          sort_pass_kernel<K, V><<<tile_grid, kSortThreads, tile_smem, s.stream>>>(a);
+      } else {
+        sort_pass_kernel<K, V><<<tile_grid, kSortThreads, tile_smem, s.stream>>>(a);
+      }
+      RFX_CUDA_TRY(cudaGetLastError());
+      return RFX_OK;
+    };
+    const int v = os_ok ? tune_pick(TUNE_SORT_PASS, (uint64_t)K << 8 | V, s.n, 4, launch, s.stream) : 1;
+    rfx_status st = launch(v);
+    if (st != RFX_OK) return st;
     ++s.executed;
     s.in_alt = !s.in_alt;
     const uint8_t* tk = kout;

@@ -25,6 +25,10 @@ def _declare():
     L.rfx_exec_stats.argtypes = [P, C.POINTER(u64), C.POINTER(u64), C.POINTER(u64), C.c_char_p, C.c_size_t]
     L.rfx_exec_copy_out.restype = st
     L.rfx_exec_copy_out.argtypes = [P, C.c_char_p, P, u64, P]
+    L.rfx_exec_capture.restype = st
+    L.rfx_exec_capture.argtypes = [P, P]
+    L.rfx_exec_replay.restype = st
+    L.rfx_exec_replay.argtypes = [P, P]
 
 
 _declare()
@@ -70,6 +74,16 @@ class Executor:
 
     def run(self, stream=None):
         self._check("rfx_exec_run", R.LIB.rfx_exec_run(self.h, R._stream(stream)))
+
+    def capture(self, stream):
+        """Capture the plan as a CUDA graph on `stream` (a torch.cuda.Stream, not the
+        default stream); runs it once eagerly first."""
+        self._check("rfx_exec_capture", R.LIB.rfx_exec_capture(self.h, R._stream(stream)))
+
+    def replay(self, stream):
+        """Launch the captured graph; raises when an intermediate size differs from the
+        captured one (RFX_ERR_CAPACITY: run eagerly or capture again)."""
+        self._check("rfx_exec_replay", R.LIB.rfx_exec_replay(self.h, R._stream(stream)))
 
     def output(self, name, stream=None):
         """A copy of the variable's rows as a (rows, row_bytes) uint8 tensor."""

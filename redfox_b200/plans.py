@@ -47,6 +47,18 @@ def join_aggregate(r, s, stream=None):
     return keys, sums, counts, total
 
 
+def join_aggregate_fused(r, s, stream=None):
+    """The same plan with the join and the aggregate as one operator: sort R, sort S, then
+    SUM(amount) and COUNT per key straight from the sorted relations (rfx_join_aggregate;
+    the join rows are never written).  Returns (keys u32, sums int64, counts u32) -- the
+    bytes join_aggregate returns."""
+    r = r.clone()
+    s = s.clone()
+    R.sort_pairs(r, begin_bit=32, end_bit=64, stream=stream)
+    R.sort_pairs(s, begin_bit=64, end_bit=96, stream=stream)
+    return R.join_aggregate(r, 32, s, 64, 0, 64, 4, stream=stream)
+
+
 # ---------------------------------------------------------------- three-relation pipeline
 C2_D1_ROWS = 1_500_000
 C2_D2_ROWS = 15_000_000

@@ -481,6 +481,10 @@ def _declare_tuple_ops():
     more = {
         "rfx_reduce_tuples": (st, [P, u64, P, u32, u32, u32, u32, P, u32, P, P, P, P, sz, P]),
         "rfx_join_tuples_emit": (st, [P, u32, u64, P, u64, u32, P, u64, u32, u32, P, sz, P]),
+        "rfx_multi_select_workspace": (sz, [u64]),
+        "rfx_multi_select": (st, [P, u64, P, P, u64, u32, u32, u32, P, P, u32, u32, u32, u32, u32, P, sz, P]),
+        "rfx_join_aggregate_workspace": (sz, [u64, u32]),
+        "rfx_join_aggregate": (st, [P, u64, u32, u32, P, u64, u32, u32, u32, u32, P, u32, P, P, P, P, sz, P]),
     }
     for name, (res, args) in more.items():
         f = getattr(LIB, name)
@@ -524,6 +528,68 @@ def join_tuples_two_step(left, lvbits, right, rvbits, out_bytes, stream=None):
     return out[:total], total
 
 
+def multi_select(rows, field, bounds, key, val, capacity=None, stream=None):
+    """One scan of `rows` for many range selections: bounds = [(lo, hi), ...] (at most 256
+    queries); field / key / val = (shift, width) bit fields of a row.  Returns the 8-byte
+    rows ((key << 8 | q) << val_width) | val in (row, query) order (int64 tensor) and
+    their number.  With capacity None the count is taken first (two calls)."""
+    import torch
+    n = rows.shape[0]
+    nq = len(bounds)
+    lo = (C.c_uint32 * nq)(*[b[0] for b in bounds])
+    hi = (C.c_uint32 * nq)(*[b[1] for b in bounds])
+    cnt = torch.zeros(1, dtype=torch.int64, device=rows.device)
+    wsb = LIB.rfx_multi_select_workspace(n)
+    ws = _empty_bytes(wsb, rows.device)
+
+    def call(out, cap):
+        check("rfx_multi_select", LIB.rfx_multi_select(
+            _ptr(out), cap, _ptr(cnt), _ptr(rows), n, _width(rows), field[0], field[1], lo, hi, nq, key[0], key[1],
+            val[0], val[1], _ptr(ws), wsb, _stream(stream)))
+    if capacity is None:
+        call(None, 0)
+        capacity = int(cnt.item())
+    out = torch.empty(max(1, capacity), dtype=torch.int64, device=rows.device)
+    call(out, capacity)
+    k = int(cnt.item())
+    return out[:min(k, capacity)], k
+
+
+class JoinAggregate:
+    """A prepared rfx_join_aggregate (join on the key + SUM(right value) and COUNT per key,
+    no join rows written): outputs of capacity nr and the workspace allocated once, sizes
+    stay on the device, so repeated calls allocate nothing and can be graph-captured."""
+
+    def __init__(self, nr, out_key_bytes=4, device="cuda"):
+        import torch
+        self.nr = nr
+        self.kb = out_key_bytes
+        self.keys = torch.empty(max(1, nr), dtype={4: torch.int32, 8: torch.int64}[out_key_bytes], device=device)
+        self.sums = torch.empty(max(1, nr), dtype=torch.int64, device=device)
+        self.counts = torch.empty(max(1, nr), dtype=torch.int32, device=device)
+        self.groups = torch.zeros(1, dtype=torch.int64, device=device)
+        self.wsb = LIB.rfx_join_aggregate_workspace(nr, out_key_bytes)
+        self.ws = _empty_bytes(self.wsb, device)
+
+    def __call__(self, left, lvbits, right, rvbits, value_shift, value_bits, stream=None):
+        assert right.shape[0] <= self.nr
+        check("rfx_join_aggregate", LIB.rfx_join_aggregate(
+            _ptr(left), left.shape[0], _width(left), lvbits, _ptr(right), right.shape[0], _width(right), rvbits,
+            value_shift, value_bits, _ptr(self.keys), self.kb, _ptr(self.sums), _ptr(self.counts), _ptr(self.groups),
+            _ptr(self.ws), self.wsb, _stream(stream)))
+
+    def result(self):
+        g = int(self.groups.item())
+        return self.keys[:g], self.sums[:g], self.counts[:g]
+
+
+def join_aggregate(left, lvbits, right, rvbits, value_shift, value_bits, out_key_bytes=4, stream=None):
+    """(keys, sums, counts) of the join of left and right on their keys, aggregated on the key."""
+    ja = JoinAggregate(right.shape[0], out_key_bytes, device=left.device)
+    ja(left, lvbits, right, rvbits, value_shift, value_bits, stream)
+    return ja.result()
+
+
 # ---------------------------------------------------------------- autotuning
 def _declare_tune():
     LIB.rfx_tune_set.restype = None
@@ -538,7 +604,8 @@ def _declare_tune():
 
 _declare_tune()
 
-TUNE_OPS = {1: "reduce_tuples", 2: "set_filter", 3: "select_compact", 4: "filter_aggregate"}
+TUNE_OPS = {1: "reduce_tuples", 2: "set_filter", 3: "select_compact", 4: "filter_aggregate", 5: "sort_pass"}
+TUNE_SORT_PASS = 5   # variants: 0 onesweep pass, 1 per-tile pass, 2 / 3 onesweep with other tile sizes
 
 
 def tune(mode=1):

@@ -1,9 +1,11 @@
 """Serving form: resident base relations, a request loop that admits queued queries
-against a device-memory budget for their intermediates, and continuous batching --
-queries that arrive while others run are admitted as soon as a slot and budget free up,
-and their work overlaps on the device (one CUDA stream per slot; every operator is a
-persistent kernel that claims its tiles dynamically, so kernels of different queries
-share the SMs without waiting on one another).
+against a device-memory budget for their intermediates, and continuous batching: the
+queries admitted since the last round started are packed into one batched plan (the query
+id folded into the low 8 bits of every key, as the batched form folds it into the high
+bits), so one scan of D1 and D2, one sort, one join, one intersection, one join with F and
+one reduce serve all of them.  Up to `slots` rounds are in flight at once on their own
+CUDA streams, so a round admitted while another runs overlaps it on the device (every
+operator is a persistent kernel that claims its tiles dynamically).
 
 The query (the three-relation pipeline with parameters): select D1 on a segment, select
 D2 on a date range [lo, lo + width), join D2 to D1, optionally intersect the D2 keys with
@@ -15,7 +17,8 @@ sorted list of log-uniform [1e3, 1e6] distinct keys drawn from D2's keys.
 `Scheduler` is the admission logic alone (no GPU): FIFO, at most `slots` queries in
 flight, and the sum of the in-flight queries' estimated intermediate bytes within the
 budget (a query larger than the whole budget runs alone).  `simulate` drives it with a
-given service time per query on a virtual clock.  `Server` runs it for real.
+given service time per query on a virtual clock.  `Server` runs it for real: batched
+rounds (`run_round`), or one plain query at a time (`run_query`) as the serial baseline.
 """
 import collections
 import math
@@ -216,29 +219,137 @@ def run_alone(res, q, device="cuda"):
     return tuple(t.cpu() for t in out)
 
 
-class Server:
-    """Request loop over resident relations: a dispatcher admits arrived queries through a
-    Scheduler, and one worker thread per slot runs each admitted query on the slot's CUDA
-    stream and copies its result to the host.  Latency = host time from arrival to the
-    result on the host."""
+def _fold_lists(lists, stream=None):
+    """Per-query sorted distinct u32 key lists -> one sorted list of (key << 8 | q) in
+    8-byte elements (int64)."""
+    import torch
 
-    def __init__(self, res, slots=8, budget_bytes=BUDGET_BYTES, device="cuda"):
+    from . import rfx as R
+    parts = [(lst.to(torch.int64) & 0xFFFFFFFF) << 8 | q for q, lst in enumerate(lists)]
+    folded = torch.cat(parts) if parts else torch.zeros(0, dtype=torch.int64)
+    R.sort_pairs(folded, begin_bit=0, end_bit=40, stream=stream)
+    return folded
+
+
+def run_round(res, queries, lists=None, stream=None):
+    """The queries of one admission round as one batched plan.  Every key carries the
+    query id q (index in `queries`, < 256) in its low 8 bits, so each operator serves all
+    queries at once and never mixes them:
+
+      D1 scan    rows (pk << 8 | q, seg)        for each q with seg == segment_q
+      D2 scan    rows (fk << 8 | q, pk)         for each q with date in [lo_q, hi_q)
+      sort       D2 rows on (fk, q)
+      join       on (pk, q) = (fk, q)           -> (pk1, q, seg, pk2)
+      project    (pk2, q), sort, and with lists: intersect with the folded lists
+      join F     on pk2 (the query bits sit below the key)  -> (pk2, q, amount)
+      reduce     SUM(amount), COUNT by (pk2, q)
+
+    `lists`: None, or one sorted distinct u32 key list per query (every query of the
+    round then has one).  Returns the reduce's (keys = pk2 << 8 | q as int64, sums,
+    counts) on the device; `split_round` separates the queries."""
+    import torch
+
+    from . import rfx as R
+    assert 0 < len(queries) <= 256
+    d1m, _ = R.multi_select(res.d1, (0, 8), [(q.segment, q.segment + 1) for q in queries], (8, 32), (0, 8),
+                            stream=stream)                                         # Tuple<32,8,8>
+    d2m, _ = R.multi_select(res.d2, (0, 32), [(q.date_lo, q.date_hi) for q in queries], (32, 24), (64, 32),
+                            stream=stream)                                         # Tuple<24,8,32>
+    d1r = d1m.view(torch.uint8).view(-1, 8)
+    d2r = d2m.view(torch.uint8).view(-1, 8)
+    R.sort_pairs(d2r, begin_bit=32, end_bit=64, stream=stream)                      # on (fk, q)
+    j1, _ = R.join_tuples_two_step(d1r, 8, d2r, 32, 16, stream=stream)               # (pk1, q, seg, pk2)
+    keys = R.project(j1, [32, 8, 8, 32], [32, 8], [3, 1], stream=stream).clone()    # (pk2, q)
+    R.sort_pairs(keys, begin_bit=0, end_bit=40, stream=stream)
+    if lists is not None:
+        keys = R.set_op(R.SET_INTERSECTION, keys, _fold_lists(lists, stream).view(torch.uint8).view(-1, 8),
+                        stream=stream)
+    j2, total = R.join_tuples_two_step(keys, 8, res.f_sorted, 64, 16, stream=stream)  # (pk2, q, amount)
+    gk, gs, gc, _ = R.reduce_tuples(j2, 64, 0, 64, 8, n=total, stream=stream)
+    return gk, gs, gc
+
+
+def split_round(gk, gs, gc, nq):
+    """Host copies of a round's groups -> per query (keys u32, sums int64, counts u32) in
+    key order (the round's groups are ordered by (pk2, q))."""
+    import numpy as np
+    k = gk.cpu().numpy().view(np.uint64)
+    sums = gs.cpu().numpy()
+    counts = gc.cpu().numpy().view(np.uint32)
+    q = (k & np.uint64(0xFF)).astype(np.int64)
+    order = np.argsort(q, kind="stable")
+    bounds = np.searchsorted(q[order], np.arange(nq + 1))
+    out = []
+    for i in range(nq):
+        sel = order[bounds[i]:bounds[i + 1]]
+        out.append(((k[sel] >> np.uint64(8)).astype(np.uint32), sums[sel], counts[sel]))
+    return out
+
+
+def run_round_host(res, queries, device="cuda", stream=None):
+    """A round end to end: lists generated, queries with and without a list run as two
+    batched plans (the intersection applies to the first only), results on the host in
+    the order of `queries`."""
+    import torch
+    res_by_q = [None] * len(queries)
+    with_list = [i for i, q in enumerate(queries) if q.list_size > 0]
+    without = [i for i, q in enumerate(queries) if q.list_size == 0]
+    for idx, has in ((with_list, True), (without, False)):
+        if not idx:
+            continue
+        qs = [queries[i] for i in idx]
+        lists = [query_list(q, res.n2, device) for q in qs] if has else None
+        gk, gs, gc = run_round(res, qs, lists, stream=stream)
+        if stream is not None:
+            stream.synchronize()
+        else:
+            torch.cuda.synchronize()
+        for i, r in zip(idx, split_round(gk, gs, gc, len(qs))):
+            res_by_q[i] = r
+    return res_by_q
+
+
+class Server:
+    """Request loop over resident relations.  A dispatcher admits arrived queries through a
+    Scheduler (FIFO, budget) and packs the admitted queries into rounds of at most
+    `max_batch`; up to `slots` worker threads each run a round on their own CUDA stream
+    (`run_round`) and complete its queries when its results are on the host.  With
+    plain=True every round is one query run by `run_query` (the serial plain baseline
+    when slots = 1).  Latency = host time from arrival to the result on the host."""
+
+    def __init__(self, res, slots=2, budget_bytes=BUDGET_BYTES, device="cuda", max_batch=128, plain=False):
         import torch
         self.res = res
         self.slots = slots
         self.budget = budget_bytes
+        self.plain = plain
+        self.max_batch = 1 if plain else max(1, min(256, max_batch))
         self.device = torch.device(device)
         if self.device.index is None:
             self.device = torch.device("cuda", torch.cuda.current_device())
         self.streams = [torch.cuda.Stream(device=self.device) for _ in range(slots)]
 
+    def _run(self, i, rnd, keep_results):
+        import torch
+        if self.plain:
+            q = rnd[0]
+            lst = query_list(q, self.res.n2, self.device)
+            out = run_query(self.res, q, lst)
+            host = tuple(t.to("cpu", non_blocking=True) for t in out)
+            self.streams[i].synchronize()
+            return [host]
+        return run_round_host(self.res, rnd, self.device, stream=self.streams[i])
+
     def serve(self, requests, keep_results=False):
         import torch
-        sch = Scheduler(self.slots, self.budget)
+        sch = Scheduler(self.slots * self.max_batch, self.budget)
         cv = threading.Condition()
-        work = [collections.deque() for _ in range(self.slots)]
+        ready = collections.deque()        # admitted, not yet in a round
+        work = [None] * self.slots          # the round each worker runs
+        busy = [False] * self.slots
         stop = [False]
         errors = []
+        self.rounds = []
         t0 = time.perf_counter()
 
         def worker(i):
@@ -246,22 +357,24 @@ class Server:
             with torch.cuda.stream(self.streams[i]):
                 while True:
                     with cv:
-                        while not work[i] and not stop[0]:
+                        while work[i] is None and not stop[0]:
                             cv.wait()
-                        if not work[i]:
+                        if work[i] is None:
                             return
-                        q = work[i].popleft()
+                        rnd = work[i]
                     try:
-                        lst = query_list(q, self.res.n2, self.device)
-                        out = run_query(self.res, q, lst)
-                        host = tuple(t.to("cpu", non_blocking=True) for t in out)
-                        self.streams[i].synchronize()
-                        q.result = host if keep_results else (int(host[0].shape[0]),)
+                        outs = self._run(i, rnd, keep_results)
+                        for q, host in zip(rnd, outs):
+                            q.result = host if keep_results else (int(host[0].shape[0]),)
                     except Exception as e:  # reported after the run
-                        errors.append((q.qid, repr(e)))
-                    q.done = time.perf_counter() - t0
+                        errors.append(([q.qid for q in rnd], repr(e)))
+                    done = time.perf_counter() - t0
                     with cv:
-                        sch.complete(q)
+                        for q in rnd:
+                            q.done = done
+                            sch.complete(q)
+                        work[i] = None
+                        busy[i] = False
                         cv.notify_all()
 
         threads = [threading.Thread(target=worker, args=(i,), daemon=True) for i in range(self.slots)]
@@ -275,9 +388,18 @@ class Server:
                 while nxt < len(order) and order[nxt].arrival <= now:
                     sch.arrive(order[nxt])
                     nxt += 1
-                for q, slot in sch.admissions():
-                    q.start = now
-                    work[slot].append(q)
+                for q, _slot in sch.admissions():
+                    ready.append(q)
+                for i in range(self.slots):
+                    if not ready:
+                        break
+                    if not busy[i]:
+                        rnd = [ready.popleft() for _ in range(min(self.max_batch, len(ready)))]
+                        for q in rnd:
+                            q.start = now
+                        self.rounds.append(len(rnd))
+                        work[i] = rnd
+                        busy[i] = True
                 cv.notify_all()
                 timeout = None
                 if nxt < len(order):

@@ -31,7 +31,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REFROOT = os.environ.get("RFX_REFERENCE_ROOT", "/root/reference")
+REFROOT = os.environ.get("RFX_REFERENCE_ROOT",
+                         os.path.join(os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))),
+                                      "reference"))
 sys.path.insert(0, REPO)
 
 import oracle as O  # noqa: E402

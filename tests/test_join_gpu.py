@@ -126,3 +126,57 @@ def test_reference_compatible_join_entries(cuda):
                                  C.c_void_p(lc.data_ptr()), 5000) == R.OK
     eli, eri = O.join_expand(elb, esc, etot)
     assert np.array_equal(to_np(li), eli) and np.array_equal(to_np(ri), eri)
+
+
+def _join_agg_oracle(left, right):
+    """join_tuples of R = Tuple<32,32> and S = Tuple<32,64> (output (key, payload, amount),
+    key in bits 96..127), then SUM(amount) and COUNT per key, on the oracle."""
+    out = O.join_tuples(left, 32, right, 64, 16)
+    if len(out) == 0:
+        return np.zeros(0, np.uint32), np.zeros(0, np.int64), np.zeros(0, np.uint32)
+    limbs = out.view(np.uint64)
+    keys = (limbs[:, 1] >> np.uint64(32)).astype(np.uint32)
+    vals = limbs[:, 0].astype(np.int64)
+    k, sums = O.reduce_sum_i64(keys, vals)
+    _, counts = O.reduce_count(keys)
+    return k, sums, counts
+
+
+@pytest.mark.parametrize("nr,ns,dom,extra", [(0, 100, 10, 0), (100, 0, 10, 0), (1, 1, 1, 0), (1000, 4000, 256, 0),
+                                             (50_000, 200_000, 12_500, 0), (20_000, 300_000, 40_000, 5_000),
+                                             (3_000, 500_000, 2_000, 0)])
+def test_join_aggregate_equals_join_then_reduce(cuda, nr, ns, dom, extra):
+    """rfx_join_aggregate == rfx_join_tuples + rfx_reduce_tuples == the oracle, including
+    right keys with no left match (`extra` rows with keys outside R's domain), left keys
+    with no right match, heavy duplication on both sides, and empty inputs."""
+    import torch
+    rng = np.random.default_rng(nr + 7 * ns)
+    rk = np.sort(rng.integers(0, dom, nr)).astype(np.uint64)
+    r = O.pack([32, 32], [rk, rng.integers(0, 2**32, nr).astype(np.uint64)])
+    sk = np.concatenate([rng.integers(0, dom, ns - extra), rng.integers(dom, 2 * dom, extra)]).astype(np.uint64)
+    s = O.pack([32, 64], [np.sort(sk), rng.integers(100, 10**7, ns).astype(np.uint64)])
+    rd, sd = _dev(r, cuda), _dev(s, cuda)
+    keys, sums, counts = R.join_aggregate(rd, 32, sd, 64, 0, 64, 4)
+    ek, es, ec = _join_agg_oracle(r, s) if nr and ns else (np.zeros(0, np.uint32),) * 3
+    assert np.array_equal(to_np(keys).view(np.uint32), ek)
+    assert np.array_equal(to_np(sums), np.asarray(es, np.int64))
+    assert np.array_equal(to_np(counts).view(np.uint32), np.asarray(ec, np.uint32))
+    if nr and ns:
+        out, total = R.join_tuples_two_step(rd, 32, sd, 64, 16)
+        gk, gs, gc, _ = R.reduce_tuples(out, 96, 0, 64, 4, n=total)
+        assert torch.equal(gk, keys) and torch.equal(gs, sums) and torch.equal(gc, counts)
+
+
+def test_join_aggregate_skewed_key(cuda):
+    """One key with 300K right rows and 2K left rows: its count (6e8) and its sum wrap
+    exactly like the 6e8 join rows would (checked against the closed form)."""
+    nr, ns = 2_000, 300_000
+    rng = np.random.default_rng(3)
+    r = O.pack([32, 32], [np.full(nr, 7, np.uint64), np.arange(nr, dtype=np.uint64)])
+    amounts = rng.integers(100, 10**7, ns).astype(np.uint64)
+    s = O.pack([32, 64], [np.full(ns, 7, np.uint64), amounts])
+    keys, sums, counts = R.join_aggregate(_dev(r, cuda), 32, _dev(s, cuda), 64, 0, 64, 4)
+    assert to_np(keys).view(np.uint32).tolist() == [7]
+    exp_sum = (int(amounts.astype(object).sum()) * nr) % (1 << 64)
+    assert int(to_np(sums).view(np.uint64)[0]) == exp_sum
+    assert int(to_np(counts).view(np.uint32)[0]) == (nr * ns) % (1 << 32)

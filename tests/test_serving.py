@@ -3,7 +3,11 @@ byte-budget limits, oversize queries running alone, and the effect of concurrenc
 latency under Poisson arrivals."""
 import math
 
+import numpy as np
+
 from redfox_b200 import serving as S
+
+from helpers import three_relation_oracle_data
 
 
 def _q(qid, arrival, est):
@@ -81,3 +85,65 @@ def test_simulated_budget_limits_concurrency():
     # FIFO: start times are non-decreasing in arrival (qid) order
     starts = [q.start for q in reqs]
     assert starts == sorted(starts)
+
+
+def _multi_select_np(rows, field, bounds, key, val):
+    """numpy restatement of rfx_multi_select: per row in order, per query in order, emit
+    ((key << 8 | q) << val_width) | val when lo_q <= field < hi_q."""
+    W = rows.shape[1]
+    limbs = rows.view(np.uint64) if W >= 8 else rows.view(np.uint32).astype(np.uint64)
+    if W == 16:
+        as_int = [int(lo) | (int(hi) << 64) for lo, hi in limbs]
+    else:
+        as_int = [int(x) for x in limbs.ravel()]
+
+    def bits(x, sw):
+        return (x >> sw[0]) & ((1 << sw[1]) - 1)
+    out = []
+    for x in as_int:
+        f = bits(x, field)
+        for q, (lo, hi) in enumerate(bounds):
+            if lo <= f < hi:
+                out.append((((bits(x, key) << 8) | q) << val[1]) | bits(x, val))
+    return np.array(out, dtype=np.uint64)
+
+
+def test_round_plan_layout_on_oracle():
+    """The batched round's bit layout (query id in the low 8 bits of every key) run with
+    the oracle's operators gives every query exactly the per-query oracle plan's groups."""
+    import oracle as O
+    from redfox_b200 import serving as S
+
+    from helpers import serving_query_oracle
+    n1, n2, n3 = 3000, 30000, 120000
+    d1, d2, f, _, _ = three_relation_oracle_data(n1, n2, n3, 10, 10)
+    fs = O.sort_pairs(f, begin_bit=64, end_bit=96)
+    reqs = S.gen_requests(12, 1e6, seed=5, n2=n2)
+    lists = {}
+    for q in reqs:
+        if q.list_size:
+            raw = O.uniform(q.list_size, q.list_seed, 0, 0, n2).astype(np.uint32)
+            lists[q.qid] = O.unique(O.sort_pairs(raw))
+    for group in ([q for q in reqs if q.list_size], [q for q in reqs if not q.list_size]):
+        d1m = _multi_select_np(d1, (0, 8), [(q.segment, q.segment + 1) for q in group], (8, 32), (0, 8))
+        d2m = _multi_select_np(d2, (0, 32), [(q.date_lo, q.date_hi) for q in group], (32, 24), (64, 32))
+        d2m = O.sort_pairs(d2m.view(np.uint8).reshape(-1, 8), begin_bit=32, end_bit=64)
+        j1 = O.join_tuples(d1m.view(np.uint8).reshape(-1, 8), 8, d2m, 32, 16)
+        keys = O.project(j1, [32, 8, 8, 32], [32, 8], [3, 1])
+        keys = O.sort_pairs(keys, begin_bit=0, end_bit=40)
+        if group and group[0].list_size:
+            folded = np.concatenate([(lists[q.qid].astype(np.uint64) << np.uint64(8)) | np.uint64(i)
+                                     for i, q in enumerate(group)])
+            folded = O.sort_pairs(folded, begin_bit=0, end_bit=40)
+            keys = O.set_intersection(keys.view(np.uint64).ravel(), folded).view(np.uint8).reshape(-1, 8)
+        j2 = O.join_tuples(keys, 8, fs, 64, 16)
+        limbs = j2.view(np.uint64)
+        gkey = limbs[:, 1]                              # (pk2 << 8 | q): bits 64..103
+        amt = limbs[:, 0].astype(np.int64)
+        k, sums = O.reduce_sum_i64(gkey, amt)
+        _, counts = O.reduce_count(gkey)
+        for i, q in enumerate(group):
+            sel = (k & np.uint64(0xFF)) == np.uint64(i)
+            ek, es, ec = serving_query_oracle(d1, d2, fs, q.segment, q.date_lo, q.date_hi, lists.get(q.qid))
+            assert np.array_equal((k[sel] >> np.uint64(8)).astype(np.uint32), ek), q
+            assert np.array_equal(sums[sel], es) and np.array_equal(counts[sel].astype(np.uint32), ec), q

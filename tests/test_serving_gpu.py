@@ -1,6 +1,7 @@
-"""The serving loop on the GPU: every query's result is the same served in the mix (several
-in flight on different streams) as run alone, and matches the oracle; a small memory budget
-limits how many run at once without changing any result."""
+"""The serving loop on the GPU: every query's result is the same served in the mix (packed
+into batched rounds with other queries, rounds overlapping on two streams) as run alone,
+and matches the oracle; a small memory budget limits how many run at once without changing
+any result."""
 import numpy as np
 import pytest
 
@@ -23,16 +24,31 @@ def _requests(res, n, seed):
     return S.gen_requests(n, rate=1e6, seed=seed, n2=res.n2)   # all arrive within microseconds
 
 
+def test_round_equals_alone(resident):
+    """One batched round of 40 mixed queries (with and without key lists, every segment)
+    gives each query exactly its plain result."""
+    reqs = _requests(resident, 40, seed=23)
+    assert any(q.list_size for q in reqs) and any(not q.list_size for q in reqs)
+    outs = S.run_round_host(resident, reqs, "cuda")
+    for q, got in zip(reqs, outs):
+        alone = S.run_alone(resident, q)
+        assert np.array_equal(got[0], alone[0].numpy().view(np.uint32)), q
+        assert np.array_equal(got[1], alone[1].numpy()), q
+        assert np.array_equal(got[2], alone[2].numpy().view(np.uint32)), q
+
+
 def test_served_results_equal_alone_and_oracle(resident):
     reqs = _requests(resident, 16, seed=21)
-    srv = S.Server(resident, slots=4)
+    srv = S.Server(resident, slots=2)
     sch = srv.serve(reqs, keep_results=True)
     assert sch.peak_queries > 1                          # they really overlapped
+    assert max(srv.rounds) > 1                           # and were packed into rounds
     d1, d2, f = to_np(resident.d1), to_np(resident.d2), to_np(resident.f_sorted)
     for i, q in enumerate(reqs):
         alone = S.run_alone(resident, q)
-        for a, b in zip(q.result, alone):
-            assert np.array_equal(a.numpy(), b.numpy()), q
+        assert np.array_equal(q.result[0], alone[0].numpy().view(np.uint32)), q
+        assert np.array_equal(q.result[1], alone[1].numpy()), q
+        assert np.array_equal(q.result[2], alone[2].numpy().view(np.uint32)), q
         if i < 4:
             lst = S.query_list(q, resident.n2, "cuda")
             lst = None if lst is None else to_np(lst).view(np.uint32)
@@ -47,10 +63,20 @@ def test_served_results_equal_alone_and_oracle(resident):
 def test_small_budget_limits_concurrency(resident):
     reqs = _requests(resident, 10, seed=22)
     budget = 2 * max(q.est_bytes for q in reqs)
-    sch = S.Server(resident, slots=8, budget_bytes=budget).serve(reqs, keep_results=True)
-    assert sch.peak_queries <= 8
+    sch = S.Server(resident, slots=2, budget_bytes=budget).serve(reqs, keep_results=True)
     assert sch.peak_bytes <= budget
     for q in reqs[:3]:
         alone = S.run_alone(resident, q)
-        for a, b in zip(q.result, alone):
-            assert np.array_equal(a.numpy(), b.numpy())
+        assert np.array_equal(q.result[0], alone[0].numpy().view(np.uint32))
+        assert np.array_equal(q.result[1], alone[1].numpy())
+        assert np.array_equal(q.result[2], alone[2].numpy().view(np.uint32))
+
+
+def test_plain_server_is_one_query_at_a_time(resident):
+    reqs = _requests(resident, 6, seed=24)
+    srv = S.Server(resident, slots=1, plain=True)
+    sch = srv.serve(reqs, keep_results=True)
+    assert sch.peak_queries == 1 and max(srv.rounds) == 1
+    q = reqs[0]
+    alone = S.run_alone(resident, q)
+    assert all(np.array_equal(a.numpy(), b.numpy()) for a, b in zip(q.result, alone))

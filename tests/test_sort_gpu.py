@@ -130,3 +130,42 @@ def test_reference_compatible_entries(cuda):
     torch.cuda.synchronize()
     assert R.LIB.rfx_b40c_sort_key(C.c_void_p(dk.data_ptr()), n, 37) == R.OK
     assert np.array_equal(to_np(dk), O.sort_pairs(k64, begin_bit=0, end_bit=37))
+
+
+# Tile sizes of the two pass kernels: the pipelined onesweep pass (3072 / 6144 / 8192 keys
+# of 16 / 8 / 4 bytes) and the per-tile pass (3072 / 4096 / 4096); sizes around both,
+# and sizes with many tiles per block (a persistent grid of one block per SM).
+ONESWEEP_SIZES = {16: [3071, 3072, 3073, 9217, 2_000_003], 8: [6143, 6144, 6145, 18_433, 3_000_001],
+                  4: [8191, 8192, 8193, 24_577, 4_000_037]}
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+@pytest.mark.parametrize("kb", [4, 8, 16])
+def test_sort_pass_variants_match_oracle(cuda, kb, variant):
+    """Both pass kernels (forced through the tuner's pin) give the oracle's stable order,
+    on whole keys and on a bit range that leaves payload bits outside the key."""
+    try:
+        R.tune_force(R.TUNE_SORT_PASS, variant)
+        for n in ONESWEEP_SIZES[kb]:
+            keys = _keys(n, kb, seed=n * 3 + kb)
+            for begin, end in ((0, kb * 8), (kb * 4, kb * 8 - 3)):
+                d = _dev(keys, cuda)
+                R.sort_pairs(d, begin_bit=begin, end_bit=end)
+                assert np.array_equal(to_np(d), O.sort_pairs(keys, begin_bit=begin, end_bit=end, threads=8)), (n, begin)
+        assert R.device_status() == R.OK
+    finally:
+        R.tune_force(R.TUNE_SORT_PASS, -1)
+
+
+def test_sort_unaligned_slice_uses_per_tile_pass(cuda):
+    """A key array that starts 8 bytes into an allocation (not 16-byte aligned) is sorted by
+    the per-tile pass with the same result."""
+    import torch
+    n = 100_001
+    keys = _keys(n + 1, 8, seed=77)
+    d = _dev(keys, cuda)
+    sub = d[1:]
+    assert sub.data_ptr() % 16 == 8
+    R.sort_pairs(sub, begin_bit=0, end_bit=64)
+    assert np.array_equal(to_np(sub), O.sort_pairs(keys[1:], begin_bit=0, end_bit=64))
+    assert torch.equal(d[0], _dev(keys[0], cuda))

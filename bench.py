@@ -54,6 +54,7 @@ def parse():
                                                                                 "sort_large", "setops", "pipelines",
                                                                                 "strings_f64"]))
     ap.add_argument("--reps", type=int, default=5, help="timed calls per operator with --only")
+    ap.add_argument("--sort-rows", type=int, default=60_000_000, help="rows of the large sorts (sort_large group)")
     ap.add_argument("--section", default=None, choices=["strings_f64", "batched", "serving"],
                     help="run one secondary benchmark alone and print its JSON (used by the main run, "
                          "which gives each secondary benchmark a fresh process and allocator)")
@@ -458,19 +459,34 @@ def _op_sort_c0(ctx, peak, reps):
             "sort_tuples_1M_8B_on_key": _sort_line(r, 8, 32, 64, reps, peak, note="R rows (key, payload); fits L2")}
 
 
+SORT_ROWS = 60_000_000   # rows of the large sorts (--sort-rows: smaller for profiling)
+
+
 def _op_sort_large(ctx, peak, reps):
     import torch
 
+    from redfox_b200 import plans as PL
     from redfox_b200 import rfx as R
-    _, _, f, _, _ = ctx.c2()
-    out = {"sort_tuples_60M_16B_on_fk": _sort_line(f, 16, 64, 96, 3, peak, flags=R.SORT_SKIP_TRIVIAL, passes=3,
-                                                   note="fk < 2^24: the top digit is constant and skipped")}
-    n = 60_000_000
+    n = SORT_ROWS
+    tag = "%dM" % (n // 1_000_000) if n % 1_000_000 == 0 else str(n)
+    # the three-relation workload's F (fk uniform over D2's keys, amount), the same generator
+    f = R.gen_uniform_rows(n, [32, 64], PL.C2_SEED + 2, [0, 100], [PL.C2_D2_ROWS, 10_000_000], device=ctx.dev)
+    out = {"sort_tuples_%s_16B_on_fk" % tag: _sort_line(f, 16, 64, 96, 3, peak, flags=R.SORT_SKIP_TRIVIAL, passes=3,
+                                                        note="fk < 2^24: the top digit is constant and skipped")}
+    R.tune_force(R.TUNE_SORT_PASS, 1)
+    try:
+        out["sort_tuples_%s_16B_on_fk_onesweep_pass" % tag] = _sort_line(f, 16, 64, 96, 3, peak,
+                                                                         flags=R.SORT_SKIP_TRIVIAL, passes=3,
+                                                                         note="the pipelined onesweep pass")
+    finally:
+        R.tune_force(R.TUNE_SORT_PASS, -1)
+    del f
     keys = R.gen_uniform_rows(n, [32], 0x5EED0101, [0], [1 << 32], device=ctx.dev)
-    out["sort_keys_60M_u32"] = _sort_line(keys.view(torch.uint8).view(n, 4), 4, 0, 32, 3, peak,
-                                          note="uniform 32-bit keys, 4 passes")
+    out["sort_keys_%s_u32" % tag] = _sort_line(keys.view(torch.uint8).view(n, 4), 4, 0, 32, 3, peak,
+                                               note="uniform 32-bit keys, 4 passes")
+    del keys
     rows8 = R.gen_uniform_rows(n, [32, 32], 0x5EED0102, [0, 0], [1 << 32, 1 << 32], device=ctx.dev)
-    out["sort_tuples_60M_8B_on_key"] = _sort_line(rows8, 8, 32, 64, 3, peak, note="Tuple<32,32> rows on the key")
+    out["sort_tuples_%s_8B_on_key" % tag] = _sort_line(rows8, 8, 32, 64, 3, peak, note="Tuple<32,32> rows on the key")
     return out
 
 
@@ -488,6 +504,14 @@ def _op_join(ctx, peak, reps):
     jout = torch.empty((total, 16), dtype=torch.uint8, device=ctx.dev)
     ms = _time_ms(lambda: tj(jout, total, rs, 32, ss, 64), reps)
     ops["join_fused_1Mx4M"] = _op_line(total, total * 16 + nl * 8 + nr * 16 + nl * 16, ms, peak, inputs=nl + nr)
+    # the same with the emit that gathers rows per output (the tuner's other variant)
+    R.tune_force(R.TUNE_JOIN_EMIT, 1)
+    try:
+        ms = _time_ms(lambda: tj(jout, total, rs, 32, ss, 64), reps)
+    finally:
+        R.tune_force(R.TUNE_JOIN_EMIT, -1)
+    ops["join_fused_1Mx4M_gather_emit"] = _op_line(total, total * 16 + nl * 8 + nr * 16 + nl * 16, ms, peak,
+                                                   inputs=nl + nr)
     # find_bounds alone on the split u32 keys
     lk = ((rs.view(torch.int64).view(-1) >> 32) & 0xFFFFFFFF).to(torch.int32)
     rk = (ss.view(torch.int64).view(-1, 2)[:, 1] & 0xFFFFFFFF).to(torch.int32)
@@ -1022,6 +1046,8 @@ def main_only(args):
 
     from redfox_b200 import rfx as R
     from redfox_b200 import workloads as WL
+    global SORT_ROWS
+    SORT_ROWS = args.sort_rows
     dev = torch.device("cuda:0")
     peak = measured_peak_hbm()[0]
     only = [x for x in args.only.split(",") if x]

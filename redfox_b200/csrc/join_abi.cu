@@ -4,6 +4,7 @@
 
 #include "host_common.h"
 #include "join_kernels.cuh"
+#include "tune.h"
 
 namespace rfx {
 namespace {
@@ -16,6 +17,8 @@ struct FbLayout {
   size_t clear;
   uint64_t* lb64;
   uint64_t* off64;
+  uint64_t* tile_owner;   // fused join: first owner of each output tile (nl + 2 tiles)
+  uint64_t n_owner;
   size_t total;
 };
 
@@ -28,6 +31,8 @@ FbLayout fb_layout(void* ws, uint64_t nl, bool with_offsets) {
   c.used = L.clear;
   L.lb64 = with_offsets ? c.take<uint64_t>(nl + 1) : nullptr;
   L.off64 = with_offsets ? c.take<uint64_t>(nl + 1) : nullptr;
+  L.n_owner = with_offsets ? nl + 2 : 0;
+  L.tile_owner = with_offsets ? c.take<uint64_t>(nl + 2) : nullptr;
   L.total = align_up(c.used, 256);
   return L;
 }
@@ -104,14 +109,27 @@ JaLayout ja_layout(void* ws, uint64_t nr, uint32_t kb) {
   return L;
 }
 
+// Emit variants: 0 = operands of each tile staged in shared memory by bulk copies,
+// 1 = rows gathered from global memory per output.
 template <int LE, int RE, int OE>
 rfx_status launch_tj(TupleJoinArgs& a, cudaStream_t s) {
-  auto k = tuple_join_kernel<LE, RE, OE>;
   const uint64_t tiles = (a.cap + kExpTile - 1) / kExpTile;
-  const int grid = persistent_grid((const void*)k, kJoinThreads, 0, tiles ? tiles : 1);
-  k<<<grid, kJoinThreads, 0, s>>>(a);
-  RFX_CUDA_TRY(cudaGetLastError());
-  return RFX_OK;
+  auto run = [&](int v) -> rfx_status {
+    if (v == 0) {
+      auto k = tuple_join_staged_kernel<LE, RE, OE>;
+      RFX_CUDA_TRY(allow_smem((const void*)k, JsLayout::BYTES));
+      const int grid = persistent_grid((const void*)k, kJoinThreads, JsLayout::BYTES, tiles ? tiles : 1);
+      k<<<grid, kJoinThreads, JsLayout::BYTES, s>>>(a);
+    } else {
+      auto k = tuple_join_kernel<LE, RE, OE>;
+      const int grid = persistent_grid((const void*)k, kJoinThreads, 0, tiles ? tiles : 1);
+      k<<<grid, kJoinThreads, 0, s>>>(a);
+    }
+    RFX_CUDA_TRY(cudaGetLastError());
+    return RFX_OK;
+  };
+  // the emit writes only `out`, so candidates can be timed on the caller's call
+  return run(tune_pick(TUNE_JOIN_EMIT, ((uint64_t)LE << 16) | ((uint64_t)RE << 8) | OE, a.cap, 2, run, s));
 }
 
 template <int LE, int RE>
@@ -256,6 +274,8 @@ extern "C" rfx_status rfx_join_tuples(void* out, uint32_t out_bytes, uint64_t ca
   a.rshift = right_value_bits;
   a.lb64 = L.lb64;
   a.off64 = L.off64;
+  a.tile_owner = L.tile_owner;
+  a.n_owner = L.n_owner;
   a.d_total = d_count;
   a.status = L.status;
   a.tile_counter = L.counter;
@@ -272,6 +292,9 @@ extern "C" rfx_status rfx_join_tuples(void* out, uint32_t out_bytes, uint64_t ca
   j.off64 = L.off64;
   j.out = static_cast<uint8_t*>(out);
   j.cap = capacity;
+  j.tile_owner = L.tile_owner;
+  j.n_owner = L.n_owner;
+  j.err = err;
   return dispatch_tj(left_bytes, right_bytes, out_bytes, j, s);
 }
 
@@ -390,5 +413,8 @@ extern "C" rfx_status rfx_join_tuples_emit(void* out, uint32_t out_bytes, uint64
   j.off64 = L.off64;
   j.out = static_cast<uint8_t*>(out);
   j.cap = capacity;
+  j.tile_owner = L.tile_owner;
+  j.n_owner = L.n_owner;
+  j.err = device_error_word();
   return dispatch_tj(left_bytes, right_bytes, out_bytes, j, as_stream(stream));
 }

@@ -13,6 +13,7 @@
 
 #include "search.cuh"
 #include "sort_kernels.cuh"
+#include "tile_ring.cuh"
 
 namespace rfx {
 
@@ -32,6 +33,8 @@ struct FindBoundsArgs {
   int32_t* scan32;
   uint64_t* lb64;            // workspace outputs for the fused join (may be null)
   uint64_t* off64;           // exclusive offsets, off64[nl] = total
+  uint64_t* tile_owner;      // fused join: per output tile of kExpTile rows, the left row
+  uint64_t n_owner;          // that owns its first output (tiles >= n_owner are not recorded)
   uint64_t* d_total;
   uint64_t* status;
   uint32_t* tile_counter;
@@ -133,13 +136,18 @@ __global__ void __launch_bounds__(kJoinThreads) find_bounds_kernel(const FindBou
     uint64_t tsum = 0;
     u128 prevk = 0;
     uint64_t plo = 0, phi = 0;
+    // the thread's keys first, all loads in flight together (the searches below branch on
+    // them, which would otherwise serialise the loads)
+    u128 keys[kFbIPT];
+#pragma unroll
+    for (int j = 0; j < kFbIPT; ++j) keys[j] = first + j < nl ? L.key(first + j) : (u128)0;
 #pragma unroll
     for (int j = 0; j < kFbIPT; ++j) {
       const uint64_t i = first + j;
       lo[j] = 0;
       cnt[j] = 0;
       if (i >= nl) continue;
-      const u128 k = L.key(i);
+      const u128 k = keys[j];
       if (j > 0 && k == prevk) {
         lo[j] = plo;
         cnt[j] = phi - plo;
@@ -195,6 +203,12 @@ __global__ void __launch_bounds__(kJoinThreads) find_bounds_kernel(const FindBou
     for (int j = 0; j < kFbIPT; ++j) {
       const uint64_t i = first + j;
       if (i >= nl) continue;
+      if (a.tile_owner && cnt[j]) {
+        // every output tile that starts inside this row's outputs [run, run + cnt) is owned
+        // by it at its first output
+        for (uint64_t b = (run + kExpTile - 1) / kExpTile; b < a.n_owner && b * kExpTile < run + cnt[j]; ++b)
+          a.tile_owner[b] = i;
+      }
       if (a.lb32) a.lb32[i] = (int32_t)lo[j];
       if (a.scan32) a.scan32[i] = (int32_t)(uint32_t)run;
       if (a.lb64) a.lb64[i] = lo[j];
@@ -393,6 +407,9 @@ struct TupleJoinArgs {
   const uint64_t* off64;   // nl + 1 entries
   uint8_t* out;
   uint64_t cap;
+  const uint64_t* tile_owner;   // from the count pass (may be null)
+  uint64_t n_owner;
+  uint32_t* err;
 };
 
 // Offsets of the left rows that cover a block's outputs, staged in shared memory.
@@ -506,6 +523,214 @@ __global__ void __launch_bounds__(kJoinThreads) tuple_join_kernel(const TupleJoi
       const uint64_t j = lbi + (k - offi);
       if (j < a.nr)  // guards a timed-out scan
         store_u128<OE>(a.out, k, (load_u128<LE>(a.left, i) << a.rv_bits) | (load_u128<RE>(a.right, j) & rmask));
+    }
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------ staged emit
+// The emit with every operand of a tile in shared memory.  Per tile of kExpTile outputs:
+// the owners of its first and last output come from the count pass (tile_owner), the
+// offsets and lower bounds of the left rows in between are staged, each output finds its
+// row by the mark + max-scan, and the tile's left rows and the window of right rows it
+// touches (rows [jlo, jhi) of the right relation: right runs of equal keys are revisited
+// by every left row with that key) are brought into shared memory by bulk copies
+// (cp.async.bulk, this GPU's memory; an mbarrier counts the bytes; a range that is not
+// 16-byte aligned or would read past the array is copied by the threads instead).  The
+// outputs are then assembled from shared memory and stored in order, so the tile's
+// global traffic is its output rows plus one pass over its input windows.
+constexpr int kJsSpan = 1024;              // left rows staged per tile
+constexpr int kJsLeftBytes = kJsSpan * 16;
+constexpr int kJsRightBytes = 16384;       // right window staged per tile
+
+struct JsLayout {
+  static constexpr size_t OFF = 0;                                        // u64[kJsSpan + 1]
+  static constexpr size_t LB = OFF + 8 * (kJsSpan + 1);                   // u64[kJsSpan]
+  static constexpr size_t OWN = LB + 8 * kJsSpan;                         // u16[kExpTile]
+  static constexpr size_t LEFT = (OWN + 2 * kExpTile + 127) / 128 * 128;  // left rows (+16 slack)
+  static constexpr size_t RIGHT = LEFT + kJsLeftBytes + 128;              // right window (+16 slack)
+  static constexpr size_t BYTES = RIGHT + kJsRightBytes + 128;
+};
+
+template <int E>
+__device__ __forceinline__ u128 smem_row(const uint8_t* p) {
+  if constexpr (E == 4) return (u128)*reinterpret_cast<const uint32_t*>(p);
+  else if constexpr (E == 8) return (u128)*reinterpret_cast<const unsigned long long*>(p);
+  else {
+    const ulonglong2 v = *reinterpret_cast<const ulonglong2*>(p);
+    return ((u128)v.y << 64) | (u128)v.x;
+  }
+}
+
+// Stages bytes [b0, b1) of `src` (an array of `limit` bytes) into `dst`: returns the first
+// byte copied (16-byte aligned) when one bulk copy was issued on `bar` (*tx += its bytes),
+// or copies with all threads when `bulk` is false.  Called by thread 0 (bulk) or by all
+// threads (plain) -- see the caller.
+__device__ __forceinline__ uint64_t js_align_lo(uint64_t b0) { return b0 & ~15ull; }
+__device__ __forceinline__ uint64_t js_align_hi(uint64_t b1) { return (b1 + 15) & ~15ull; }
+
+template <int LE, int RE, int OE>
+__global__ void __launch_bounds__(kJoinThreads) tuple_join_staged_kernel(const TupleJoinArgs a) {
+  extern __shared__ __align__(128) uint8_t js[];
+  uint64_t* s_off = reinterpret_cast<uint64_t*>(js + JsLayout::OFF);
+  uint64_t* s_lb = reinterpret_cast<uint64_t*>(js + JsLayout::LB);
+  uint16_t* s_own = reinterpret_cast<uint16_t*>(js + JsLayout::OWN);
+  uint8_t* s_left = js + JsLayout::LEFT;
+  uint8_t* s_right = js + JsLayout::RIGHT;
+  __shared__ uint64_t s_i0, s_i1, s_lbase, s_rbase;
+  __shared__ unsigned long long s_jlo, s_jhi;
+  __shared__ uint32_t s_mode;          // bit 0 left staged, 1 right staged, 2 bulk copies issued
+  __shared__ uint32_t s_wmax[kJoinThreads / 32];
+  __shared__ __align__(8) uint64_t s_bar;
+  const uint32_t t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const uint64_t total = a.off64[a.nl];
+  const uint64_t nout = total < a.cap ? total : a.cap;
+  const u128 rmask = a.rv_bits >= 128 ? ~(u128)0 : (((u128)1 << a.rv_bits) - 1);
+  const bool bulk_ok = ((reinterpret_cast<uintptr_t>(a.left) | reinterpret_cast<uintptr_t>(a.right)) & 15u) == 0;
+  if (t == 0) {
+    mbar_init(&s_bar, 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  uint32_t phase = 0;
+  for (uint64_t k0 = (uint64_t)blockIdx.x * kExpTile; k0 < nout; k0 += (uint64_t)gridDim.x * kExpTile) {
+    const uint64_t tile = k0 / kExpTile;
+    const uint64_t k1 = min(k0 + (uint64_t)kExpTile, nout);
+    // owners of the first and last output
+    const bool rec0 = a.tile_owner && tile < a.n_owner;
+    const bool rec1 = a.tile_owner && tile + 1 < a.n_owner && k1 < total;
+    if (t < 32) {
+      const uint64_t i0 = rec0 ? __ldg(a.tile_owner + tile) : owner_warp(a.off64, a.nl, k0);
+      if (t == 0) s_i0 = i0;
+    } else if (t < 64) {
+      const uint64_t i1 = rec1 ? __ldg(a.tile_owner + tile + 1) : owner_warp(a.off64, a.nl, k1 - 1);
+      if (t == 32) s_i1 = i1;
+    }
+    if (t == 64) {
+      s_jlo = ~0ull;
+      s_jhi = 0;
+    }
+    __syncthreads();
+    const uint64_t i0 = s_i0, span = s_i1 - i0 + 1;
+    if (span > (uint64_t)kJsSpan) {
+      // more left rows than the stage holds (rows with very few outputs): search per output
+#pragma unroll 2
+      for (int v = 0; v < kExpVT; ++v) {
+        const uint64_t k = k0 + (uint64_t)v * kJoinThreads + t;
+        if (k >= k1) break;
+        const uint64_t i = owner_global(a.off64, a.nl, k);
+        const uint64_t j = __ldg(a.lb64 + i) + (k - __ldg(a.off64 + i));
+        if (j < a.nr)
+          store_u128<OE>(a.out, k, (load_u128<LE>(a.left, i) << a.rv_bits) | (load_u128<RE>(a.right, j) & rmask));
+      }
+      __syncthreads();
+      continue;
+    }
+    for (uint32_t x = t; x <= (uint32_t)span; x += kJoinThreads) s_off[x] = __ldg(a.off64 + i0 + x);
+    for (uint32_t x = t; x < (uint32_t)span; x += kJoinThreads) s_lb[x] = __ldg(a.lb64 + i0 + x);
+    for (uint32_t x = t; x < (uint32_t)kExpTile; x += kJoinThreads) s_own[x] = 0;
+    __syncthreads();
+    // marks (each row's first output in the tile) and the right rows the tile touches
+    {
+      unsigned long long jlo = ~0ull, jhi = 0;
+      for (uint32_t x = t; x < (uint32_t)span; x += kJoinThreads) {
+        const uint64_t o0 = s_off[x], o1 = s_off[x + 1];
+        const uint64_t a0 = o0 > k0 ? o0 : k0, a1 = o1 < k1 ? o1 : k1;
+        if (a0 >= a1) continue;
+        if (x > 0) s_own[a0 - k0] = (uint16_t)x;
+        jlo = min(jlo, (unsigned long long)(s_lb[x] + (a0 - o0)));
+        jhi = max(jhi, (unsigned long long)(s_lb[x] + (a1 - o0)));
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        jlo = min(jlo, __shfl_xor_sync(0xffffffffu, jlo, o));
+        jhi = max(jhi, __shfl_xor_sync(0xffffffffu, jhi, o));
+      }
+      if (lane == 0) {
+        atomicMin(&s_jlo, jlo);
+        atomicMax(&s_jhi, jhi);
+      }
+    }
+    __syncthreads();
+    // stage the left rows [i0, i0 + span) and the right window [jlo, jhi)
+    if (t == 0) {
+      uint32_t mode = 0, tx = 0;
+      const uint64_t lb0 = js_align_lo(i0 * LE), lb1 = js_align_hi((i0 + span) * LE);
+      const uint64_t jlo = s_jlo, jhi = s_jhi > a.nr ? a.nr : s_jhi;
+      const uint64_t rb0 = js_align_lo(jlo * RE), rb1 = js_align_hi(jhi * RE);
+      if (lb1 - lb0 <= (uint64_t)kJsLeftBytes + 16) mode |= 1;
+      if (jlo < jhi && rb1 - rb0 <= (uint64_t)kJsRightBytes + 16) mode |= 2;
+      s_lbase = lb0;
+      s_rbase = rb0;
+      const bool lbulk = (mode & 1) && bulk_ok && lb1 <= a.nl * LE;
+      const bool rbulk = (mode & 2) && bulk_ok && rb1 <= a.nr * RE;
+      if (lbulk || rbulk) {
+        fence_proxy_async_smem();
+        tx = (lbulk ? (uint32_t)(lb1 - lb0) : 0u) + (rbulk ? (uint32_t)(rb1 - rb0) : 0u);
+        mbar_arrive_tx(&s_bar, tx);
+        if (lbulk) bulk_copy_g2s(s_left, a.left + lb0, (uint32_t)(lb1 - lb0), &s_bar);
+        if (rbulk) bulk_copy_g2s(s_right, a.right + rb0, (uint32_t)(rb1 - rb0), &s_bar);
+        mode |= 4 | (lbulk ? 8u : 0u) | (rbulk ? 16u : 0u);
+      }
+      s_mode = mode;
+    }
+    // every output's row by an inclusive max-scan of the marks (row 0 owns the start)
+    {
+      constexpr uint32_t PER = kExpTile / kJoinThreads;
+      __syncthreads();
+      uint32_t m = 0, v[PER];
+#pragma unroll
+      for (uint32_t j = 0; j < PER; ++j) {
+        m = max(m, (uint32_t)s_own[t * PER + j]);
+        v[j] = m;
+      }
+      uint32_t inc = m;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= (uint32_t)o) inc = max(inc, y);
+      }
+      if (lane == 31) s_wmax[warp] = inc;
+      uint32_t ex = __shfl_up_sync(0xffffffffu, inc, 1);
+      if (lane == 0) ex = 0;
+      __syncthreads();
+      for (uint32_t w = 0; w < warp; ++w) ex = max(ex, s_wmax[w]);
+#pragma unroll
+      for (uint32_t j = 0; j < PER; ++j) s_own[t * PER + j] = (uint16_t)max(v[j], ex);
+    }
+    const uint32_t mode = s_mode;
+    // the parts the bulk copies did not take: plain loads by all threads (4-byte words;
+    // row sizes and the window bases are multiples of 4, the aligned ends stay inside
+    // the arrays)
+    if ((mode & 1) && !(mode & 8)) {
+      const uint64_t b0 = i0 * LE, b1 = (i0 + span) * LE;
+      for (uint64_t b = b0 + 4ull * t; b < b1; b += 4ull * kJoinThreads)
+        *reinterpret_cast<uint32_t*>(s_left + (b - s_lbase)) = *reinterpret_cast<const uint32_t*>(a.left + b);
+    }
+    if ((mode & 2) && !(mode & 16)) {
+      const uint64_t jhi = s_jhi > a.nr ? a.nr : s_jhi;
+      const uint64_t b0 = (uint64_t)s_jlo * RE, b1 = jhi * RE;
+      for (uint64_t b = b0 + 4ull * t; b < b1; b += 4ull * kJoinThreads)
+        *reinterpret_cast<uint32_t*>(s_right + (b - s_rbase)) = *reinterpret_cast<const uint32_t*>(a.right + b);
+    }
+    if (mode & 4) {
+      if (!mbar_wait(&s_bar, phase)) raise_error(a.err, kErrTimeout);
+      phase ^= 1u;
+    }
+    __syncthreads();
+    // outputs in order: consecutive threads write consecutive rows
+#pragma unroll
+    for (int v = 0; v < kExpVT; ++v) {
+      const uint64_t k = k0 + (uint64_t)v * kJoinThreads + t;
+      if (k >= k1) break;
+      const uint32_t x = s_own[k - k0];
+      const uint64_t i = i0 + x;
+      const uint64_t j = s_lb[x] + (k - s_off[x]);
+      if (j >= a.nr) continue;   // guards a timed-out scan
+      const u128 L = (mode & 1) ? smem_row<LE>(s_left + (i * LE - s_lbase)) : load_u128<LE>(a.left, i);
+      const bool rin = (mode & 2) && (uint64_t)j >= (uint64_t)s_jlo && j < (uint64_t)s_jhi;
+      const u128 Rv = rin ? smem_row<RE>(s_right + (j * RE - s_rbase)) : load_u128<RE>(a.right, j);
+      store_u128<OE>(a.out, k, (L << a.rv_bits) | (Rv & rmask));
     }
     __syncthreads();
   }

@@ -45,6 +45,8 @@ rfx_status dispatch(uint32_t kb, SortPlan& s, uint32_t vb) {
 struct SortLayout {
   uint8_t* alt_keys;
   uint8_t* alt_vals;
+  uint8_t* alt2_keys;   // with 3 or more digit passes: lets an odd number of passes end in
+  uint8_t* alt2_vals;   // the caller's buffers instead of being copied back
   uint32_t* ctrl;  // ghist | trivial | done | counters
   uint32_t* status;
   size_t ctrl_bytes;  // bytes to clear per chunk (ctrl + status)
@@ -61,6 +63,9 @@ SortLayout layout(void* ws, uint64_t n, uint32_t kb, uint32_t vb, uint32_t begin
   Carver c(ws);
   L.alt_keys = c.take<uint8_t>(n * kb);
   L.alt_vals = c.take<uint8_t>(vb ? n * vb : 0);
+  const bool second = L.passes >= 3;
+  L.alt2_keys = second ? c.take<uint8_t>(n * kb) : nullptr;
+  L.alt2_vals = second && vb ? c.take<uint8_t>(n * vb) : nullptr;
   c.used = align_up(c.used, 256);
   const size_t ctrl_start = c.used;
   L.ctrl = c.take<uint32_t>(kMaxSortPasses * kRadix + 2 * kMaxSortPasses + 1);
@@ -104,6 +109,8 @@ rfx_status sort_pairs_impl(void* keys, void* vals, uint64_t n, uint32_t kb, uint
     s.vals = cur_v;
     s.alt_keys = oth_k;
     s.alt_vals = oth_v;
+    s.alt2_keys = L.alt2_keys;
+    s.alt2_vals = L.alt2_vals;
     s.n = n;
     s.begin_bit = lo;
     s.end_bit = hi;

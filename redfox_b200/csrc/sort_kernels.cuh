@@ -210,31 +210,88 @@ sort_histogram_kernel(const uint8_t* __restrict__ keys, uint64_t n, uint32_t beg
   }
 }
 
-// ------------------------------------------------------------------ onesweep pass
+// ------------------------------------------------------------------ per-tile pass
 // Two blocks per SM: the per-item keys and ranks must fit 128 registers, so digits and
 // tile positions are recomputed where needed instead of being kept live.
+//
+// A block claims its next tile one ahead and, where the keys are 16-byte aligned and two
+// tile buffers fit, copies that tile's keys into shared memory with cp.async while it
+// ranks, resolves and writes the current one, so the load of a tile never waits on the
+// memory system.  Per tile: rank in registers, count digits and publish the tile's
+// aggregate, scatter the keys into the tile's own buffer in digit order, resolve the
+// global digit offsets by decoupled look-back (after the scatter, so the predecessors
+// have had that long to publish), then write the buffer out in digit runs.
+template <int K, int V>
+struct SortBuffers {
+  static constexpr int EB = (int)sizeof(Elem<K>) > (V > 0 ? (int)sizeof(Elem<V>) : 0) ? (int)sizeof(Elem<K>)
+                                                                                        : (int)sizeof(Elem<V>);
+  static constexpr int TILE = SortTuning<K, V>::TILE;
+  // prefetch when the raw keys are whole 16-byte chunks and two buffers fit two blocks
+  static constexpr bool PF = K >= 4 && 2 * TILE * EB <= 100 * 1024;
+  static constexpr size_t SMEM = (size_t)(PF ? 2 : 1) * TILE * EB;
+};
+
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, uint32_t src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
+               "l"(src), "r"(src_bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// The raw keys of tile `tile` (tcount keys) into `dst`, in 16-byte chunks (the last one
+// zero-filled past the array).
+template <int K>
+__device__ __forceinline__ void sort_prefetch(uint8_t* dst, const uint8_t* keys, uint64_t tile, uint32_t tile_keys,
+                                              uint64_t n) {
+  const uint64_t b0 = tile * (uint64_t)tile_keys * K;
+  const uint64_t bend = n * K;
+  const uint64_t b1 = b0 + (uint64_t)tile_keys * K < bend ? b0 + (uint64_t)tile_keys * K : bend;
+  const uint32_t chunks = (uint32_t)((b1 - b0 + 15) / 16);
+  for (uint32_t c = threadIdx.x; c < chunks; c += kSortThreads) {
+    const uint64_t src = b0 + 16ull * c;
+    const uint32_t bytes = (uint32_t)(bend - src < 16 ? bend - src : 16);
+    cp_async16(dst + 16u * c, keys + src, bytes);
+  }
+}
+
 template <int K, int V>
 __global__ void __launch_bounds__(kSortThreads, 2)
 sort_pass_kernel(const SortPassArgs a) {
   using T = SortTuning<K, V>;
+  using SB = SortBuffers<K, V>;
   constexpr int IPT = T::IPT;
   constexpr int TILE = T::TILE;
-  extern __shared__ __align__(16) uint8_t sbuf[];              // TILE * SBYTES scatter buffer
+  extern __shared__ __align__(16) uint8_t sbuf[];              // 1 or 2 buffers of TILE * EB
   __shared__ uint32_t whist[kSortWarps][kRadix];               // per-warp digit counts
   __shared__ uint32_t s_local[kRadix];                         // tile-local digit start
   __shared__ uint32_t s_global[kRadix];                        // global base of the digit run
   __shared__ uint8_t s_dig[TILE];                              // digit of each sorted slot
   __shared__ uint32_t s_scan[kSortWarps];
-  __shared__ uint32_t s_tile;
+  __shared__ uint32_t s_tile[2];
   const uint32_t t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const uint64_t num_tiles = (a.n + TILE - 1) / TILE;
+  const bool pf = SB::PF && (reinterpret_cast<uintptr_t>(a.keys_in) & 15u) == 0;
+  if (t == 0) s_tile[0] = atomicAdd(a.tile_counter, 1u);
+  __syncthreads();
+  if (pf && s_tile[0] < num_tiles) sort_prefetch<K>(sbuf, a.keys_in, s_tile[0], TILE, a.n);
+  cp_async_commit();
 
-  while (true) {
-    if (t == 0) s_tile = atomicAdd(a.tile_counter, 1u);
+  for (uint32_t it = 0;; ++it) {
+    const uint64_t tile = s_tile[it & 1];
+    uint8_t* stage = sbuf + (pf ? (size_t)(it & 1) * TILE * SB::EB : 0);
+    if (t == 0) s_tile[(it + 1) & 1] = atomicAdd(a.tile_counter, 1u);   // the next tile, one ahead
     for (uint32_t k = t; k < kSortWarps * kRadix; k += kSortThreads) (&whist[0][0])[k] = 0;
     __syncthreads();
-    const uint64_t tile = s_tile;
-    if (tile >= num_tiles) break;
+    if (tile >= num_tiles) break;   // the tile claimed next is larger still: no copy in flight
+    const uint64_t next = s_tile[(it + 1) & 1];
+    if (pf) {
+      if (next < num_tiles) sort_prefetch<K>(sbuf + (size_t)((it + 1) & 1) * TILE * SB::EB, a.keys_in, next, TILE, a.n);
+      cp_async_commit();
+      cp_async_wait<1>();          // this tile's copy (the next one may stay in flight)
+      __syncthreads();
+    }
     const uint64_t tbase = tile * TILE;
     const uint32_t tcount = (uint32_t)min((uint64_t)TILE, a.n - tbase);
     // warp w owns items [w*32*IPT, (w+1)*32*IPT) of the tile, item j of lane l at j*32+l
@@ -244,7 +301,7 @@ sort_pass_kernel(const SortPassArgs a) {
 #pragma unroll
     for (int j = 0; j < IPT; ++j) {
       const uint32_t li = wbase + j * 32 + lane;
-      if (li < tcount) key[j] = load_elem<K>(a.keys_in, tbase + li);
+      if (li < tcount) key[j] = pf ? load_elem<K>(stage, li) : load_elem<K>(a.keys_in, tbase + li);
     }
 #pragma unroll
     for (int j = 0; j < IPT; ++j) {
@@ -268,7 +325,7 @@ sort_pass_kernel(const SortPassArgs a) {
       __syncwarp();
     }
     __syncthreads();
-    // per digit: exclusive over warps, tile count, tile-local start, look-back
+    // per digit: exclusive over warps, the tile's count (published at once), tile-local start
     uint32_t count = 0;
     if (t < kRadix) {
 #pragma unroll
@@ -277,6 +334,7 @@ sort_pass_kernel(const SortPassArgs a) {
         whist[w][t] = count;
         count += c;
       }
+      st_relaxed_u32(a.status + tile * kRadix + t, (tile == 0 ? kSFlagInc : kSFlagAgg) | count);
     }
     // block exclusive scan of count over the 256 digits
     uint32_t incl = count;
@@ -291,16 +349,23 @@ sort_pass_kernel(const SortPassArgs a) {
       uint32_t wpre = 0;
       for (uint32_t w = 0; w < warp; ++w) wpre += s_scan[w];
       s_local[t] = wpre + incl - count;
-      // decoupled look-back for this digit, kSortLookWindow predecessors per round trip
-      // (independent loads, all in flight at once): with hundreds of tiles in flight the
-      // nearest inclusive predecessor is tens of tiles back, and a one-by-one walk would
-      // pay a round trip per tile
-      uint32_t* st = a.status + tile * kRadix + t;
+    }
+    __syncthreads();
+    // keys: scatter into tile order in shared memory (every thread's keys are in registers)
+    Elem<K>* skeys = reinterpret_cast<Elem<K>*>(stage);
+#pragma unroll
+    for (int j = 0; j < IPT; ++j) {
+      const uint32_t li = wbase + j * 32 + lane;
+      if (li < tcount) {
+        const uint32_t d = elem_bits<K>(key[j], a.shift) & a.mask;
+        skeys[s_local[d] + whist[warp][d] + rank[j]] = key[j];
+      }
+    }
+    // decoupled look-back for digit t, kSortLookWindow predecessors per round trip
+    // (independent loads, all in flight at once)
+    if (t < kRadix) {
       uint32_t prefix = 0;
-      if (tile == 0) {
-        st_relaxed_u32(st, kSFlagInc | count);
-      } else {
-        st_relaxed_u32(st, kSFlagAgg | count);
+      if (tile > 0) {
         int64_t base = (int64_t)tile - 1;
         uint32_t spins = 0;
         while (base >= 0) {
@@ -335,20 +400,9 @@ sort_pass_kernel(const SortPassArgs a) {
           if (r_inc < kSortLookWindow) break;
           base -= kSortLookWindow;
         }
-        st_relaxed_u32(st, kSFlagInc | ((prefix + count) & kSValMask));
+        st_relaxed_u32(a.status + tile * kRadix + t, kSFlagInc | ((prefix + count) & kSValMask));
       }
       s_global[t] = a.gexcl[t] + prefix;
-    }
-    __syncthreads();
-    // keys: scatter into tile order in shared memory, then out in digit runs
-    Elem<K>* skeys = reinterpret_cast<Elem<K>*>(sbuf);
-#pragma unroll
-    for (int j = 0; j < IPT; ++j) {
-      const uint32_t li = wbase + j * 32 + lane;
-      if (li < tcount) {
-        const uint32_t d = elem_bits<K>(key[j], a.shift) & a.mask;
-        skeys[s_local[d] + whist[warp][d] + rank[j]] = key[j];
-      }
     }
     __syncthreads();
     for (uint32_t i = t; i < tcount; i += kSortThreads) {
@@ -360,7 +414,7 @@ sort_pass_kernel(const SortPassArgs a) {
     }
     if constexpr (V > 0) {
       __syncthreads();
-      Elem<V>* svals = reinterpret_cast<Elem<V>*>(sbuf);
+      Elem<V>* svals = reinterpret_cast<Elem<V>*>(stage);
 #pragma unroll
       for (int j = 0; j < IPT; ++j) {
         const uint32_t li = wbase + j * 32 + lane;
@@ -378,6 +432,7 @@ sort_pass_kernel(const SortPassArgs a) {
     }
     __syncthreads();
   }
+  cp_async_wait<0>();
 }
 
 }  // namespace rfx

@@ -14,6 +14,8 @@ struct SortPlan {
   uint8_t* vals;
   uint8_t* alt_keys;
   uint8_t* alt_vals;
+  uint8_t* alt2_keys;   // a second pair of alternate buffers (may be null): an odd number
+  uint8_t* alt2_vals;   // of passes >= 3 then ends in keys / vals without a copy
   uint64_t n;
   uint32_t begin_bit;
   uint32_t end_bit;     // end_bit - begin_bit <= 128
@@ -32,14 +34,27 @@ struct SortPlan {
   bool in_alt;          // out: the sorted data ended in the alternate buffers
 };
 
+// Look-back status words are laid out per tile of the smallest tile any pass variant
+// uses, so every variant's tiles fit the same status area.
+template <int K, int V>
+constexpr int min_sort_tile() {
+  if constexpr (V == 0 && (K == 4 || K == 8 || K == 16)) {
+    constexpr int a = SortTuning<K, V>::TILE, b = OsTuning<K, OsIpt<K>::SMALL>::TILE;
+    constexpr int c = OsTuning<K, OsIpt<K>::DEF>::TILE, d = OsTuning<K, OsIpt<K>::ALT>::TILE;
+    constexpr int ab = a < b ? a : b, cd = c < d ? c : d;
+    return ab < cd ? ab : cd;
+  } else {
+    return SortTuning<K, V>::TILE;
+  }
+}
+
 template <int K, int V>
 uint64_t sort_tiles(uint64_t n) {
-  return (n + SortTuning<K, V>::TILE - 1) / SortTuning<K, V>::TILE;
+  return (n + min_sort_tile<K, V>() - 1) / min_sort_tile<K, V>();
 }
 
 template <int K, int V>
 rfx_status run_sort_kv(SortPlan& s) {
-  using T = SortTuning<K, V>;
   // histogram of every digit
   {
     auto hk = sort_histogram_kernel<K>;
@@ -54,12 +69,12 @@ rfx_status run_sort_kv(SortPlan& s) {
     RFX_CUDA_TRY(cudaStreamSynchronize(s.stream));
     for (uint32_t p = 0; p < s.passes; ++p) triv[p] = s.host_trivial[p];
   }
-  // Pass variants: 0 = the pipelined onesweep pass (TMA stages + look-back warp) where it
-  // applies -- keys without values in 4/8/16-byte containers on 16-byte aligned buffers --
-  // 1 = the per-tile pass (every width, values too), 2 / 3 = the onesweep pass with fewer
-  // / other numbers of items per thread.  The autotuner may pick per size class.
-  constexpr size_t ek = sizeof(Elem<K>), ev = V > 0 ? sizeof(Elem<V>) : 0;
-  const size_t tile_smem = (size_t)T::TILE * (ek > ev ? ek : ev);
+  // Pass variants: 0 = the per-tile pass (every width, values too; the next tile's keys
+  // prefetched into shared memory); 1 / 2 / 3 = the pipelined onesweep pass (TMA stages +
+  // a look-back warp, one block per SM) with its default / fewer / other items per thread,
+  // where it applies: keys without values in 4/8/16-byte containers on 16-byte aligned
+  // buffers.  The autotuner may pick per size class.
+  const size_t tile_smem = SortBuffers<K, V>::SMEM;
   RFX_CUDA_TRY(allow_smem((const void*)sort_pass_kernel<K, V>, tile_smem));
   const int tile_grid = persistent_grid((const void*)sort_pass_kernel<K, V>, kSortThreads, tile_smem,
                                         s.tiles ? s.tiles : 1);
@@ -67,11 +82,13 @@ rfx_status run_sort_kv(SortPlan& s) {
   bool os_ok = false;
   int os_grid[3] = {0, 0, 0};   // default, small, alternative tiles
   if constexpr (kOnesweep) {
-    os_ok = ((reinterpret_cast<uintptr_t>(s.keys) | reinterpret_cast<uintptr_t>(s.alt_keys)) & 15u) == 0;
+    os_ok = ((reinterpret_cast<uintptr_t>(s.keys) | reinterpret_cast<uintptr_t>(s.alt_keys) |
+              reinterpret_cast<uintptr_t>(s.alt2_keys)) & 15u) == 0;
     if (os_ok) {
       auto prep = [&](const void* k, size_t smem, int tile, int* grid) -> rfx_status {
-        RFX_CUDA_TRY(allow_smem(k, smem));
         const uint64_t ot = (s.n + tile - 1) / tile;
+        if (ot > s.tiles) return RFX_ERR_INVALID;   // the status area holds s.tiles tiles
+        RFX_CUDA_TRY(allow_smem(k, smem));
         *grid = persistent_grid(k, kOsThreads, smem, ot ? ot : 1);
         return RFX_OK;
       };
@@ -81,22 +98,34 @@ rfx_status run_sort_kv(SortPlan& s) {
       rfx_status st = prep((const void*)sort_onesweep_kernel<K, TD::IPT>, TD::SMEM, TD::TILE, &os_grid[0]);
       if (st == RFX_OK) st = prep((const void*)sort_onesweep_kernel<K, TS::IPT>, TS::SMEM, TS::TILE, &os_grid[1]);
       if (st == RFX_OK) st = prep((const void*)sort_onesweep_kernel<K, TL::IPT>, TL::SMEM, TL::TILE, &os_grid[2]);
-      if (st != RFX_OK) return st;
+      if (st == RFX_ERR_INVALID) os_ok = false;   // not expected: the per-tile pass runs instead
+      else if (st != RFX_OK) return st;
     }
   }
-  const uint8_t* kin = s.keys;
-  const uint8_t* vin = s.vals;
-  uint8_t* kout = s.alt_keys;
-  uint8_t* vout = s.alt_vals;
+  // Buffers the passes go through: b[0] = keys, pass j reads b[j] and writes b[j + 1].
+  // An even number of passes alternates keys / alt and ends in keys; an odd number >= 3
+  // goes keys -> alt -> alt2 -> keys and then alternates, so it ends in keys too; a single
+  // pass (or no second buffer) ends in alt, which the caller copies back.
+  uint32_t npass = 0;
+  for (uint32_t p = 0; p < s.passes; ++p) npass += triv[p] ? 0u : 1u;
+  uint8_t* kb[kMaxSortPasses + 1];
+  uint8_t* vb[kMaxSortPasses + 1];
+  const bool three = (npass % 2 == 1) && npass >= 3 && s.alt2_keys && (V == 0 || s.alt2_vals);
+  for (uint32_t j = 0; j <= npass; ++j) {
+    const bool at_keys = three ? (j == 0 || (j >= 3 && j % 2 == 1)) : (j % 2 == 0);
+    const bool at_alt2 = three && j == 2;
+    kb[j] = at_keys ? s.keys : at_alt2 ? s.alt2_keys : s.alt_keys;
+    vb[j] = at_keys ? s.vals : at_alt2 ? s.alt2_vals : s.alt_vals;
+  }
   s.executed = 0;
-  s.in_alt = false;
+  s.in_alt = kb[npass] != s.keys;
   for (uint32_t p = 0; p < s.passes; ++p) {
     if (triv[p]) continue;
     SortPassArgs a;
-    a.keys_in = kin;
-    a.keys_out = kout;
-    a.vals_in = vin;
-    a.vals_out = vout;
+    a.keys_in = kb[s.executed];
+    a.keys_out = kb[s.executed + 1];
+    a.vals_in = vb[s.executed];
+    a.vals_out = vb[s.executed + 1];
     a.n = s.n;
     a.shift = s.begin_bit + 8 * p;
     const uint32_t w = s.end_bit - a.shift < 8 ? s.end_bit - a.shift : 8;
@@ -118,7 +147,7 @@ rfx_status run_sort_kv(SortPlan& s) {
         using TD = OsTuning<K, OsIpt<K>::DEF>;
         using TS = OsTuning<K, OsIpt<K>::SMALL>;
         using TL = OsTuning<K, OsIpt<K>::ALT>;
-        if (os_ok && v == 0)
+        if (os_ok && v == 1)
           sort_onesweep_kernel<K, TD::IPT><<<os_grid[0], kOsThreads, TD::SMEM, s.stream>>>(a);
         else if (os_ok && v == 2)
           sort_onesweep_kernel<K, TS::IPT><<<os_grid[1], kOsThreads, TS::SMEM, s.stream>>>(a);
@@ -132,17 +161,10 @@ rfx_status run_sort_kv(SortPlan& s) {
       RFX_CUDA_TRY(cudaGetLastError());
       return RFX_OK;
     };
-    const int v = os_ok ? tune_pick(TUNE_SORT_PASS, (uint64_t)K << 8 | V, s.n, 4, launch, s.stream) : 1;
+    const int v = os_ok ? tune_pick(TUNE_SORT_PASS, (uint64_t)K << 8 | V, s.n, 4, launch, s.stream) : 0;
     rfx_status st = launch(v);
     if (st != RFX_OK) return st;
     ++s.executed;
-    s.in_alt = !s.in_alt;
-    const uint8_t* tk = kout;
-    const uint8_t* tv = vout;
-    kout = const_cast<uint8_t*>(kin);
-    vout = const_cast<uint8_t*>(vin);
-    kin = tk;
-    vin = tv;
   }
   return RFX_OK;
 }

@@ -64,6 +64,13 @@ __device__ __forceinline__ void tma_load_lines(void* dst, const CUtensorMap* map
       ::"r"(smem_u32(dst)), "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(line), "r"(smem_u32(bar))
       : "memory");
 }
+// A 1-D bulk copy of `bytes` (a multiple of 16, both addresses 16-byte aligned) from this
+// GPU's global memory into shared memory; completion counted on `bar`.  No multicast.
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+               ::"r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
 __device__ __forceinline__ void prefetch_map(const CUtensorMap* map) {
   asm volatile("prefetch.tensormap [%0];" ::"l"(reinterpret_cast<uint64_t>(map)) : "memory");
 }

@@ -22,7 +22,8 @@ enum TuneOp : uint32_t {
   TUNE_SET_FILTER = 2,    // set intersection / difference / union's B - A: 8 or 4 items per thread
   TUNE_SCAN_COMPACT = 3,  // plan-specialised select / project: items per thread
   TUNE_SCAN_AGGREGATE = 4,  // plan-specialised filter-aggregate: rows per thread per iteration
-  TUNE_SORT_PASS = 5,     // radix sort pass: onesweep (TMA stages + look-back warp; 3 tile sizes) or per tile
+  TUNE_SORT_PASS = 5,     // radix sort pass: per tile, or onesweep (TMA stages + look-back warp; 3 tile sizes)
+  TUNE_JOIN_EMIT = 6,     // fused join emit: operands staged in shared memory by bulk copies, or gathered
 };
 
 // Size class of n: floor(log2(n)) / 2 (classes of 4x).

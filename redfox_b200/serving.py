@@ -269,28 +269,33 @@ def run_round(res, queries, lists=None, stream=None):
     return gk, gs, gc
 
 
-def split_round(gk, gs, gc, nq):
-    """Host copies of a round's groups -> per query (keys u32, sums int64, counts u32) in
-    key order (the round's groups are ordered by (pk2, q))."""
+def split_round(gk, gs, gc, nq, stream=None):
+    """A round's groups -> per query (keys u32, sums int64, counts u32) on the host, in key
+    order.  The groups are ordered by (pk2, q); a stable one-pass radix sort on the query
+    byte (on the device) makes each query's groups contiguous and keeps them in key order,
+    then one copy brings them to the host."""
     import numpy as np
-    k = gk.cpu().numpy().view(np.uint64)
-    sums = gs.cpu().numpy()
-    counts = gc.cpu().numpy().view(np.uint32)
-    q = (k & np.uint64(0xFF)).astype(np.int64)
-    order = np.argsort(q, kind="stable")
-    bounds = np.searchsorted(q[order], np.arange(nq + 1))
-    out = []
-    for i in range(nq):
-        sel = order[bounds[i]:bounds[i + 1]]
-        out.append(((k[sel] >> np.uint64(8)).astype(np.uint32), sums[sel], counts[sel]))
-    return out
+    import torch
+
+    from . import rfx as R
+    g = gk.shape[0]
+    q8 = (gk & 0xFF).to(torch.int32)
+    perm = torch.arange(g, dtype=torch.int32, device=gk.device)
+    if g > 1:
+        R.sort_pairs(q8, perm, begin_bit=0, end_bit=8, stream=stream)
+    p64 = perm.to(torch.int64)
+    k = (gk.index_select(0, p64) >> 8).to(torch.int32).cpu().numpy().view(np.uint32)
+    sums = gs.index_select(0, p64).cpu().numpy()
+    counts = gc.index_select(0, p64).cpu().numpy().view(np.uint32)
+    bounds = np.searchsorted(q8.cpu().numpy(), np.arange(nq + 1))
+    return [(k[bounds[i]:bounds[i + 1]], sums[bounds[i]:bounds[i + 1]], counts[bounds[i]:bounds[i + 1]])
+            for i in range(nq)]
 
 
 def run_round_host(res, queries, device="cuda", stream=None):
     """A round end to end: lists generated, queries with and without a list run as two
     batched plans (the intersection applies to the first only), results on the host in
     the order of `queries`."""
-    import torch
     res_by_q = [None] * len(queries)
     with_list = [i for i, q in enumerate(queries) if q.list_size > 0]
     without = [i for i, q in enumerate(queries) if q.list_size == 0]
@@ -300,11 +305,7 @@ def run_round_host(res, queries, device="cuda", stream=None):
         qs = [queries[i] for i in idx]
         lists = [query_list(q, res.n2, device) for q in qs] if has else None
         gk, gs, gc = run_round(res, qs, lists, stream=stream)
-        if stream is not None:
-            stream.synchronize()
-        else:
-            torch.cuda.synchronize()
-        for i, r in zip(idx, split_round(gk, gs, gc, len(qs))):
+        for i, r in zip(idx, split_round(gk, gs, gc, len(qs), stream=stream)):
             res_by_q[i] = r
     return res_by_q
 

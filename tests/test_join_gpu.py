@@ -180,3 +180,50 @@ def test_join_aggregate_skewed_key(cuda):
     exp_sum = (int(amounts.astype(object).sum()) * nr) % (1 << 64)
     assert int(to_np(sums).view(np.uint64)[0]) == exp_sum
     assert int(to_np(counts).view(np.uint32)[0]) == (nr * ns) % (1 << 32)
+
+
+@pytest.mark.parametrize("variant", [0, 1])
+def test_join_emit_variants(cuda, variant):
+    """Both emit kernels (pinned through the tuner) on the shapes that exercise the staged
+    one's paths: many outputs per left row (the right window in shared memory), rows with
+    one output each (more left rows per tile than the stage holds: per-output search),
+    a skewed key whose right run is larger than the staged window, 4-byte rows (plain
+    copies instead of bulk copies), unaligned relation bases, and a capacity cut."""
+    import torch
+    try:
+        R.tune_force(R.TUNE_JOIN_EMIT, variant)
+        rng = np.random.default_rng(11)
+        cases = []
+        # duplicate keys on both sides (the benchmark's shape, smaller)
+        lk = np.sort(rng.integers(0, 5000, 40000)).astype(np.uint64)
+        rk = np.sort(rng.integers(0, 5000, 160000)).astype(np.uint64)
+        cases.append((O.pack([32, 32], [lk, rng.integers(0, 2**32, 40000, dtype=np.uint64)]), 32,
+                      O.pack([32, 64], [rk, rng.integers(0, 2**40, 160000, dtype=np.uint64)]), 64, 16))
+        # one match per left row, sparse keys
+        ku = np.arange(0, 300000, 3, dtype=np.uint64)
+        cases.append((O.pack([32, 32], [ku, ku]), 32, O.pack([32, 32], [ku, ku + 1]), 32, 8))
+        # a skewed key: 3 left rows x 50000 right rows, then ordinary keys
+        lk = np.concatenate([np.full(3, 5, np.uint64), np.arange(6, 3000, dtype=np.uint64)])
+        rk = np.concatenate([np.full(50000, 5, np.uint64), np.repeat(np.arange(6, 3000, dtype=np.uint64), 2)])
+        cases.append((O.pack([32, 32], [lk, np.arange(len(lk), dtype=np.uint64)]), 32,
+                      O.pack([32, 64], [rk, np.arange(len(rk), dtype=np.uint64)]), 64, 16))
+        # 4-byte rows on both sides
+        lk = np.sort(rng.integers(0, 2000, 20000)).astype(np.uint64)
+        rk = np.sort(rng.integers(0, 2000, 30000)).astype(np.uint64)
+        cases.append((O.pack([24, 8], [lk, lk & np.uint64(0xff)]), 8, O.pack([24, 8], [rk, rk & np.uint64(0x7f)]), 8,
+                      8))
+        for left, lvb, right, rvb, ob in cases:
+            exp = O.join_tuples(left, lvb, right, rvb, ob)
+            got, total = R.join_tuples(_dev(left, cuda), lvb, _dev(right, cuda), rvb, ob)
+            assert total == len(exp) and np.array_equal(to_np(got), exp)
+            # bases 1 row into their allocations (not 16-byte aligned for 8- and 4-byte rows)
+            dl = _dev(np.concatenate([left[:1], left]), cuda)[1:]
+            dr = _dev(np.concatenate([right[:1], right]), cuda)[1:]
+            got, total = R.join_tuples(dl, lvb, dr, rvb, ob)
+            assert total == len(exp) and np.array_equal(to_np(got), exp)
+            part, _ = R.join_tuples(_dev(left, cuda), lvb, _dev(right, cuda), rvb, ob, capacity=len(exp) // 2 + 7)
+            assert np.array_equal(to_np(part), exp[:len(exp) // 2 + 7])
+        torch.cuda.synchronize()
+        assert R.device_status() == R.OK
+    finally:
+        R.tune_force(R.TUNE_JOIN_EMIT, -1)

@@ -480,6 +480,13 @@ def _op_sort_large(ctx, peak, reps):
                                                                          note="the pipelined onesweep pass")
     finally:
         R.tune_force(R.TUNE_SORT_PASS, -1)
+    R.tune_force(R.TUNE_SORT_PASS, 4)
+    try:
+        out["sort_tuples_%s_16B_on_fk_match_rank" % tag] = _sort_line(f, 16, 64, 96, 3, peak,
+                                                                      flags=R.SORT_SKIP_TRIVIAL, passes=3,
+                                                                      note="per-tile pass ranking with match_any")
+    finally:
+        R.tune_force(R.TUNE_SORT_PASS, -1)
     del f
     keys = R.gen_uniform_rows(n, [32], 0x5EED0101, [0], [1 << 32], device=ctx.dev)
     out["sort_keys_%s_u32" % tag] = _sort_line(keys.view(torch.uint8).view(n, 4), 4, 0, 32, 3, peak,
@@ -841,10 +848,11 @@ def serving_benchmark(dev, nq, rates=(100.0, 300.0, 1000.0, 3000.0, 5000.0), slo
     S.run_round_host(res, warm, dev)
     out = {"resident_gb": res.nbytes() / 1e9, "slots": slots, "budget_gb": S.BUDGET_BYTES / 1e9,
            "queries_per_rate": nq, "rates": {}}
+    servers = (("serial", S.Server(res, slots=1, device=dev, plain=True)),
+               ("serving", S.Server(res, slots=slots, device=dev)))   # pinned result buffers made once
     for rate in rates:
         line = {}
-        for name, srv in (("serial", S.Server(res, slots=1, device=dev, plain=True)),
-                          ("serving", S.Server(res, slots=slots, device=dev))):
+        for name, srv in servers:
             reqs = S.gen_requests(nq, rate)
             torch.cuda.synchronize()
             torch.cuda.reset_peak_memory_stats(dev)

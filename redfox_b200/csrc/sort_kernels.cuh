@@ -20,11 +20,13 @@ constexpr int kSortWarps = kSortThreads / 32;
 constexpr int kMaxSortPasses = 16;  // up to 128 key bits per call
 constexpr int kSortLookWindow = 16;  // predecessors examined per look-back round trip
 
-// Items per thread by the bytes moved per item.
+// Items per thread by the bytes moved per item: tiles of 24-48 KB (as large as 128
+// registers allow without spills), so the per-tile fixed costs (barriers, the look-back)
+// are spread over enough keys.
 template <int K, int V>
 struct SortTuning {
   static constexpr int B = K + V;
-  static constexpr int IPT = B <= 8 ? 16 : B <= 16 ? 12 : B <= 32 ? 8 : B <= 64 ? 4 : 2;
+  static constexpr int IPT = B <= 4 ? 24 : B <= 8 ? 20 : B <= 16 ? 12 : B <= 32 ? 8 : B <= 64 ? 4 : 2;
   static constexpr int TILE = kSortThreads * IPT;
   static constexpr int SBYTES = (K > V ? K : V);
 };
@@ -86,14 +88,16 @@ __device__ __forceinline__ uint32_t elem_bits(const Elem<K>& e, uint32_t shift) 
   if constexpr (Elem<K>::NW == 1) {
     return e.w[0] >> shift;
   } else {
-    const uint32_t q = shift >> 5, r = shift & 31;
-    uint32_t lo = 0, hi = 0;
+    const uint32_t q = shift >> 5;
+    uint32_t lo = e.w[0], hi = e.w[1];
 #pragma unroll
-    for (int k = 0; k < Elem<K>::NW; ++k) {
-      lo = (k == (int)q) ? e.w[k] : lo;
-      hi = (k == (int)q + 1) ? e.w[k] : hi;
+    for (int k = 1; k < Elem<K>::NW; ++k) {
+      if ((int)q == k) {
+        lo = e.w[k];
+        hi = k + 1 < Elem<K>::NW ? e.w[k + 1] : 0u;
+      }
     }
-    return r ? ((lo >> r) | (hi << (32 - r))) : lo;
+    return __funnelshift_r(lo, hi, shift & 31);
   }
 }
 
@@ -256,7 +260,29 @@ __device__ __forceinline__ void sort_prefetch(uint8_t* dst, const uint8_t* keys,
   }
 }
 
-template <int K, int V>
+// The lanes of a warp whose digit equals this lane's (within `valid`): the intersection
+// over the digit's bits of the ballot of lanes sharing that bit (lop3-friendly form), or
+// the hardware match.
+template <bool MATCH>
+__device__ __forceinline__ unsigned digit_peers(uint32_t d, bool valid, uint32_t bits) {
+  if constexpr (MATCH) {
+    const unsigned m = __match_any_sync(0xffffffffu, valid ? d : 0xffffffffu);
+    return valid ? m : 0u;
+  } else {
+    unsigned peers = __ballot_sync(0xffffffffu, valid);
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+      if ((uint32_t)b < bits) {
+        const unsigned bb = __ballot_sync(0xffffffffu, (d >> b) & 1u);
+        const unsigned mb = 0u - ((d >> b) & 1u);   // all ones where this lane's bit is set
+        peers &= ~(bb ^ mb);
+      }
+    }
+    return peers;
+  }
+}
+
+template <int K, int V, bool MATCH = false>
 __global__ void __launch_bounds__(kSortThreads, 2)
 sort_pass_kernel(const SortPassArgs a) {
   using T = SortTuning<K, V>;
@@ -266,13 +292,14 @@ sort_pass_kernel(const SortPassArgs a) {
   extern __shared__ __align__(16) uint8_t sbuf[];              // 1 or 2 buffers of TILE * EB
   __shared__ uint32_t whist[kSortWarps][kRadix];               // per-warp digit counts
   __shared__ uint32_t s_local[kRadix];                         // tile-local digit start
-  __shared__ uint32_t s_global[kRadix];                        // global base of the digit run
+  __shared__ unsigned long long s_gb[kRadix];                  // output index of slot i = s_gb[digit] + i
   __shared__ uint8_t s_dig[TILE];                              // digit of each sorted slot
   __shared__ uint32_t s_scan[kSortWarps];
   __shared__ uint32_t s_tile[2];
   const uint32_t t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const uint64_t num_tiles = (a.n + TILE - 1) / TILE;
   const bool pf = SB::PF && (reinterpret_cast<uintptr_t>(a.keys_in) & 15u) == 0;
+  const uint32_t dbits = 32 - __clz(a.mask);   // bits in this pass's digit (ballots needed)
   if (t == 0) s_tile[0] = atomicAdd(a.tile_counter, 1u);
   __syncthreads();
   if (pf && s_tile[0] < num_tiles) sort_prefetch<K>(sbuf, a.keys_in, s_tile[0], TILE, a.n);
@@ -308,18 +335,11 @@ sort_pass_kernel(const SortPassArgs a) {
       const uint32_t li = wbase + j * 32 + lane;
       const bool valid = li < tcount;
       const uint32_t d = valid ? (elem_bits<K>(key[j], a.shift) & a.mask) : 0u;
-      // lanes with the same digit: the intersection of the 8 digit-bit ballots (valid
-      // lanes only)
-      unsigned peers = __ballot_sync(0xffffffffu, valid);
-#pragma unroll
-      for (int b = 0; b < 8; ++b) {
-        const unsigned bb = __ballot_sync(0xffffffffu, (d >> b) & 1u);
-        peers &= ((d >> b) & 1u) ? bb : ~bb;
-      }
+      const unsigned peers = digit_peers<MATCH>(d, valid, dbits);
       const unsigned lower = peers & ((1u << lane) - 1);
       uint32_t base = 0;
       if (valid) base = whist[warp][d];
-      rank[j] = base + __popc(lower);
+      rank[j] = (base + __popc(lower)) | (d << 16);   // the digit rides along: extracted once
       __syncwarp();
       if (valid && lower == 0) whist[warp][d] = base + __popc(peers);
       __syncwarp();
@@ -351,14 +371,17 @@ sort_pass_kernel(const SortPassArgs a) {
       s_local[t] = wpre + incl - count;
     }
     __syncthreads();
-    // keys: scatter into tile order in shared memory (every thread's keys are in registers)
+    // keys: scatter into tile order in shared memory (every thread's keys are in registers),
+    // each slot's digit beside it
     Elem<K>* skeys = reinterpret_cast<Elem<K>*>(stage);
 #pragma unroll
     for (int j = 0; j < IPT; ++j) {
       const uint32_t li = wbase + j * 32 + lane;
       if (li < tcount) {
-        const uint32_t d = elem_bits<K>(key[j], a.shift) & a.mask;
-        skeys[s_local[d] + whist[warp][d] + rank[j]] = key[j];
+        const uint32_t d = rank[j] >> 16;
+        const uint32_t slot = s_local[d] + whist[warp][d] + (rank[j] & 0xffffu);
+        skeys[slot] = key[j];
+        s_dig[slot] = (uint8_t)d;
       }
     }
     // decoupled look-back for digit t, kSortLookWindow predecessors per round trip
@@ -402,15 +425,13 @@ sort_pass_kernel(const SortPassArgs a) {
         }
         st_relaxed_u32(a.status + tile * kRadix + t, kSFlagInc | ((prefix + count) & kSValMask));
       }
-      s_global[t] = a.gexcl[t] + prefix;
+      // (global start of the digit's run) - (its tile-local start), modulo 2^64
+      s_gb[t] = (unsigned long long)a.gexcl[t] + prefix - s_local[t];
     }
     __syncthreads();
     for (uint32_t i = t; i < tcount; i += kSortThreads) {
-      const Elem<K> k = skeys[i];
-      const uint32_t d = elem_bits<K>(k, a.shift) & a.mask;
-      s_dig[i] = (uint8_t)d;
-      const uint64_t pos = (uint64_t)s_global[d] + (i - s_local[d]);
-      if (pos < a.n) store_elem<K>(a.keys_out, pos, k);
+      const uint64_t pos = s_gb[s_dig[i]] + i;
+      if (pos < a.n) store_elem<K>(a.keys_out, pos, skeys[i]);
     }
     if constexpr (V > 0) {
       __syncthreads();
@@ -419,14 +440,13 @@ sort_pass_kernel(const SortPassArgs a) {
       for (int j = 0; j < IPT; ++j) {
         const uint32_t li = wbase + j * 32 + lane;
         if (li < tcount) {
-          const uint32_t d = elem_bits<K>(key[j], a.shift) & a.mask;
-          svals[s_local[d] + whist[warp][d] + rank[j]] = load_elem<V>(a.vals_in, tbase + li);
+          const uint32_t d = rank[j] >> 16;
+          svals[s_local[d] + whist[warp][d] + (rank[j] & 0xffffu)] = load_elem<V>(a.vals_in, tbase + li);
         }
       }
       __syncthreads();
       for (uint32_t i = t; i < tcount; i += kSortThreads) {
-        const uint32_t d = s_dig[i];
-        const uint64_t pos = (uint64_t)s_global[d] + (i - s_local[d]);
+        const uint64_t pos = s_gb[s_dig[i]] + i;
         if (pos < a.n) store_elem<V>(a.vals_out, pos, svals[i]);
       }
     }

@@ -73,9 +73,12 @@ rfx_status run_sort_kv(SortPlan& s) {
   // prefetched into shared memory); 1 / 2 / 3 = the pipelined onesweep pass (TMA stages +
   // a look-back warp, one block per SM) with its default / fewer / other items per thread,
   // where it applies: keys without values in 4/8/16-byte containers on 16-byte aligned
-  // buffers.  The autotuner may pick per size class.
+  // buffers; 4 = the per-tile pass ranking with __match_any_sync instead of bit ballots
+  // (same keys).  The autotuner may pick per size class.
   const size_t tile_smem = SortBuffers<K, V>::SMEM;
   RFX_CUDA_TRY(allow_smem((const void*)sort_pass_kernel<K, V>, tile_smem));
+  if constexpr (V == 0 && (K == 4 || K == 8 || K == 16))
+    RFX_CUDA_TRY(allow_smem((const void*)sort_pass_kernel<K, V, true>, tile_smem));
   const int tile_grid = persistent_grid((const void*)sort_pass_kernel<K, V>, kSortThreads, tile_smem,
                                         s.tiles ? s.tiles : 1);
   constexpr bool kOnesweep = V == 0 && (K == 4 || K == 8 || K == 16);
@@ -147,7 +150,9 @@ rfx_status run_sort_kv(SortPlan& s) {
         using TD = OsTuning<K, OsIpt<K>::DEF>;
         using TS = OsTuning<K, OsIpt<K>::SMALL>;
         using TL = OsTuning<K, OsIpt<K>::ALT>;
-        if (os_ok && v == 1)
+        if (v == 4)
+          sort_pass_kernel<K, V, true><<<tile_grid, kSortThreads, tile_smem, s.stream>>>(a);
+        else if (os_ok && v == 1)
           sort_onesweep_kernel<K, TD::IPT><<<os_grid[0], kOsThreads, TD::SMEM, s.stream>>>(a);
         else if (os_ok && v == 2)
           sort_onesweep_kernel<K, TS::IPT><<<os_grid[1], kOsThreads, TS::SMEM, s.stream>>>(a);
@@ -161,7 +166,7 @@ rfx_status run_sort_kv(SortPlan& s) {
       RFX_CUDA_TRY(cudaGetLastError());
       return RFX_OK;
     };
-    const int v = os_ok ? tune_pick(TUNE_SORT_PASS, (uint64_t)K << 8 | V, s.n, 4, launch, s.stream) : 0;
+    const int v = os_ok ? tune_pick(TUNE_SORT_PASS, (uint64_t)K << 8 | V, s.n, 5, launch, s.stream) : 0;
     rfx_status st = launch(v);
     if (st != RFX_OK) return st;
     ++s.executed;

@@ -607,7 +607,8 @@ _declare_tune()
 TUNE_OPS = {1: "reduce_tuples", 2: "set_filter", 3: "select_compact", 4: "filter_aggregate", 5: "sort_pass",
             6: "join_emit"}
 TUNE_JOIN_EMIT = 6   # variants: 0 operands staged in shared memory by bulk copies, 1 gathered per output
-TUNE_SORT_PASS = 5   # variants: 0 per-tile pass, 1 / 2 / 3 pipelined onesweep pass with three tile sizes
+TUNE_SORT_PASS = 5   # variants: 0 per-tile pass, 1 / 2 / 3 pipelined onesweep pass (three tile sizes),
+#                      4 per-tile pass ranking with match_any
 
 
 def tune(mode=1):

@@ -269,11 +269,46 @@ def run_round(res, queries, lists=None, stream=None):
     return gk, gs, gc
 
 
-def split_round(gk, gs, gc, nq, stream=None):
+class PinnedStage:
+    """A page-locked host buffer that results are copied into (device-to-host copies from
+    pageable memory run at a fraction of the link's speed); grown geometrically, reused."""
+
+    def __init__(self, nbytes=0):
+        import torch
+        # pinning memory takes long (hundreds of MB per ~0.1 s): done up front, not per round
+        self.buf = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True) if nbytes else None
+
+    def take(self, nbytes):
+        import torch
+        if self.buf is None or self.buf.numel() < nbytes:
+            cap = max(nbytes, 2 * (self.buf.numel() if self.buf is not None else 0), 1 << 20)
+            self.buf = torch.empty(cap, dtype=torch.uint8, pin_memory=True)
+        return self.buf
+
+
+def to_host(tensors, stream=None, stage=None, copy=False):
+    """Device tensors -> numpy arrays.  With a PinnedStage the copies go through its
+    page-locked buffer (the arrays are views of it unless copy=True)."""
+    import torch
+    if stage is None:
+        return [t.cpu().numpy() for t in tensors]
+    sizes = [t.numel() * t.element_size() for t in tensors]
+    buf = stage.take(sum((b + 255) // 256 * 256 for b in sizes))
+    views, off = [], 0
+    for t, b in zip(tensors, sizes):
+        v = buf[off:off + b].view(t.dtype).view(t.shape)
+        v.copy_(t, non_blocking=True)
+        views.append(v)
+        off += (b + 255) // 256 * 256
+    (stream or torch.cuda.current_stream()).synchronize()
+    return [v.numpy().copy() if copy else v.numpy() for v in views]
+
+
+def split_round(gk, gs, gc, nq, stream=None, stage=None, copy=True):
     """A round's groups -> per query (keys u32, sums int64, counts u32) on the host, in key
     order.  The groups are ordered by (pk2, q); a stable one-pass radix sort on the query
     byte (on the device) makes each query's groups contiguous and keeps them in key order,
-    then one copy brings them to the host."""
+    then one copy per column brings them to the host (through `stage` when given)."""
     import numpy as np
     import torch
 
@@ -284,18 +319,18 @@ def split_round(gk, gs, gc, nq, stream=None):
     if g > 1:
         R.sort_pairs(q8, perm, begin_bit=0, end_bit=8, stream=stream)
     p64 = perm.to(torch.int64)
-    k = (gk.index_select(0, p64) >> 8).to(torch.int32).cpu().numpy().view(np.uint32)
-    sums = gs.index_select(0, p64).cpu().numpy()
-    counts = gc.index_select(0, p64).cpu().numpy().view(np.uint32)
-    bounds = np.searchsorted(q8.cpu().numpy(), np.arange(nq + 1))
+    kk = (gk.index_select(0, p64) >> 8).to(torch.int32)
+    k, sums, counts, qh = to_host([kk, gs.index_select(0, p64), gc.index_select(0, p64), q8], stream, stage, copy)
+    k, counts = k.view(np.uint32), counts.view(np.uint32)
+    bounds = np.searchsorted(qh, np.arange(nq + 1))
     return [(k[bounds[i]:bounds[i + 1]], sums[bounds[i]:bounds[i + 1]], counts[bounds[i]:bounds[i + 1]])
             for i in range(nq)]
 
 
-def run_round_host(res, queries, device="cuda", stream=None):
+def run_round_host(res, queries, device="cuda", stream=None, stage=None, copy=True):
     """A round end to end: lists generated, queries with and without a list run as two
     batched plans (the intersection applies to the first only), results on the host in
-    the order of `queries`."""
+    the order of `queries` (copied out of `stage` unless copy=False)."""
     res_by_q = [None] * len(queries)
     with_list = [i for i, q in enumerate(queries) if q.list_size > 0]
     without = [i for i, q in enumerate(queries) if q.list_size == 0]
@@ -305,7 +340,7 @@ def run_round_host(res, queries, device="cuda", stream=None):
         qs = [queries[i] for i in idx]
         lists = [query_list(q, res.n2, device) for q in qs] if has else None
         gk, gs, gc = run_round(res, qs, lists, stream=stream)
-        for i, r in zip(idx, split_round(gk, gs, gc, len(qs), stream=stream)):
+        for i, r in zip(idx, split_round(gk, gs, gc, len(qs), stream=stream, stage=stage, copy=copy)):
             res_by_q[i] = r
     return res_by_q
 
@@ -318,7 +353,11 @@ class Server:
     plain=True every round is one query run by `run_query` (the serial plain baseline
     when slots = 1).  Latency = host time from arrival to the result on the host."""
 
-    def __init__(self, res, slots=2, budget_bytes=BUDGET_BYTES, device="cuda", max_batch=128, plain=False):
+    # result bytes staged per query: (key, sum, count, query byte) for each of its groups,
+    # at most one per D2 row and in practice below 3M
+    STAGE_GROUPS_PER_QUERY = 3_000_000
+
+    def __init__(self, res, slots=2, budget_bytes=BUDGET_BYTES, device="cuda", max_batch=64, plain=False):
         import torch
         self.res = res
         self.slots = slots
@@ -329,17 +368,19 @@ class Server:
         if self.device.index is None:
             self.device = torch.device("cuda", torch.cuda.current_device())
         self.streams = [torch.cuda.Stream(device=self.device) for _ in range(slots)]
+        # results reach the host through these page-locked buffers, sized for a full round
+        per_query = 20 * min(self.STAGE_GROUPS_PER_QUERY, res.n2)
+        self.stages = [PinnedStage(self.max_batch * per_query) for _ in range(slots)]
 
     def _run(self, i, rnd, keep_results):
-        import torch
+        import numpy as np
         if self.plain:
             q = rnd[0]
             lst = query_list(q, self.res.n2, self.device)
-            out = run_query(self.res, q, lst)
-            host = tuple(t.to("cpu", non_blocking=True) for t in out)
-            self.streams[i].synchronize()
-            return [host]
-        return run_round_host(self.res, rnd, self.device, stream=self.streams[i])
+            k, sm, c = to_host(run_query(self.res, q, lst), self.streams[i], self.stages[i], copy=keep_results)
+            return [(k.view(np.uint32), sm, c.view(np.uint32))]
+        return run_round_host(self.res, rnd, self.device, stream=self.streams[i], stage=self.stages[i],
+                              copy=keep_results)
 
     def serve(self, requests, keep_results=False):
         import torch

@@ -132,14 +132,14 @@ def test_reference_compatible_entries(cuda):
     assert np.array_equal(to_np(dk), O.sort_pairs(k64, begin_bit=0, end_bit=37))
 
 
-# Tile sizes of the two pass kernels: the pipelined onesweep pass (3072 / 6144 / 8192 keys
-# of 16 / 8 / 4 bytes) and the per-tile pass (3072 / 4096 / 4096); sizes around both,
-# and sizes with many tiles per block (a persistent grid of one block per SM).
-ONESWEEP_SIZES = {16: [3071, 3072, 3073, 9217, 2_000_003], 8: [6143, 6144, 6145, 18_433, 3_000_001],
-                  4: [8191, 8192, 8193, 24_577, 4_000_037]}
+# Tile sizes of the two pass kernels: the per-tile pass (3072 / 5120 / 6144 keys of 16 / 8
+# / 4 bytes) and the pipelined onesweep pass (3072 / 6144 / 8192 by default); sizes around
+# both, and sizes with many tiles per block (persistent grids).
+ONESWEEP_SIZES = {16: [3071, 3072, 3073, 9217, 2_000_003], 8: [5119, 5120, 5121, 6145, 18_433, 3_000_001],
+                  4: [6143, 6144, 6145, 8193, 24_577, 4_000_037]}
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
 @pytest.mark.parametrize("kb", [4, 8, 16])
 def test_sort_pass_variants_match_oracle(cuda, kb, variant):
     """Every pass kernel variant (pinned through the tuner) gives the oracle's stable

@@ -578,6 +578,15 @@ def _op_setops(ctx, peak, reps):
             no = int(c.item())
             ops["%s_%s" % (name, tag)] = _op_line(a.shape[0] + b.shape[0], (a.shape[0] + b.shape[0] + no) * 4, ms,
                                                   peak, out=no, note=note)
+            if name == "intersect":   # the tuner's 16-items-per-thread variant beside the default
+                R.tune_force(2, 2)
+                try:
+                    ms = _time_ms(run, reps)
+                finally:
+                    R.tune_force(2, -1)
+                ops["%s_%s_16_per_thread" % (name, tag)] = _op_line(a.shape[0] + b.shape[0],
+                                                                    (a.shape[0] + b.shape[0] + no) * 4, ms, peak,
+                                                                    out=no, note=note)
     return ops
 
 

@@ -75,6 +75,19 @@ __device__ __forceinline__ uint64_t block_exclusive_u64(uint64_t x, uint64_t* s_
 // otherwise.  A window that does not fit falls back to searches in global memory.
 constexpr uint32_t kFbWindowBytes = 64 * 1024;
 
+// First index in [lo, n) of the sorted u64 window with w[i] >= k (strict: > k).
+template <bool STRICT>
+__device__ __forceinline__ uint32_t smem_bound64(const uint64_t* w, uint32_t lo, uint32_t n, uint64_t k) {
+  uint32_t hi = n;
+  while (lo < hi) {
+    const uint32_t mid = (lo + hi) >> 1;
+    const uint64_t m = w[mid];
+    if (STRICT ? (m <= k) : (m < k)) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
 template <typename T>
 __device__ __forceinline__ uint32_t smem_bound(const T* w, uint32_t n, u128 k, bool strict) {
   uint32_t lo = 0, hi = n;
@@ -154,8 +167,14 @@ __global__ void __launch_bounds__(kJoinThreads) find_bounds_kernel(const FindBou
       } else {
         uint64_t l, h;
         if (staged && key64) {
-          l = wlo + smem_bound<uint64_t>(s_win64, (uint32_t)wn, k, false);
-          h = wlo + smem_bound<uint64_t>(s_win64, (uint32_t)wn, k, true);
+          // 64-bit compares (a left key beyond 64 bits lies above the whole window)
+          if ((uint64_t)(k >> 64)) {
+            l = h = wlo + wn;
+          } else {
+            const uint32_t l32 = smem_bound64<false>(s_win64, 0, (uint32_t)wn, (uint64_t)k);
+            l = wlo + l32;
+            h = wlo + smem_bound64<true>(s_win64, l32, (uint32_t)wn, (uint64_t)k);
+          }
         } else if (staged) {
           l = wlo + smem_bound<u128>(s_win128, (uint32_t)wn, k, false);
           h = wlo + smem_bound<u128>(s_win128, (uint32_t)wn, k, true);

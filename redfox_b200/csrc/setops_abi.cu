@@ -53,16 +53,17 @@ rfx_status launch_filter_ipt(int mode, SetFilterArgs& a, cudaStream_t s) {
   return RFX_OK;
 }
 
-// Variant 0: 8 items per thread, 1: 4 (unique: always 8).  `clear` zeroes the look-back
+// Variant 0: 8 items per thread, 1: 4, 2: 16 (unique: always 8).  `clear` zeroes the look-back
 // status and tile counter before each launch.
 template <int E>
 rfx_status launch_filter(int mode, SetFilterArgs& a, cudaStream_t s, void* clear = nullptr, size_t clear_bytes = 0) {
   auto run = [&](int v) -> rfx_status {
     if (clear) RFX_CUDA_TRY(cudaMemsetAsync(clear, 0, clear_bytes, s));
-    return v == 0 || mode == KEEP_HEADS ? launch_filter_ipt<E, 8>(mode, a, s) : launch_filter_ipt<E, 4>(mode, a, s);
+    if (v == 0 || mode == KEEP_HEADS) return launch_filter_ipt<E, 8>(mode, a, s);
+    return v == 1 ? launch_filter_ipt<E, 4>(mode, a, s) : launch_filter_ipt<E, 16>(mode, a, s);
   };
   if (mode == KEEP_HEADS || !clear) return run(0);
-  return run(tune_pick(TUNE_SET_FILTER, ((uint64_t)E << 8) | (uint64_t)mode, a.na + a.nb, 2, run, s));
+  return run(tune_pick(TUNE_SET_FILTER, ((uint64_t)E << 8) | (uint64_t)mode, a.na + a.nb, 3, run, s));
 }
 
 rfx_status dispatch_filter(uint32_t e, int mode, SetFilterArgs& a, cudaStream_t s, void* clear = nullptr,

@@ -18,7 +18,7 @@
 namespace rfx {
 
 constexpr int kSetThreads = 256;
-// Items per thread: 8 by default, 4 as the tuner's alternative (unique always 8);
+// Items per thread: 8 by default, 4 and 16 as the tuner's alternatives (unique always 8);
 // elements up to 8 bytes live in 64-bit registers.
 constexpr int kSetIPT = 8;
 constexpr int kSetTile = kSetThreads * kSetIPT;
@@ -61,22 +61,24 @@ __device__ __forceinline__ uint64_t block_exclusive_u32(uint32_t x, uint32_t* s_
   return wpre + incl - x;
 }
 
+// Binary searches in a sorted shared-memory window, compared in the window's own type
+// (64-bit compares for elements up to 8 bytes).
 template <typename T>
-__device__ __forceinline__ uint32_t smem_lower(const T* w, uint32_t n, u128 k) {
+__device__ __forceinline__ uint32_t smem_lower(const T* w, uint32_t n, T k) {
   uint32_t lo = 0, hi = n;
   while (lo < hi) {
     const uint32_t mid = (lo + hi) >> 1;
-    if ((u128)w[mid] < k) lo = mid + 1;
+    if (w[mid] < k) lo = mid + 1;
     else hi = mid;
   }
   return lo;
 }
 template <typename T>
-__device__ __forceinline__ uint32_t smem_lower_strict(const T* w, uint32_t n, u128 k) {
+__device__ __forceinline__ uint32_t smem_lower_strict(const T* w, uint32_t n, T k) {
   uint32_t lo = 0, hi = n;
   while (lo < hi) {
     const uint32_t mid = (lo + hi) >> 1;
-    if ((u128)w[mid] <= k) lo = mid + 1;
+    if (w[mid] <= k) lo = mid + 1;
     else hi = mid;
   }
   return lo;

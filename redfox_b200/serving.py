@@ -308,7 +308,8 @@ def split_round(gk, gs, gc, nq, stream=None, stage=None, copy=True):
     """A round's groups -> per query (keys u32, sums int64, counts u32) on the host, in key
     order.  The groups are ordered by (pk2, q); a stable one-pass radix sort on the query
     byte (on the device) makes each query's groups contiguous and keeps them in key order,
-    then one copy per column brings them to the host (through `stage` when given)."""
+    then one copy per column (16 bytes per group) and the per-query group counts bring them
+    to the host (through `stage` when given)."""
     import numpy as np
     import torch
 
@@ -320,9 +321,11 @@ def split_round(gk, gs, gc, nq, stream=None, stage=None, copy=True):
         R.sort_pairs(q8, perm, begin_bit=0, end_bit=8, stream=stream)
     p64 = perm.to(torch.int64)
     kk = (gk.index_select(0, p64) >> 8).to(torch.int32)
-    k, sums, counts, qh = to_host([kk, gs.index_select(0, p64), gc.index_select(0, p64), q8], stream, stage, copy)
+    per_q = torch.bincount(q8, minlength=nq)[:nq]          # groups of each query, on the device
+    k, sums, counts, nper = to_host([kk, gs.index_select(0, p64), gc.index_select(0, p64), per_q], stream, stage,
+                                    copy)
     k, counts = k.view(np.uint32), counts.view(np.uint32)
-    bounds = np.searchsorted(qh, np.arange(nq + 1))
+    bounds = np.concatenate([[0], np.cumsum(nper)])
     return [(k[bounds[i]:bounds[i + 1]], sums[bounds[i]:bounds[i + 1]], counts[bounds[i]:bounds[i + 1]])
             for i in range(nq)]
 

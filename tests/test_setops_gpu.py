@@ -105,3 +105,24 @@ def test_reference_compatible_set_entries(cuda):
     assert np.array_equal(to_np(u)[:k], g["e4_c1_unique"])
     assert R.LIB.rfx_set_union_compat(P(out.data_ptr()), P(size.data_ptr()), P(da.data_ptr()), P(da.data_ptr()),
                                       P(db.data_ptr()), P(db.data_ptr()), 99) == R.ERR_UNSUPPORTED
+
+
+@pytest.mark.parametrize("variant", [0, 1, 2])
+@pytest.mark.parametrize("dtype", [np.uint32, np.uint64])
+def test_set_filter_variants(cuda, variant, dtype):
+    """Each items-per-thread variant of the set filters (pinned through the tuner) gives the
+    STL results, across tile boundaries of every variant (1024 / 2048 / 4096 elements) and
+    with runs of equal values that cross tiles."""
+    try:
+        R.tune_force(2, variant)
+        rng = np.random.default_rng(variant * 10 + np.dtype(dtype).itemsize)
+        for na, nb, hi in ((4095, 4097, 900), (4096, 1000, 50), (300_001, 120_007, 100_000), (8193, 8191, 3)):
+            a = np.sort(rng.integers(0, hi, na)).astype(dtype)
+            b = np.sort(rng.integers(0, hi, nb)).astype(dtype)
+            da, db = _dev(a, cuda), _dev(b, cuda)
+            for op, ref in ((R.SET_UNION, O.set_union), (R.SET_DIFFERENCE, O.set_difference),
+                            (R.SET_INTERSECTION, O.set_intersection)):
+                assert np.array_equal(to_np(R.set_op(op, da, db)), ref(a, b)), (op, na, nb)
+        assert R.device_status() == R.OK
+    finally:
+        R.tune_force(2, -1)

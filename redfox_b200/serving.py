@@ -333,7 +333,19 @@ def split_round(gk, gs, gc, nq, stream=None, stage=None, copy=True):
 def run_round_host(res, queries, device="cuda", stream=None, stage=None, copy=True):
     """A round end to end: lists generated, queries with and without a list run as two
     batched plans (the intersection applies to the first only), results on the host in
-    the order of `queries` (copied out of `stage` unless copy=False)."""
+    the order of `queries` (copied out of `stage` unless copy=False).  A round of one query
+    runs the plain plan."""
+    import contextlib
+
+    import numpy as np
+    import torch
+    if len(queries) == 1:
+        # nothing to share: the plain plan (fewer passes than the batched one), on `stream`
+        q = queries[0]
+        with torch.cuda.stream(stream) if stream is not None else contextlib.nullcontext():
+            out = run_query(res, q, query_list(q, res.n2, device))
+        k, sm, c = to_host(out, stream, stage, copy)
+        return [(k.view(np.uint32), sm, c.view(np.uint32))]
     res_by_q = [None] * len(queries)
     with_list = [i for i, q in enumerate(queries) if q.list_size > 0]
     without = [i for i, q in enumerate(queries) if q.list_size == 0]

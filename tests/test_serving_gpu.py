@@ -82,3 +82,20 @@ def test_plain_server_is_one_query_at_a_time(resident):
     assert np.array_equal(q.result[0], alone[0].numpy().view(np.uint32))
     assert np.array_equal(q.result[1], alone[1].numpy())
     assert np.array_equal(q.result[2], alone[2].numpy().view(np.uint32))
+
+
+def test_single_query_round_on_a_side_stream(resident):
+    """A round of one query runs the plain plan on the round's stream; the batched plan
+    given the same single query agrees with it."""
+    import torch
+    reqs = _requests(resident, 3, seed=25)
+    st = torch.cuda.Stream()
+    for q in reqs:
+        got = S.run_round_host(resident, [q], "cuda", stream=st, stage=S.PinnedStage(1 << 20))[0]
+        alone = S.run_alone(resident, q)
+        lst = S.query_list(q, resident.n2, "cuda")
+        gk, gs, gc = S.run_round(resident, [q], None if lst is None else [lst])
+        bk, bs, bc = S.split_round(gk, gs, gc, 1)[0]
+        for a, b in ((got[0], alone[0].numpy().view(np.uint32)), (got[1], alone[1].numpy()),
+                     (got[2], alone[2].numpy().view(np.uint32)), (bk, got[0]), (bs, got[1]), (bc, got[2])):
+            assert np.array_equal(a, b), q

@@ -578,15 +578,16 @@ def _op_setops(ctx, peak, reps):
             no = int(c.item())
             ops["%s_%s" % (name, tag)] = _op_line(a.shape[0] + b.shape[0], (a.shape[0] + b.shape[0] + no) * 4, ms,
                                                   peak, out=no, note=note)
-            if name == "intersect":   # the tuner's 16-items-per-thread variant beside the default
-                R.tune_force(2, 2)
-                try:
-                    ms = _time_ms(run, reps)
-                finally:
-                    R.tune_force(2, -1)
-                ops["%s_%s_16_per_thread" % (name, tag)] = _op_line(a.shape[0] + b.shape[0],
-                                                                    (a.shape[0] + b.shape[0] + no) * 4, ms, peak,
-                                                                    out=no, note=note)
+            if name == "intersect":   # the tuner's other variants (4; one-pass 1 and 3) beside the default
+                for v, suffix in ((4, "two_pass_16_per_thread"), (1, "one_pass"), (3, "one_pass_16_per_thread")):
+                    R.tune_force(2, v)
+                    try:
+                        ms = _time_ms(run, reps)
+                    finally:
+                        R.tune_force(2, -1)
+                    ops["%s_%s_%s" % (name, tag, suffix)] = _op_line(a.shape[0] + b.shape[0],
+                                                                     (a.shape[0] + b.shape[0] + no) * 4, ms, peak,
+                                                                     out=no, note=note)
     return ops
 
 
@@ -859,6 +860,11 @@ def serving_benchmark(dev, nq, rates=(100.0, 300.0, 1000.0, 3000.0, 5000.0), slo
            "queries_per_rate": nq, "rates": {}}
     servers = (("serial", S.Server(res, slots=1, device=dev, plain=True)),
                ("serving", S.Server(res, slots=slots, device=dev)))   # pinned result buffers made once
+    for _, srv in servers:
+        # untimed: a burst (one large round per slot) and a few spaced queries (rounds of one),
+        # so each server's streams have their memory pools and kernels before the timed runs
+        srv.serve(S.gen_requests(8 * slots, 1e6, seed=S.SERVING_SEED + 98))
+        srv.serve(S.gen_requests(2 * slots, 200.0, seed=S.SERVING_SEED + 97))
     for rate in rates:
         line = {}
         for name, srv in servers:
@@ -871,6 +877,7 @@ def serving_benchmark(dev, nq, rates=(100.0, 300.0, 1000.0, 3000.0, 5000.0), slo
             line[name]["peak_in_flight"] = sch.peak_queries
             line[name]["rounds"] = len(srv.rounds)
             line[name]["mean_round"] = sum(srv.rounds) / max(1, len(srv.rounds))
+            line[name]["max_round_ms"] = 1e3 * max((e - b for _, b, e in srv.round_log), default=0.0)
             line[name]["peak_intermediate_gb"] = (torch.cuda.max_memory_allocated(dev) - base) / 1e9
         line["speedup_queries_per_s"] = line["serving"]["queries_per_s"] / line["serial"]["queries_per_s"]
         out["rates"][str(int(rate))] = line

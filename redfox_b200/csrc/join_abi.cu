@@ -37,13 +37,27 @@ FbLayout fb_layout(void* ws, uint64_t nl, bool with_offsets) {
   return L;
 }
 
+// The window of find_bounds: what a tile of kFbTile left rows is expected to need (nr / nl
+// right keys per left row, 1.25x for variation, 512 more) at the width the kernel stores
+// the keys in, between 8 and 64 KB.  Smaller windows leave room for more blocks per SM; a tile
+// whose window does not fit searches in global memory instead.
+uint32_t fb_window_bytes(uint64_t nl, uint64_t nr, uint32_t re, uint32_t rshift) {
+  const uint32_t kbits = re * 8u > rshift ? re * 8u - rshift : 0u;
+  const double kw = re <= 4 ? 4.0 : kbits <= 64 ? 8.0 : 16.0;
+  double want = nl ? (1.25 * kFbTile * ((double)nr / (double)nl) + 512.0) * kw : 0.0;
+  if (want < 8192.0) want = 8192.0;
+  if (want > (double)kFbWindowBytes) want = kFbWindowBytes;
+  return (uint32_t)align_up((uint64_t)want, 4096);
+}
+
 template <int LE, int RE>
 rfx_status launch_fb(FindBoundsArgs& a, cudaStream_t s) {
   auto k = find_bounds_kernel<LE, RE>;
   RFX_CUDA_TRY(allow_smem((const void*)k, kFbWindowBytes));
   const uint64_t tiles = (a.nl + kFbTile - 1) / kFbTile;
-  const int grid = persistent_grid((const void*)k, kJoinThreads, kFbWindowBytes, tiles ? tiles : 1);
-  k<<<grid, kJoinThreads, kFbWindowBytes, s>>>(a);
+  a.window_bytes = fb_window_bytes(a.nl, a.nr, RE, a.rshift);
+  const int grid = persistent_grid((const void*)k, kJoinThreads, a.window_bytes, tiles ? tiles : 1);
+  k<<<grid, kJoinThreads, a.window_bytes, s>>>(a);
   RFX_CUDA_TRY(cudaGetLastError());
   return RFX_OK;
 }
@@ -62,6 +76,7 @@ rfx_status launch_group(FindBoundsArgs& a, cudaStream_t s) {
   auto k = find_bounds_kernel<LE, RE, true>;
   RFX_CUDA_TRY(allow_smem((const void*)k, kFbWindowBytes));
   const uint64_t tiles = (a.nl + kFbTile - 1) / kFbTile;
+  a.window_bytes = kFbWindowBytes;   // the group count is on the device: the largest window
   const int grid = persistent_grid((const void*)k, kJoinThreads, kFbWindowBytes, tiles ? tiles : 1);
   k<<<grid, kJoinThreads, kFbWindowBytes, s>>>(a);
   RFX_CUDA_TRY(cudaGetLastError());

@@ -29,6 +29,7 @@ struct FindBoundsArgs {
   const uint8_t* right;
   uint64_t nr;
   uint32_t lshift, rshift;   // key = container >> shift
+  uint32_t window_bytes;     // dynamic shared memory of the launch (the window)
   int32_t* lb32;             // reference outputs (may be null)
   int32_t* scan32;
   uint64_t* lb64;            // workspace outputs for the fused join (may be null)
@@ -70,34 +71,37 @@ __device__ __forceinline__ uint64_t block_exclusive_u64(uint64_t x, uint64_t* s_
   return wpre + incl - x;
 }
 
-// Right-side keys a block's left keys can match, staged in dynamic shared memory
-// (kFbWindowBytes): u64 keys when the key (container >> shift) has at most 64 bits, u128
-// otherwise.  A window that does not fit falls back to searches in global memory.
+// Right-side keys a block's left keys can match, staged in dynamic shared memory of
+// FindBoundsArgs::window_bytes (at most kFbWindowBytes): u32 keys when the right
+// container has at most 4 bytes, u64 when the key (container >> shift) has at most 64
+// bits, u128 otherwise.  A window that does not fit falls back to searches in global
+// memory.
 constexpr uint32_t kFbWindowBytes = 64 * 1024;
 
-// First index in [lo, n) of the sorted u64 window with w[i] >= k (strict: > k).
-template <bool STRICT>
-__device__ __forceinline__ uint32_t smem_bound64(const uint64_t* w, uint32_t lo, uint32_t n, uint64_t k) {
+// First index in [lo, n) of the sorted window with w[i] >= k (strict: > k).
+template <bool STRICT, typename T>
+__device__ __forceinline__ uint32_t smem_bound_t(const T* w, uint32_t lo, uint32_t n, T k) {
   uint32_t hi = n;
   while (lo < hi) {
     const uint32_t mid = (lo + hi) >> 1;
-    const uint64_t m = w[mid];
+    const T m = w[mid];
     if (STRICT ? (m <= k) : (m < k)) lo = mid + 1;
     else hi = mid;
   }
   return lo;
 }
 
-template <typename T>
-__device__ __forceinline__ uint32_t smem_bound(const T* w, uint32_t n, u128 k, bool strict) {
-  uint32_t lo = 0, hi = n;
-  while (lo < hi) {
-    const uint32_t mid = (lo + hi) >> 1;
-    const u128 m = (u128)w[mid];
-    if (strict ? (m <= k) : (m < k)) lo = mid + 1;
-    else hi = mid;
+// The same bound found by galloping forward from `from` (every w[i] with i < from lies
+// before k): cheap when consecutive sorted keys land close together.
+template <bool STRICT, typename T>
+__device__ __forceinline__ uint32_t smem_gallop_t(const T* w, uint32_t from, uint32_t n, T k) {
+  uint32_t lo = from, hi = from, step = 1;
+  while (hi < n && (STRICT ? (w[hi] <= k) : (w[hi] < k))) {
+    lo = hi + 1;
+    hi = lo + step;
+    step <<= 1;
   }
-  return lo;
+  return smem_bound_t<STRICT>(w, lo, hi < n ? hi : n, k);
 }
 
 // GROUP = false: find_bounds (lower bounds, equality counts, their exclusive scan, total).
@@ -106,24 +110,29 @@ __device__ __forceinline__ uint32_t smem_bound(const T* w, uint32_t n, u128 k, b
 template <int LE, int RE, bool GROUP = false>
 __global__ void __launch_bounds__(kJoinThreads) find_bounds_kernel(const FindBoundsArgs a) {
   extern __shared__ __align__(16) uint8_t fb_window[];
-  uint64_t* s_win64 = reinterpret_cast<uint64_t*>(fb_window);
+  // the narrow window type; keys above its range lie above the whole window
+  using W = std::conditional_t<(RE <= 4), uint32_t, uint64_t>;
+  W* s_win = reinterpret_cast<W*>(fb_window);
   u128* s_win128 = reinterpret_cast<u128*>(fb_window);
-  const bool key64 = RE <= 8 || (uint32_t)RE * 8u - a.rshift <= 64u;
-  const uint64_t CAP = key64 ? kFbWindowBytes / 8 : kFbWindowBytes / 16;
+  const bool narrow = RE <= 4 || (uint32_t)RE * 8u - a.rshift <= 64u;
+  const uint64_t WB = a.window_bytes;
   __shared__ uint64_t s_warp[kJoinThreads / 32];
   __shared__ uint64_t s_prefix;
-  __shared__ uint32_t s_tile;
+  __shared__ uint32_t s_tile[2];
   __shared__ uint64_t s_lo, s_hi;
   const uint32_t t = threadIdx.x;
   const uint64_t nl = a.d_nl ? min(a.nl, *a.d_nl) : a.nl;
   const uint64_t num_tiles = (nl + kFbTile - 1) / kFbTile;
   const KeyView<LE> L{a.left, nl, a.lshift};
   const KeyView<RE> R{a.right, a.nr, a.rshift};
-  while (true) {
-    if (t == 0) s_tile = atomicAdd(a.tile_counter, 1u);
+  // tiles are claimed one ahead, so the claim's round trip overlaps the current tile; a
+  // claimed tile is always processed (its successors' look-backs wait for it)
+  if (t == 0) s_tile[0] = atomicAdd(a.tile_counter, 1u);
+  for (uint32_t it = 0;; ++it) {
     __syncthreads();
-    const uint64_t tile = s_tile;
+    const uint64_t tile = s_tile[it & 1];
     if (tile >= num_tiles) break;
+    if (t == 0) s_tile[(it + 1) & 1] = atomicAdd(a.tile_counter, 1u);
     const uint64_t tfirst = tile * kFbTile;
     const uint64_t tlast = min(tfirst + kFbTile, nl) - 1;
     // the window of right keys between the tile's smallest and largest left key
@@ -136,13 +145,14 @@ __global__ void __launch_bounds__(kJoinThreads) find_bounds_kernel(const FindBou
     }
     __syncthreads();
     const uint64_t wlo = s_lo, wn = s_hi > s_lo ? s_hi - s_lo : 0;
-    const bool staged = wn <= CAP;
-    if (staged) {
-      if (key64)
-        for (uint64_t x = t; x < wn; x += kJoinThreads) s_win64[x] = (uint64_t)R.key(wlo + x);
-      else
-        for (uint64_t x = t; x < wn; x += kJoinThreads) s_win128[x] = R.key(wlo + x);
-    }
+    const bool staged = wn * (narrow ? sizeof(W) : 16u) <= WB;
+    // a few loads in flight per thread while staging (one round trip per key otherwise)
+    if (staged && narrow)
+      block_stage<(sizeof(W) == 4 ? 8 : 4)>(wn, t, kJoinThreads, [&](uint64_t x) { return (W)R.key(wlo + x); },
+                                             [&](uint64_t x, W v) { s_win[x] = v; });
+    else if (staged)
+      block_stage<2>(wn, t, kJoinThreads, [&](uint64_t x) { return R.key(wlo + x); },
+                     [&](uint64_t x, u128 v) { s_win128[x] = v; });
     __syncthreads();
     const uint64_t first = tfirst + (uint64_t)t * kFbIPT;
     uint64_t lo[kFbIPT], cnt[kFbIPT];
@@ -166,18 +176,24 @@ __global__ void __launch_bounds__(kJoinThreads) find_bounds_kernel(const FindBou
         cnt[j] = phi - plo;
       } else {
         uint64_t l, h;
-        if (staged && key64) {
-          // 64-bit compares (a left key beyond 64 bits lies above the whole window)
-          if ((uint64_t)(k >> 64)) {
+        // the thread's keys ascend: the first is searched in the whole window, the next
+        // ones gallop forward from the previous key's upper bound
+        const uint32_t from = j == 0 ? 0u : (uint32_t)(phi - wlo);
+        if (staged && narrow) {
+          // compares in the window's type (a larger left key lies above the whole window)
+          if ((k >> (8 * sizeof(W))) != 0) {
             l = h = wlo + wn;
           } else {
-            const uint32_t l32 = smem_bound64<false>(s_win64, 0, (uint32_t)wn, (uint64_t)k);
-            l = wlo + l32;
-            h = wlo + smem_bound64<true>(s_win64, l32, (uint32_t)wn, (uint64_t)k);
+            const uint32_t lw = j == 0 ? smem_bound_t<false>(s_win, 0u, (uint32_t)wn, (W)k)
+                                       : smem_gallop_t<false>(s_win, from, (uint32_t)wn, (W)k);
+            l = wlo + lw;
+            h = wlo + smem_gallop_t<true>(s_win, lw, (uint32_t)wn, (W)k);
           }
         } else if (staged) {
-          l = wlo + smem_bound<u128>(s_win128, (uint32_t)wn, k, false);
-          h = wlo + smem_bound<u128>(s_win128, (uint32_t)wn, k, true);
+          const uint32_t lw = j == 0 ? smem_bound_t<false>(s_win128, 0u, (uint32_t)wn, k)
+                                     : smem_gallop_t<false>(s_win128, from, (uint32_t)wn, k);
+          l = wlo + lw;
+          h = wlo + smem_gallop_t<true>(s_win128, lw, (uint32_t)wn, k);
         } else {
           l = j == 0 ? bsearch<RE>(R, k, 0, a.nr, false) : gallop<RE>(R, k, phi, false);
           h = gallop<RE>(R, k, l, true);
@@ -215,7 +231,6 @@ __global__ void __launch_bounds__(kJoinThreads) find_bounds_kernel(const FindBou
         a.ocnt[run] = a.gcnt[i] * (uint32_t)cnt[j];
         ++run;
       }
-      __syncthreads();
       continue;
     }
 #pragma unroll
@@ -234,7 +249,6 @@ __global__ void __launch_bounds__(kJoinThreads) find_bounds_kernel(const FindBou
       if (a.off64) a.off64[i] = run;
       run += cnt[j];
     }
-    __syncthreads();
   }
   if (nl == 0 && blockIdx.x == 0 && t == 0) {
     *a.d_total = 0;
@@ -297,12 +311,13 @@ join_expand_kernel(int32_t* __restrict__ li, int32_t* __restrict__ ri, uint64_t 
     __syncthreads();
     const uint64_t i0 = s_i0, span = s_i1 - i0 + 1;
     const bool staged = span <= (uint64_t)kExpCap;
-    if (staged) {
-      for (uint64_t x = t; x < span; x += kJoinThreads) {
-        s_scan[x] = (uint32_t)__ldg(scan + i0 + x);
-        s_lb[x] = __ldg(lb + i0 + x);
-      }
-    }
+    if (staged)
+      block_stage<8>(span, t, kJoinThreads,
+                     [&](uint64_t x) { return make_int2(__ldg(scan + i0 + x), __ldg(lb + i0 + x)); },
+                     [&](uint64_t x, int2 v) {
+                       s_scan[x] = (uint32_t)v.x;
+                       s_lb[x] = v.y;
+                     });
     __syncthreads();
     for (int v = 0; v < kExpVT; ++v) {
       const uint64_t k = k0 + (uint64_t)v * kJoinThreads + t;
@@ -489,8 +504,13 @@ __global__ void __launch_bounds__(kJoinThreads) tuple_join_kernel(const TupleJoi
     const uint64_t i0 = s_i0, span = s_i1 - i0 + 1;
     const bool staged = span <= (uint64_t)kStageCap;
     if (staged) {
-      for (uint64_t x = t; x <= span; x += kJoinThreads) s_off[x] = __ldg(a.off64 + i0 + x);
-      for (uint64_t x = t; x < span; x += kJoinThreads) s_lb[x] = __ldg(a.lb64 + i0 + x);
+      block_stage<4>(span + 1, t, kJoinThreads,
+                     [&](uint64_t x) { return make_ulonglong2(__ldg(a.off64 + i0 + x),
+                                                              x < span ? __ldg(a.lb64 + i0 + x) : 0ull); },
+                     [&](uint64_t x, ulonglong2 v) {
+                       s_off[x] = v.x;
+                       if (x < span) s_lb[x] = v.y;
+                     });
       for (uint32_t x = t; x < (uint32_t)kExpTile; x += kJoinThreads) s_own[x] = 0;
     }
     __syncthreads();
@@ -645,8 +665,13 @@ __global__ void __launch_bounds__(kJoinThreads) tuple_join_staged_kernel(const T
       __syncthreads();
       continue;
     }
-    for (uint32_t x = t; x <= (uint32_t)span; x += kJoinThreads) s_off[x] = __ldg(a.off64 + i0 + x);
-    for (uint32_t x = t; x < (uint32_t)span; x += kJoinThreads) s_lb[x] = __ldg(a.lb64 + i0 + x);
+    block_stage<4>(span + 1, t, kJoinThreads,
+                   [&](uint64_t x) { return make_ulonglong2(__ldg(a.off64 + i0 + x),
+                                                            x < span ? __ldg(a.lb64 + i0 + x) : 0ull); },
+                   [&](uint64_t x, ulonglong2 v) {
+                     s_off[x] = v.x;
+                     if (x < span) s_lb[x] = v.y;
+                   });
     for (uint32_t x = t; x < (uint32_t)kExpTile; x += kJoinThreads) s_own[x] = 0;
     __syncthreads();
     // marks (each row's first output in the tile) and the right rows the tile touches

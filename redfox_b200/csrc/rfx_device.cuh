@@ -29,6 +29,29 @@ __device__ __forceinline__ void raise_error(uint32_t* err, uint32_t code) {
 // the back-off below); a healthy predecessor publishes within microseconds.
 constexpr uint32_t kSpinLimit = 1u << 22;
 
+// cp.async of one 16-byte chunk into shared memory; only `src_bytes` (<= 16) are read, the
+// rest of the chunk is zero-filled.
+__device__ __forceinline__ void cp_async16(void* dst, const void* src, uint32_t src_bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
+               "l"(src), "r"(src_bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
+// Up to `len` bytes of `src` from byte b0 (src + b0 16-byte aligned) into `dst`, block-
+// strided 16-byte chunks; nothing at or past byte `bend` (the end of the array) is read.
+__device__ __forceinline__ void block_prefetch16(uint8_t* dst, const uint8_t* src, uint64_t b0, uint64_t len,
+                                                 uint64_t bend, uint32_t nthreads) {
+  const uint64_t b1 = b0 + len < bend ? b0 + len : bend;
+  const uint32_t chunks = b1 > b0 ? (uint32_t)((b1 - b0 + 15) / 16) : 0u;
+  for (uint32_t c = threadIdx.x; c < chunks; c += nthreads) {
+    const uint64_t at = b0 + 16ull * c;
+    cp_async16(dst + 16u * c, src + at, (uint32_t)(bend - at < 16 ? bend - at : 16));
+  }
+}
+
 // ------------------------------------------------------------------ memory order
 __device__ __forceinline__ uint64_t ld_relaxed_u64(const uint64_t* p) {
   uint64_t v;

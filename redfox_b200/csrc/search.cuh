@@ -112,4 +112,25 @@ __device__ __forceinline__ uint64_t warp_search(const KeyView<E>& v, u128 k, uin
   return lo + __popc(__ballot_sync(0xffffffffu, before));
 }
 
+// Block-strided copy of items [0, n): thread t moves items t, t + nt, ... as st(x, ld(x)),
+// U loads in flight before their stores (a plain strided loop waits for each load in turn,
+// one memory round trip per item).
+template <int U, typename LD, typename ST>
+__device__ __forceinline__ void block_stage(uint64_t n, uint32_t t, uint32_t nt, LD ld, ST st) {
+  using V = decltype(ld(uint64_t(0)));
+  for (uint64_t x0 = t; x0 < n; x0 += (uint64_t)U * nt) {
+    V v[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const uint64_t x = x0 + (uint64_t)u * nt;
+      if (x < n) v[u] = ld(x);
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      const uint64_t x = x0 + (uint64_t)u * nt;
+      if (x < n) st(x, v[u]);
+    }
+  }
+}
+
 }  // namespace rfx

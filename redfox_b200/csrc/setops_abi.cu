@@ -15,6 +15,9 @@ struct FilterLayout {
   uint64_t* status;
   uint32_t* counter;
   uint64_t* split;   // 3 words per tile (filled by set_split_kernel)
+  uint8_t* mask;     // two-pass form: one bit per element
+  uint32_t* counts;  // two-pass form: kept elements per tile
+  uint64_t* offsets; // two-pass form: each tile's output offset
   size_t clear;
   size_t total;
 };
@@ -23,11 +26,15 @@ FilterLayout filter_layout(void* ws, uint64_t n) {
   FilterLayout L;
   Carver c(ws);
   const uint64_t tiles = (n + kSetTileMin - 1) / kSetTileMin + 1;
+  const uint64_t mark_tiles = (n + kMarkTile - 1) / kMarkTile + 1;
   L.status = c.take<uint64_t>(tiles);
   L.counter = c.take<uint32_t>(1);
   L.clear = align_up(c.used, 256);
   c.used = L.clear;
   L.split = c.take<uint64_t>(3 * tiles);
+  L.mask = c.take<uint8_t>(mark_tiles * kSetThreads);
+  L.counts = c.take<uint32_t>(mark_tiles);
+  L.offsets = c.take<uint64_t>(mark_tiles);
   L.total = align_up(c.used, 256);
   return L;
 }
@@ -53,27 +60,69 @@ rfx_status launch_filter_ipt(int mode, SetFilterArgs& a, cudaStream_t s) {
   return RFX_OK;
 }
 
-// Variant 0: 8 items per thread, 1: 4, 2: 16 (unique: always 8).  `clear` zeroes the look-back
-// status and tile counter before each launch.
-template <int E>
-rfx_status launch_filter(int mode, SetFilterArgs& a, cudaStream_t s, void* clear = nullptr, size_t clear_bytes = 0) {
-  auto run = [&](int v) -> rfx_status {
-    if (clear) RFX_CUDA_TRY(cudaMemsetAsync(clear, 0, clear_bytes, s));
-    if (v == 0 || mode == KEEP_HEADS) return launch_filter_ipt<E, 8>(mode, a, s);
-    return v == 1 ? launch_filter_ipt<E, 4>(mode, a, s) : launch_filter_ipt<E, 16>(mode, a, s);
-  };
-  if (mode == KEEP_HEADS || !clear) return run(0);
-  return run(tune_pick(TUNE_SET_FILTER, ((uint64_t)E << 8) | (uint64_t)mode, a.na + a.nb, 3, run, s));
+// The two-pass form: split entries, mark (keep bits and per-tile counts), offsets and the
+// total, compaction.  Needs no cleared workspace.
+template <int E, int IPT>
+rfx_status launch_two_pass(int mode, SetFilterArgs& a, const FilterLayout& L, cudaStream_t s) {
+  constexpr int TILE = kSetThreads * IPT;
+  const uint64_t tiles = (a.na + TILE - 1) / TILE;
+  if (tiles) {
+    const uint64_t work = 3 * tiles * 32;   // one warp per search
+    set_split_kernel<E, TILE><<<(int)((work + 255) / 256), 256, 0, s>>>(a.a, a.na, a.b, a.nb, L.split);
+    RFX_CUDA_TRY(cudaGetLastError());
+    a.split = L.split;
+    auto k = mode == KEEP_MATCHED ? set_mark_kernel<E, KEEP_MATCHED, IPT> : set_mark_kernel<E, KEEP_UNMATCHED, IPT>;
+    // the B window a tile is expected to need (nb / na per item, 1.25x, 512 more), at least
+    // 2048 elements and at most 48 KiB
+    typedef SetWord<E> WT;
+    double want = 1.25 * TILE * ((double)a.nb / (double)a.na) + 512.0;
+    if (want < 2048.0) want = 2048.0;
+    if (want * sizeof(WT) > 48.0 * 1024) want = 48.0 * 1024 / sizeof(WT);
+    a.wcap = (uint32_t)want;
+    const size_t smem = align_up((size_t)a.wcap * sizeof(WT), 16);
+    RFX_CUDA_TRY(allow_smem((const void*)k, smem));
+    const int grid = persistent_grid((const void*)k, kSetThreads, smem, tiles);
+    k<<<grid, kSetThreads, smem, s>>>(a, L.mask, L.counts);
+    RFX_CUDA_TRY(cudaGetLastError());
+  }
+  set_offsets_kernel<<<1, kOffsetThreads, 0, s>>>(L.counts, tiles, L.offsets, a.d_count);
+  RFX_CUDA_TRY(cudaGetLastError());
+  if (tiles) {
+    const int grid = persistent_grid((const void*)set_compact_kernel<E, IPT>, kSetThreads, 0, tiles);
+    set_compact_kernel<E, IPT><<<grid, kSetThreads, 0, s>>>(a.a, a.na, L.mask, L.offsets, a.out, a.na);
+    RFX_CUDA_TRY(cudaGetLastError());
+  }
+  return RFX_OK;
 }
 
-rfx_status dispatch_filter(uint32_t e, int mode, SetFilterArgs& a, cudaStream_t s, void* clear = nullptr,
-                           size_t clear_bytes = 0) {
+// Variants of intersection / difference / union's B - A: 0 the two-pass form with 8 items
+// per thread; 1, 2, 3 the one-pass form (decoupled look-back) with 8, 4 and 16 items per
+// thread; 4 the two-pass form with 16 items per thread.  Unique and
+// filters whose output overlaps A (in place) always take the one-pass form with 8 items
+// per thread.  The one-pass form's look-back status and tile counter are zeroed before
+// each launch.
+template <int E>
+rfx_status launch_filter(int mode, SetFilterArgs& a, cudaStream_t s, const FilterLayout* L, bool in_place) {
+  auto run = [&](int v) -> rfx_status {
+    if (v == 0 && L) return launch_two_pass<E, 8>(mode, a, *L, s);
+    if (v == 4 && L) return launch_two_pass<E, 16>(mode, a, *L, s);
+    if (L) RFX_CUDA_TRY(cudaMemsetAsync(L->status, 0, L->clear, s));
+    if (v <= 1 || mode == KEEP_HEADS) return launch_filter_ipt<E, 8>(mode, a, s);
+    return v == 2 ? launch_filter_ipt<E, 4>(mode, a, s) : launch_filter_ipt<E, 16>(mode, a, s);
+  };
+  if (mode == KEEP_HEADS || !L) return run(1);
+  if (in_place) return run(1);
+  return run(tune_pick(TUNE_SET_FILTER, ((uint64_t)E << 8) | (uint64_t)mode, a.na + a.nb, 5, run, s));
+}
+
+rfx_status dispatch_filter(uint32_t e, int mode, SetFilterArgs& a, cudaStream_t s, const FilterLayout* L = nullptr,
+                           bool in_place = false) {
   switch (e) {
-    case 1: return launch_filter<1>(mode, a, s, clear, clear_bytes);
-    case 2: return launch_filter<2>(mode, a, s, clear, clear_bytes);
-    case 4: return launch_filter<4>(mode, a, s, clear, clear_bytes);
-    case 8: return launch_filter<8>(mode, a, s, clear, clear_bytes);
-    case 16: return launch_filter<16>(mode, a, s, clear, clear_bytes);
+    case 1: return launch_filter<1>(mode, a, s, L, in_place);
+    case 2: return launch_filter<2>(mode, a, s, L, in_place);
+    case 4: return launch_filter<4>(mode, a, s, L, in_place);
+    case 8: return launch_filter<8>(mode, a, s, L, in_place);
+    case 16: return launch_filter<16>(mode, a, s, L, in_place);
     default: return RFX_ERR_UNSUPPORTED;
   }
 }
@@ -161,7 +210,7 @@ rfx_status set_op_impl(uint32_t op, void* out, uint64_t* d_count, const void* a,
     f.nb = na;
     f.out = L.diff;
     f.d_count = L.d_nd;
-    rfx_status st = dispatch_filter(e, KEEP_UNMATCHED, f, s, ws, L.f.clear);
+    rfx_status st = dispatch_filter(e, KEEP_UNMATCHED, f, s, &L.f);
     if (st != RFX_OK) return st;
     return dispatch_merge(e, a, na, L.diff, nb, L.d_nd, out, d_count, s);
   }
@@ -171,7 +220,11 @@ rfx_status set_op_impl(uint32_t op, void* out, uint64_t* d_count, const void* a,
   f.nb = nb;
   f.out = static_cast<uint8_t*>(out);
   f.d_count = d_count;
-  return dispatch_filter(e, op == RFX_SET_INTERSECTION ? KEEP_MATCHED : KEEP_UNMATCHED, f, s, ws, L.f.clear);
+  // an output overlapping A (in place) needs the one-pass form, whose writes never pass
+  // the inputs not yet read
+  const uintptr_t oa = reinterpret_cast<uintptr_t>(out), aa = reinterpret_cast<uintptr_t>(a);
+  const bool overlap = na && oa < aa + na * e && aa < oa + na * e;
+  return dispatch_filter(e, op == RFX_SET_INTERSECTION ? KEEP_MATCHED : KEEP_UNMATCHED, f, s, &L.f, overlap);
 }
 
 size_t unique_workspace_impl(uint64_t n, uint32_t e) {

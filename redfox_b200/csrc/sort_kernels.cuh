@@ -235,29 +235,12 @@ struct SortBuffers {
   static constexpr size_t SMEM = (size_t)(PF ? 2 : 1) * TILE * EB;
 };
 
-__device__ __forceinline__ void cp_async16(void* dst, const void* src, uint32_t src_bytes) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(dst))),
-               "l"(src), "r"(src_bytes)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
-
 // The raw keys of tile `tile` (tcount keys) into `dst`, in 16-byte chunks (the last one
 // zero-filled past the array).
 template <int K>
 __device__ __forceinline__ void sort_prefetch(uint8_t* dst, const uint8_t* keys, uint64_t tile, uint32_t tile_keys,
                                               uint64_t n) {
-  const uint64_t b0 = tile * (uint64_t)tile_keys * K;
-  const uint64_t bend = n * K;
-  const uint64_t b1 = b0 + (uint64_t)tile_keys * K < bend ? b0 + (uint64_t)tile_keys * K : bend;
-  const uint32_t chunks = (uint32_t)((b1 - b0 + 15) / 16);
-  for (uint32_t c = threadIdx.x; c < chunks; c += kSortThreads) {
-    const uint64_t src = b0 + 16ull * c;
-    const uint32_t bytes = (uint32_t)(bend - src < 16 ? bend - src : 16);
-    cp_async16(dst + 16u * c, keys + src, bytes);
-  }
+  block_prefetch16(dst, keys, tile * (uint64_t)tile_keys * K, (uint64_t)tile_keys * K, n * K, kSortThreads);
 }
 
 // The lanes of a warp whose digit equals this lane's (within `valid`): the intersection

@@ -364,18 +364,23 @@ class Server:
     """Request loop over resident relations.  A dispatcher admits arrived queries through a
     Scheduler (FIFO, budget) and packs the admitted queries into rounds of at most
     `max_batch`; up to `slots` worker threads each run a round on their own CUDA stream
-    (`run_round`) and complete its queries when its results are on the host.  With
-    plain=True every round is one query run by `run_query` (the serial plain baseline
-    when slots = 1).  Latency = host time from arrival to the result on the host."""
+    (`run_round`) and complete its queries when its results are on the host.  A round
+    starts beside one already running only when at least `concurrent_min` queries are
+    ready: two small rounds at once share the GPU and the host thread that launches them,
+    and both finish later than they would one after the other.  With plain=True every
+    round is one query run by `run_query` (the serial plain baseline when slots = 1).
+    Latency = host time from arrival to the result on the host."""
 
     # result bytes staged per query: (key, sum, count, query byte) for each of its groups,
     # at most one per D2 row and in practice below 3M
     STAGE_GROUPS_PER_QUERY = 3_000_000
 
-    def __init__(self, res, slots=2, budget_bytes=BUDGET_BYTES, device="cuda", max_batch=64, plain=False):
+    def __init__(self, res, slots=2, budget_bytes=BUDGET_BYTES, device="cuda", max_batch=64, plain=False,
+                 concurrent_min=8):
         import torch
         self.res = res
         self.slots = slots
+        self.concurrent_min = concurrent_min
         self.budget = budget_bytes
         self.plain = plain
         self.max_batch = 1 if plain else max(1, min(256, max_batch))
@@ -406,7 +411,8 @@ class Server:
         busy = [False] * self.slots
         stop = [False]
         errors = []
-        self.rounds = []
+        self.rounds = []                    # queries per round, in start order
+        self.round_log = []                 # (queries, start s, end s) per round, in end order
         t0 = time.perf_counter()
 
         def worker(i):
@@ -427,6 +433,7 @@ class Server:
                         errors.append(([q.qid for q in rnd], repr(e)))
                     done = time.perf_counter() - t0
                     with cv:
+                        self.round_log.append((len(rnd), rnd[0].start, done))
                         for q in rnd:
                             q.done = done
                             sch.complete(q)
@@ -448,7 +455,7 @@ class Server:
                 for q, _slot in sch.admissions():
                     ready.append(q)
                 for i in range(self.slots):
-                    if not ready:
+                    if not ready or (any(busy) and len(ready) < self.concurrent_min):
                         break
                     if not busy[i]:
                         rnd = [ready.popleft() for _ in range(min(self.max_batch, len(ready)))]

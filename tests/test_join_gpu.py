@@ -93,6 +93,32 @@ def test_fused_tuple_join(cuda, lw, lvb, rw, rvb, ow):
     assert np.array_equal(to_np(got), exp)
 
 
+def test_find_bounds_window_forms(cuda):
+    """The right-key window of each left tile: a window far larger than shared memory (few
+    left keys against millions of right keys: global-memory searches), a tiny right side
+    (the smallest window), and left keys wider than the 4-byte right keys (those above
+    2^32 match nothing)."""
+    rng = np.random.default_rng(31)
+    for nl, nr, hi in ((3000, 2_000_000, 1000), (2_000_000, 3000, 5000)):
+        left = np.sort(rng.integers(0, hi, nl)).astype(np.uint32)
+        right = np.sort(rng.integers(0, hi, nr)).astype(np.uint32)
+        lb, sc, total = R.find_bounds(_dev(left, cuda), _dev(right, cuda))
+        elb, esc, etot = O.find_bounds(left, right)
+        assert total == etot
+        assert np.array_equal(to_np(lb), elb) and np.array_equal(to_np(sc), esc)
+    nl, nr = 40000, 60000
+    lk = np.sort(np.concatenate([rng.integers(0, 1 << 20, nl // 2), rng.integers(1 << 24, 1 << 34, nl // 4),
+                                 rng.integers(1 << 38, 1 << 40, nl - nl // 2 - nl // 4)])).astype(np.uint64)
+    rk = np.sort(rng.integers(0, 1 << 20, nr)).astype(np.uint64)
+    left = O.pack([40, 24], [lk, rng.integers(0, 1 << 24, nl, dtype=np.uint64)])
+    right = O.pack([24, 8], [rk, rng.integers(0, 256, nr, dtype=np.uint64)])
+    assert left.shape[1] == 8 and right.shape[1] == 4
+    got, total = R.join_tuples(_dev(left, cuda), 24, _dev(right, cuda), 8, 8)
+    exp = O.join_tuples(left, 24, right, 8, 8)
+    assert total == len(exp) > 0
+    assert np.array_equal(to_np(got), exp)
+
+
 def test_fused_join_capacity_and_skew(cuda):
     """A Zipf-skewed key with ~1M matches; a short capacity writes a prefix and reports the total."""
     n = 200000

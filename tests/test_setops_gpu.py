@@ -107,12 +107,13 @@ def test_reference_compatible_set_entries(cuda):
                                       P(db.data_ptr()), P(db.data_ptr()), 99) == R.ERR_UNSUPPORTED
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
 @pytest.mark.parametrize("dtype", [np.uint32, np.uint64])
 def test_set_filter_variants(cuda, variant, dtype):
-    """Each items-per-thread variant of the set filters (pinned through the tuner) gives the
-    STL results, across tile boundaries of every variant (1024 / 2048 / 4096 elements) and
-    with runs of equal values that cross tiles."""
+    """The two-pass form (variants 0 and 4: 8 and 16 items per thread) and each items-per-
+    thread variant of the one-pass form (pinned through the tuner) give the STL results,
+    across tile boundaries of every variant (1024 / 2048 / 4096 elements) and with runs of
+    equal values that cross tiles."""
     try:
         R.tune_force(2, variant)
         rng = np.random.default_rng(variant * 10 + np.dtype(dtype).itemsize)
@@ -126,3 +127,25 @@ def test_set_filter_variants(cuda, variant, dtype):
         assert R.device_status() == R.OK
     finally:
         R.tune_force(2, -1)
+
+
+@pytest.mark.parametrize("op", ["intersection", "difference"])
+def test_set_filter_in_place(cuda, op):
+    """Intersection and difference written over A itself (the output overlaps the input)
+    take the one-pass form, whose writes never pass inputs not yet read: the result is the
+    oracle's, across many tiles."""
+    import torch
+    rng = np.random.default_rng(7)
+    na, nb, hi = 300_001, 120_007, 90_000
+    a = np.sort(rng.integers(0, hi, na)).astype(np.uint32)
+    b = np.sort(rng.integers(0, hi, nb)).astype(np.uint32)
+    da, db = _dev(a, cuda), _dev(b, cuda)
+    cnt = torch.zeros(1, dtype=torch.int64, device=cuda)
+    code = R.SET_INTERSECTION if op == "intersection" else R.SET_DIFFERENCE
+    wsb = R.LIB.rfx_set_op_workspace(code, na, nb, 4)
+    ws = torch.empty(wsb, dtype=torch.uint8, device=cuda)
+    R.check("set", R.LIB.rfx_set_op(code, R._ptr(da), R._ptr(cnt), R._ptr(da), na, R._ptr(db), nb, 4, R._ptr(ws),
+                                    wsb, R._stream()))
+    exp = getattr(O, "set_" + op)(a, b)
+    assert int(cnt.item()) == len(exp)
+    assert np.array_equal(to_np(da)[:len(exp)], exp)

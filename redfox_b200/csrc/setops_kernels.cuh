@@ -113,9 +113,13 @@ __device__ __forceinline__ void set_keep_flags(const SetFilterArgs& p, uint64_t 
   const uint32_t tcount = (uint32_t)min((uint64_t)TILE, p.na - tfirst);
   const uint32_t l0 = t * IPT;
   const uint64_t bn = bhi > blo0 ? bhi - blo0 : 0;
-  const bool staged = bn <= (uint64_t)wcap;
-  if (staged)
+  // staged windows keep one slot for a sentinel (the largest value) after their last element,
+  // so the merge walk below needs no bounds check
+  const bool staged = bn < (uint64_t)wcap;
+  if (staged) {
     for (uint32_t x = t; x < (uint32_t)bn; x += kSetThreads) s_b[x] = (WT)B.key(blo0 + x);
+    if (t == 0) s_b[bn] = ~(WT)0;
+  }
   // heads of this thread's items (local index of its last head, or -1); the tile's first
   // item continues the previous tile's run unless it is the array's first
   int32_t last_head = -1;
@@ -157,8 +161,12 @@ __device__ __forceinline__ void set_keep_flags(const SetFilterArgs& p, uint64_t 
     if ((heads >> j) & 1u) run_start = li;
     uint64_t nbeq;
     if (staged) {
+      // usually zero or one step: two without a branch, then a loop for the rest (the
+      // sentinel stops it at bn)
       uint32_t q = (uint32_t)pos;
-      while (q < (uint32_t)bn && s_b[q] < v[j]) ++q;
+      q += s_b[q] < v[j] ? 1u : 0u;
+      q += s_b[q] < v[j] ? 1u : 0u;
+      while (s_b[q] < v[j]) ++q;
       pos = q;
       nbeq = 0;
       if (q < (uint32_t)bn && s_b[q] == v[j]) {

@@ -118,21 +118,21 @@ __global__ void __launch_bounds__(kJoinThreads) find_bounds_kernel(const FindBou
   const uint64_t WB = a.window_bytes;
   __shared__ uint64_t s_warp[kJoinThreads / 32];
   __shared__ uint64_t s_prefix;
-  __shared__ uint32_t s_tile[2];
+  __shared__ uint32_t s_tile;
   __shared__ uint64_t s_lo, s_hi;
   const uint32_t t = threadIdx.x;
   const uint64_t nl = a.d_nl ? min(a.nl, *a.d_nl) : a.nl;
   const uint64_t num_tiles = (nl + kFbTile - 1) / kFbTile;
   const KeyView<LE> L{a.left, nl, a.lshift};
   const KeyView<RE> R{a.right, a.nr, a.rshift};
-  // tiles are claimed one ahead, so the claim's round trip overlaps the current tile; a
-  // claimed tile is always processed (its successors' look-backs wait for it)
-  if (t == 0) s_tile[0] = atomicAdd(a.tile_counter, 1u);
-  for (uint32_t it = 0;; ++it) {
+  // a tile is claimed when the block is ready for it (claiming one ahead measured slower:
+  // a claimed tile's successors wait in their look-back until its block gets to it)
+  while (true) {
     __syncthreads();
-    const uint64_t tile = s_tile[it & 1];
+    if (t == 0) s_tile = atomicAdd(a.tile_counter, 1u);
+    __syncthreads();
+    const uint64_t tile = s_tile;
     if (tile >= num_tiles) break;
-    if (t == 0) s_tile[(it + 1) & 1] = atomicAdd(a.tile_counter, 1u);
     const uint64_t tfirst = tile * kFbTile;
     const uint64_t tlast = min(tfirst + kFbTile, nl) - 1;
     // the window of right keys between the tile's smallest and largest left key

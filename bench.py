@@ -861,10 +861,10 @@ def serving_benchmark(dev, nq, rates=(100.0, 300.0, 1000.0, 3000.0, 5000.0), slo
     servers = (("serial", S.Server(res, slots=1, device=dev, plain=True)),
                ("serving", S.Server(res, slots=slots, device=dev)))   # pinned result buffers made once
     for _, srv in servers:
-        # untimed: a burst that fills the largest rounds on every slot, and a few spaced
-        # queries (rounds of one), so each server's streams have their memory pools and
-        # kernels before the timed runs
-        srv.serve(S.gen_requests(max(8, 2 * srv.max_batch * srv.slots), 1e6, seed=S.SERVING_SEED + 98))
+        # untimed, the same for both servers: a burst that fills the largest rounds on every
+        # slot, and a few spaced queries (rounds of one), so each server's streams have their
+        # memory pools and kernels before the timed runs
+        srv.serve(S.gen_requests(2 * 64 * slots, 1e6, seed=S.SERVING_SEED + 98))
         srv.serve(S.gen_requests(2 * slots, 200.0, seed=S.SERVING_SEED + 97))
     for rate in rates:
         line = {}

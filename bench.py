@@ -433,7 +433,8 @@ def _op_select(ctx, peak, reps):
     sel()
     ms = _time_ms(sel, reps)
     k = int(cnt.item())
-    return {"select_fact_60M": _op_line(n, n * 64 + k * 64, ms, peak, kept=k)}
+    tag = "%dM" % (n // 1_000_000) if n % 1_000_000 == 0 else str(n)
+    return {"select_fact_%s" % tag: _op_line(n, n * 64 + k * 64, ms, peak, kept=k)}
 
 
 def _sort_line(src, kb, begin, end, reps, peak, flags=0, note=None, passes=None):
@@ -543,6 +544,16 @@ def _op_join(ctx, peak, reps):
                                                                 rwsb, R._stream())), reps)
     groups = int(g.item())
     ops["reduce_by_key_19M_rows"] = _op_line(total, total * 16 + groups * 16, ms, peak, groups=groups)
+    # the same with the earlier design: a look-back per 32 KB tile (the tuner's variant 2)
+    R.tune_force(1, 2)
+    try:
+        ms = _time_ms(lambda: R.check("rt", R.LIB.rfx_reduce_tuples(R._ptr(jout), total, None, 16, 96, 0, 64,
+                                                                    R._ptr(okeys), 4, R._ptr(osum), R._ptr(ocnt),
+                                                                    R._ptr(g), R._ptr(rws), rwsb, R._stream())), reps)
+    finally:
+        R.tune_force(1, -1)
+    ops["reduce_by_key_19M_rows_tile_lookback"] = _op_line(total, total * 16 + groups * 16, ms, peak, groups=groups,
+                                                           note="look-back per 256-line tile (tuner variant 2)")
     # join + aggregate on the key as one operator (no join rows)
     ja = R.JoinAggregate(nr, 4, device=ctx.dev)
     ms = _time_ms(lambda: ja(rs, 32, ss, 64, 0, 64), reps)

@@ -602,9 +602,36 @@ def _op_setops(ctx, peak, reps):
     return ops
 
 
+PIPELINE_CPU_LEGS = True   # --no-cpu-baseline turns the pipelines' CPU legs off
+
+
+def _pipeline_cpu_leg(fn, args, nin, steps=5, warmup=1):
+    """The oracle's restatement of a plan (oracle/pipelines.py) on the host copies of the
+    same inputs: all host threads (median of `steps` after `warmup`; the sorts use the
+    threads, the other steps one), then one 1-thread run; also returns the result."""
+    threads = cpu_threads()
+    ts, res = [], None
+    for i in range(warmup + steps):
+        t0 = time.perf_counter()
+        res = fn(*args, threads=threads)
+        if i >= warmup:
+            ts.append(time.perf_counter() - t0)
+    t0 = time.perf_counter()
+    fn(*args, threads=1)
+    t1 = time.perf_counter() - t0
+    med = statistics.median(ts)
+    return {"value": nin / med, "unit": "tuples/s", "cores": threads, "kind": "port", "median_s": med,
+            "sample": "the whole workload, C oracle (sorts on every host thread), median of %d after %d warm-up"
+                      % (steps, warmup),
+            "one_core": {"value": nin / t1, "unit": "tuples/s", "cores": 1, "seconds": t1}}, res
+
+
 def _op_pipelines(ctx, peak, reps):
-    """The plans end to end (host reads sizes back between steps, as the reference); one
-    untimed run first compiles the plan-specialised kernels."""
+    """The plans end to end (host reads sizes back between steps, as the reference): one
+    untimed run first compiles the plan-specialised kernels, then the median of 5 timed
+    runs (wall clock).  With PIPELINE_CPU_LEGS each plan also runs on the host through the
+    oracle's restatement, timed and compared with the GPU result."""
+    import numpy as np
     import torch
 
     from redfox_b200 import plans as PL
@@ -613,6 +640,7 @@ def _op_pipelines(ctx, peak, reps):
     ops = {}
     nin0 = r.shape[0] + s.shape[0]
     nin2 = d1.shape[0] + d2.shape[0] + f.shape[0]
+    results = {}
     for name, fn, nin, note in (
             ("pipeline_join_aggregate_1Mx4M", lambda: PL.join_aggregate(r, s), nin0,
              "sort R, sort S, join (19.3M rows written), reduce; wall clock incl. size reads"),
@@ -620,13 +648,33 @@ def _op_pipelines(ctx, peak, reps):
              "sort R, sort S, join-aggregate on the key (no join rows); wall clock incl. the group count read"),
             ("pipeline_three_relation_76M", lambda: PL.three_relation(d1, d2, f, l5, l2), nin2,
              "selects, sort, 2 joins, set ops, sort of F, reduce; wall clock")):
-        fn()
+        results[name] = fn()
         torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        fn()
-        torch.cuda.synchronize()
-        ms = (time.perf_counter() - t0) * 1e3
-        ops[name] = {"tuples": nin, "ms": ms, "tuples_per_s": nin / (ms / 1e3), "note": note}
+        ts = []
+        for _ in range(5):
+            t0 = time.perf_counter()
+            fn()
+            torch.cuda.synchronize()
+            ts.append((time.perf_counter() - t0) * 1e3)
+        ms = statistics.median(ts)
+        ops[name] = {"tuples": nin, "ms": ms, "tuples_per_s": nin / (ms / 1e3), "note": note + ", median of 5"}
+    if PIPELINE_CPU_LEGS:
+        from oracle import pipelines as OP
+
+        def host(t):
+            return t.cpu().numpy()
+        leg, (ek, es, ec, _) = _pipeline_cpu_leg(OP.join_aggregate_plan, (host(r), host(s)), nin0)
+        gk, gs, gc = (host(x) for x in results["pipeline_join_aggregate_fused_1Mx4M"][:3])
+        leg["parity"] = "ok" if (np.array_equal(gk.view(np.uint32), ek) and np.array_equal(gs, es) and
+                                 np.array_equal(gc.view(np.uint32), ec.astype(np.uint32))) else "MISMATCH"
+        ops["pipeline_join_aggregate_1Mx4M"]["cpu"] = leg
+        leg, (ek, es, ec) = _pipeline_cpu_leg(
+            OP.three_relation_plan, (host(d1), host(d2), host(f), host(l5), host(l2), PL.C2_SEGMENT, PL.C2_DATE_LO,
+                                     PL.C2_DATE_HI), nin2)
+        gk, gs, gc = (host(x) for x in results["pipeline_three_relation_76M"])
+        leg["parity"] = "ok" if (np.array_equal(gk.view(np.uint32), ek) and np.array_equal(gs, es) and
+                                 np.array_equal(gc.view(np.uint32), ec.astype(np.uint32))) else "MISMATCH"
+        ops["pipeline_three_relation_76M"]["cpu"] = leg
     return ops
 
 
@@ -1057,6 +1105,8 @@ def main_ours(args):
         }
         if world == 1 and not args.no_operators:
             del dev_in_keep
+            global PIPELINE_CPU_LEGS
+            PIPELINE_CPU_LEGS = not args.no_cpu_baseline
             result["operators"] = operator_benchmarks(dev, rows, peak)
             result["tuning"] = tuning_benchmark(dev, rows)
         if world == 1:
@@ -1082,8 +1132,9 @@ def main_only(args):
 
     from redfox_b200 import rfx as R
     from redfox_b200 import workloads as WL
-    global SORT_ROWS
+    global SORT_ROWS, PIPELINE_CPU_LEGS
     SORT_ROWS = args.sort_rows
+    PIPELINE_CPU_LEGS = not args.no_cpu_baseline
     dev = torch.device("cuda:0")
     peak = measured_peak_hbm()[0]
     only = [x for x in args.only.split(",") if x]

@@ -48,15 +48,8 @@ def join_aggregate_oracle_data(nr, ns, key_domain):
 
 
 def join_aggregate_oracle(r, s):
-    rs = O.sort_pairs(r, begin_bit=32, end_bit=64, threads=THREADS)
-    ss = O.sort_pairs(s, begin_bit=64, end_bit=96, threads=THREADS)
-    out = O.join_tuples(rs, 32, ss, 64, 16)
-    limbs = out.view(np.uint64)
-    key = (limbs[:, 1] >> np.uint64(32)).astype(np.uint32)
-    amt = limbs[:, 0].astype(np.int64)
-    k, sums = O.reduce_sum_i64(key, amt)
-    _, counts = O.reduce_count(key)
-    return k, sums, counts, len(out)
+    from oracle import pipelines as OP
+    return OP.join_aggregate_plan(r, s, threads=THREADS)
 
 
 def three_relation_oracle_data(n1, n2, n3, l5, l2):
@@ -76,24 +69,10 @@ def three_relation_oracle_data(n1, n2, n3, l5, l2):
 
 
 def three_relation_oracle(d1, d2, f, list_in, list_out):
+    from oracle import pipelines as OP
     from redfox_b200 import plans as PL
-    d1s = O.select(d1, [32, 8], oracle_cmps([(O.EQ, (O.OPND_VAR, 1), (O.OPND_CONST, PL.C2_SEGMENT), O.I8)]))
-    d2f = O.select(d2, [32, 32, 32], oracle_cmps([(O.GE, (O.OPND_VAR, 2), (O.OPND_CONST, PL.C2_DATE_LO), O.I32),
-                                                  (O.LT, (O.OPND_VAR, 2), (O.OPND_CONST, PL.C2_DATE_HI), O.I32)]))
-    d2s = O.project(d2f, [32, 32, 32], [32, 32], [1, 0])
-    d2s = O.sort_pairs(d2s, begin_bit=32, end_bit=64, threads=THREADS)
-    j1 = O.join_tuples(d1s, 8, d2s, 32, 16)
-    keys = O.project(j1, [32, 8, 32], [32], [2]).view(np.uint32).ravel()
-    keys = O.sort_pairs(keys, threads=THREADS)
-    keys = O.set_difference(O.set_intersection(keys, list_in), list_out)
-    fs = O.sort_pairs(f, begin_bit=64, end_bit=96, threads=THREADS)
-    j2 = O.join_tuples(keys.view(np.uint8).reshape(-1, 4), 0, fs, 64, 16)
-    limbs = j2.view(np.uint64)
-    key = limbs[:, 1].astype(np.uint32)
-    amt = limbs[:, 0].astype(np.int64)
-    k, sums = O.reduce_sum_i64(key, amt)
-    _, counts = O.reduce_count(key)
-    return k, sums, counts
+    return OP.three_relation_plan(d1, d2, f, list_in, list_out, PL.C2_SEGMENT, PL.C2_DATE_LO, PL.C2_DATE_HI,
+                                  threads=THREADS)
 
 
 def serving_query_oracle(d1, d2, f, segment, date_lo, date_hi, keys_list=None):

@@ -376,10 +376,15 @@ sort_pass_kernel(const SortPassArgs a) {
         uint32_t spins = 0;
         while (base >= 0) {
           uint32_t w[kSortLookWindow];
+          // predecessor base - r sits r * kRadix words below base's word: constant offsets
+          // from one pointer (a window reaching past tile 0 reads "inclusive 0" there)
+          const uint32_t* pb = a.status + (uint64_t)base * kRadix + t;
+          if (base >= kSortLookWindow - 1) {
 #pragma unroll
-          for (int r = 0; r < kSortLookWindow; ++r) {
-            const int64_t idx = base - r;
-            w[r] = idx >= 0 ? ld_relaxed_u32(a.status + (uint64_t)idx * kRadix + t) : kSFlagInc;
+            for (int r = 0; r < kSortLookWindow; ++r) w[r] = ld_relaxed_u32(pb - r * kRadix);
+          } else {
+#pragma unroll
+            for (int r = 0; r < kSortLookWindow; ++r) w[r] = r <= base ? ld_relaxed_u32(pb - r * kRadix) : kSFlagInc;
           }
           int r_inc = kSortLookWindow;
 #pragma unroll

@@ -18,7 +18,7 @@ constexpr int kSortThreads = 256;
 constexpr int kRadix = 256;
 constexpr int kSortWarps = kSortThreads / 32;
 constexpr int kMaxSortPasses = 16;  // up to 128 key bits per call
-constexpr int kSortLookWindow = 16;  // predecessors examined per look-back round trip
+constexpr int kSortLookWindow = 8;  // predecessors examined per look-back round trip
 
 // Items per thread by the bytes moved per item: tiles of 24-48 KB (as large as 128
 // registers allow without spills), so the per-tile fixed costs (barriers, the look-back)

@@ -313,18 +313,38 @@ sort_pass_kernel(const SortPassArgs a) {
       const uint32_t li = wbase + j * 32 + lane;
       if (li < tcount) key[j] = pf ? load_elem<K>(stage, li) : load_elem<K>(a.keys_in, tbase + li);
     }
+    // the lanes of a warp whose key has this lane's digit: every key's bit goes into its
+    // digit's mask with one shared-memory atomic OR (the warp's 256 masks sit in the tile
+    // buffer, which is free from here until the scatter: every key is in registers), or the
+    // hardware match in the MATCH variant
+    uint32_t* s_peer = reinterpret_cast<uint32_t*>(stage) + warp * kRadix;
+    if constexpr (!MATCH) {
+      __syncthreads();   // all warps hold their keys
+      for (uint32_t k = lane; k < kRadix; k += 32) s_peer[k] = 0u;
+      __syncwarp();
+    }
 #pragma unroll
     for (int j = 0; j < IPT; ++j) {
       const uint32_t li = wbase + j * 32 + lane;
       const bool valid = li < tcount;
       const uint32_t d = valid ? (elem_bits<K>(key[j], a.shift) & a.mask) : 0u;
-      const unsigned peers = digit_peers<MATCH>(d, valid, dbits);
+      unsigned peers;
+      if constexpr (MATCH) {
+        peers = digit_peers<true>(d, valid, dbits);
+      } else {
+        if (valid) atomicOr(&s_peer[d], 1u << lane);
+        __syncwarp();
+        peers = valid ? s_peer[d] : 0u;
+      }
       const unsigned lower = peers & ((1u << lane) - 1);
       uint32_t base = 0;
       if (valid) base = whist[warp][d];
       rank[j] = (base + __popc(lower)) | (d << 16);   // the digit rides along: extracted once
       __syncwarp();
-      if (valid && lower == 0) whist[warp][d] = base + __popc(peers);
+      if (valid && lower == 0) {
+        whist[warp][d] = base + __popc(peers);
+        if constexpr (!MATCH) s_peer[d] = 0u;   // cleared for the next key by its group's first lane
+      }
       __syncwarp();
     }
     __syncthreads();

@@ -14,7 +14,7 @@
 
 namespace rfx {
 
-constexpr int kSortThreads = 256;
+constexpr int kSortThreads = 256;   // the histogram pass
 constexpr int kRadix = 256;
 constexpr int kSortWarps = kSortThreads / 32;
 constexpr int kMaxSortPasses = 16;  // up to 128 key bits per call
@@ -26,8 +26,12 @@ constexpr int kSortLookWindow = 8;  // predecessors examined per look-back round
 template <int K, int V>
 struct SortTuning {
   static constexpr int B = K + V;
-  static constexpr int IPT = B <= 4 ? 24 : B <= 8 ? 20 : B <= 16 ? 12 : B <= 32 ? 8 : B <= 64 ? 4 : 2;
-  static constexpr int TILE = kSortThreads * IPT;
+  // a digit pass: 8 warps per block for elements up to 8 bytes, 12 above (two blocks per SM
+  // either way; the larger elements' passes gain from the extra warps, the smaller lose)
+  static constexpr int THREADS = B <= 8 ? 256 : 384;
+  static constexpr int WARPS = THREADS / 32;
+  static constexpr int IPT = B <= 4 ? 24 : B <= 8 ? 20 : B <= 16 ? 8 : B <= 32 ? 5 : B <= 64 ? 3 : 1;
+  static constexpr int TILE = THREADS * IPT;
   static constexpr int SBYTES = (K > V ? K : V);
 };
 
@@ -239,8 +243,8 @@ struct SortBuffers {
 // zero-filled past the array).
 template <int K>
 __device__ __forceinline__ void sort_prefetch(uint8_t* dst, const uint8_t* keys, uint64_t tile, uint32_t tile_keys,
-                                              uint64_t n) {
-  block_prefetch16(dst, keys, tile * (uint64_t)tile_keys * K, (uint64_t)tile_keys * K, n * K, kSortThreads);
+                                              uint64_t n, uint32_t nthreads) {
+  block_prefetch16(dst, keys, tile * (uint64_t)tile_keys * K, (uint64_t)tile_keys * K, n * K, nthreads);
 }
 
 // The lanes of a warp whose digit equals this lane's (within `valid`): the intersection
@@ -266,18 +270,18 @@ __device__ __forceinline__ unsigned digit_peers(uint32_t d, bool valid, uint32_t
 }
 
 template <int K, int V, bool MATCH = false>
-__global__ void __launch_bounds__(kSortThreads, 2)
+__global__ void __launch_bounds__((SortTuning<K, V>::THREADS), 2)
 sort_pass_kernel(const SortPassArgs a) {
   using T = SortTuning<K, V>;
   using SB = SortBuffers<K, V>;
   constexpr int IPT = T::IPT;
   constexpr int TILE = T::TILE;
   extern __shared__ __align__(16) uint8_t sbuf[];              // 1 or 2 buffers of TILE * EB
-  __shared__ uint32_t whist[kSortWarps][kRadix];               // per-warp digit counts
+  __shared__ uint16_t whist[T::WARPS][kRadix];               // per-warp digit counts (a tile's fit 16 bits)
   __shared__ uint32_t s_local[kRadix];                         // tile-local digit start
   __shared__ unsigned long long s_gb[kRadix];                  // output index of slot i = s_gb[digit] + i
   __shared__ uint8_t s_dig[TILE];                              // digit of each sorted slot
-  __shared__ uint32_t s_scan[kSortWarps];
+  __shared__ uint32_t s_scan[T::WARPS];
   __shared__ uint32_t s_tile[2];
   const uint32_t t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const uint64_t num_tiles = (a.n + TILE - 1) / TILE;
@@ -285,19 +289,19 @@ sort_pass_kernel(const SortPassArgs a) {
   const uint32_t dbits = 32 - __clz(a.mask);   // bits in this pass's digit (ballots needed)
   if (t == 0) s_tile[0] = atomicAdd(a.tile_counter, 1u);
   __syncthreads();
-  if (pf && s_tile[0] < num_tiles) sort_prefetch<K>(sbuf, a.keys_in, s_tile[0], TILE, a.n);
+  if (pf && s_tile[0] < num_tiles) sort_prefetch<K>(sbuf, a.keys_in, s_tile[0], TILE, a.n, T::THREADS);
   cp_async_commit();
 
   for (uint32_t it = 0;; ++it) {
     const uint64_t tile = s_tile[it & 1];
     uint8_t* stage = sbuf + (pf ? (size_t)(it & 1) * TILE * SB::EB : 0);
     if (t == 0) s_tile[(it + 1) & 1] = atomicAdd(a.tile_counter, 1u);   // the next tile, one ahead
-    for (uint32_t k = t; k < kSortWarps * kRadix; k += kSortThreads) (&whist[0][0])[k] = 0;
+    for (uint32_t k = t; k < T::WARPS * kRadix / 2; k += T::THREADS) reinterpret_cast<uint32_t*>(&whist[0][0])[k] = 0;
     __syncthreads();
     if (tile >= num_tiles) break;   // the tile claimed next is larger still: no copy in flight
     const uint64_t next = s_tile[(it + 1) & 1];
     if (pf) {
-      if (next < num_tiles) sort_prefetch<K>(sbuf + (size_t)((it + 1) & 1) * TILE * SB::EB, a.keys_in, next, TILE, a.n);
+      if (next < num_tiles) sort_prefetch<K>(sbuf + (size_t)((it + 1) & 1) * TILE * SB::EB, a.keys_in, next, TILE, a.n, T::THREADS);
       cp_async_commit();
       cp_async_wait<1>();          // this tile's copy (the next one may stay in flight)
       __syncthreads();
@@ -342,7 +346,7 @@ sort_pass_kernel(const SortPassArgs a) {
       rank[j] = (base + __popc(lower)) | (d << 16);   // the digit rides along: extracted once
       __syncwarp();
       if (valid && lower == 0) {
-        whist[warp][d] = base + __popc(peers);
+        whist[warp][d] = (uint16_t)(base + __popc(peers));
         if constexpr (!MATCH) s_peer[d] = 0u;   // cleared for the next key by its group's first lane
       }
       __syncwarp();
@@ -352,9 +356,9 @@ sort_pass_kernel(const SortPassArgs a) {
     uint32_t count = 0;
     if (t < kRadix) {
 #pragma unroll
-      for (int w = 0; w < kSortWarps; ++w) {
+      for (int w = 0; w < T::WARPS; ++w) {
         const uint32_t c = whist[w][t];
-        whist[w][t] = count;
+        whist[w][t] = (uint16_t)count;
         count += c;
       }
       st_relaxed_u32(a.status + tile * kRadix + t, (tile == 0 ? kSFlagInc : kSFlagAgg) | count);
@@ -437,7 +441,7 @@ sort_pass_kernel(const SortPassArgs a) {
       s_gb[t] = (unsigned long long)a.gexcl[t] + prefix - s_local[t];
     }
     __syncthreads();
-    for (uint32_t i = t; i < tcount; i += kSortThreads) {
+    for (uint32_t i = t; i < tcount; i += T::THREADS) {
       const uint64_t pos = s_gb[s_dig[i]] + i;
       if (pos < a.n) store_elem<K>(a.keys_out, pos, skeys[i]);
     }
@@ -453,7 +457,7 @@ sort_pass_kernel(const SortPassArgs a) {
         }
       }
       __syncthreads();
-      for (uint32_t i = t; i < tcount; i += kSortThreads) {
+      for (uint32_t i = t; i < tcount; i += T::THREADS) {
         const uint64_t pos = s_gb[s_dig[i]] + i;
         if (pos < a.n) store_elem<V>(a.vals_out, pos, svals[i]);
       }

@@ -79,7 +79,7 @@ rfx_status run_sort_kv(SortPlan& s) {
   RFX_CUDA_TRY(allow_smem((const void*)sort_pass_kernel<K, V>, tile_smem));
   if constexpr (V == 0 && (K == 4 || K == 8 || K == 16))
     RFX_CUDA_TRY(allow_smem((const void*)sort_pass_kernel<K, V, true>, tile_smem));
-  const int tile_grid = persistent_grid((const void*)sort_pass_kernel<K, V>, kSortThreads, tile_smem,
+  const int tile_grid = persistent_grid((const void*)sort_pass_kernel<K, V>, SortTuning<K, V>::THREADS, tile_smem,
                                         s.tiles ? s.tiles : 1);
   constexpr bool kOnesweep = V == 0 && (K == 4 || K == 8 || K == 16);
   bool os_ok = false;
@@ -151,7 +151,7 @@ rfx_status run_sort_kv(SortPlan& s) {
         using TS = OsTuning<K, OsIpt<K>::SMALL>;
         using TL = OsTuning<K, OsIpt<K>::ALT>;
         if (v == 4)
-          sort_pass_kernel<K, V, true><<<tile_grid, kSortThreads, tile_smem, s.stream>>>(a);
+          sort_pass_kernel<K, V, true><<<tile_grid, SortTuning<K, V>::THREADS, tile_smem, s.stream>>>(a);
         else if (os_ok && v == 1)
           sort_onesweep_kernel<K, TD::IPT><<<os_grid[0], kOsThreads, TD::SMEM, s.stream>>>(a);
         else if (os_ok && v == 2)
@@ -159,9 +159,9 @@ rfx_status run_sort_kv(SortPlan& s) {
         else if (os_ok && v == 3)
           sort_onesweep_kernel<K, TL::IPT><<<os_grid[2], kOsThreads, TL::SMEM, s.stream>>>(a);
         else
-          sort_pass_kernel<K, V><<<tile_grid, kSortThreads, tile_smem, s.stream>>>(a);
+          sort_pass_kernel<K, V><<<tile_grid, SortTuning<K, V>::THREADS, tile_smem, s.stream>>>(a);
       } else {
-        sort_pass_kernel<K, V><<<tile_grid, kSortThreads, tile_smem, s.stream>>>(a);
+        sort_pass_kernel<K, V><<<tile_grid, SortTuning<K, V>::THREADS, tile_smem, s.stream>>>(a);
       }
       RFX_CUDA_TRY(cudaGetLastError());
       return RFX_OK;

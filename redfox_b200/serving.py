@@ -286,15 +286,15 @@ class PinnedStage:
         return self.buf
 
 
-def to_host(tensors, stream=None, stage=None, copy=False):
+def to_host(tensors, stream=None, stage=None, copy=False, at=0):
     """Device tensors -> numpy arrays.  With a PinnedStage the copies go through its
-    page-locked buffer (the arrays are views of it unless copy=True)."""
+    page-locked buffer from byte `at` on (the arrays are views of it unless copy=True)."""
     import torch
     if stage is None:
         return [t.cpu().numpy() for t in tensors]
     sizes = [t.numel() * t.element_size() for t in tensors]
-    buf = stage.take(sum((b + 255) // 256 * 256 for b in sizes))
-    views, off = [], 0
+    buf = stage.take(at + sum((b + 255) // 256 * 256 for b in sizes))
+    views, off = [], at
     for t, b in zip(tensors, sizes):
         v = buf[off:off + b].view(t.dtype).view(t.shape)
         v.copy_(t, non_blocking=True)
@@ -330,22 +330,25 @@ def split_round(gk, gs, gc, nq, stream=None, stage=None, copy=True):
             for i in range(nq)]
 
 
-def run_round_host(res, queries, device="cuda", stream=None, stage=None, copy=True):
+def run_round_host(res, queries, device="cuda", stream=None, stage=None, copy=True, batch_min=8):
     """A round end to end: lists generated, queries with and without a list run as two
     batched plans (the intersection applies to the first only), results on the host in
-    the order of `queries` (copied out of `stage` unless copy=False).  A round of one query
-    runs the plain plan."""
+    the order of `queries` (copied out of `stage` unless copy=False).  A round of fewer than
+    `batch_min` queries runs them one after another with the plain plan: a batched plan's
+    extra passes (the query byte in every key) cost more than a few queries share."""
     import contextlib
 
     import numpy as np
     import torch
-    if len(queries) == 1:
-        # nothing to share: the plain plan (fewer passes than the batched one), on `stream`
-        q = queries[0]
-        with torch.cuda.stream(stream) if stream is not None else contextlib.nullcontext():
-            out = run_query(res, q, query_list(q, res.n2, device))
-        k, sm, c = to_host(out, stream, stage, copy)
-        return [(k.view(np.uint32), sm, c.view(np.uint32))]
+    if len(queries) < batch_min:
+        outs, at = [], 0
+        for q in queries:
+            with torch.cuda.stream(stream) if stream is not None else contextlib.nullcontext():
+                out = run_query(res, q, query_list(q, res.n2, device))
+            k, sm, c = to_host(out, stream, stage, copy, at=at)
+            outs.append((k.view(np.uint32), sm, c.view(np.uint32)))
+            at += sum((t.numel() * t.element_size() + 255) // 256 * 256 for t in out)
+        return outs
     res_by_q = [None] * len(queries)
     with_list = [i for i, q in enumerate(queries) if q.list_size > 0]
     without = [i for i, q in enumerate(queries) if q.list_size == 0]

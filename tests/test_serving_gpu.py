@@ -99,3 +99,18 @@ def test_single_query_round_on_a_side_stream(resident):
         for a, b in ((got[0], alone[0].numpy().view(np.uint32)), (got[1], alone[1].numpy()),
                      (got[2], alone[2].numpy().view(np.uint32)), (bk, got[0]), (bs, got[1]), (bc, got[2])):
             assert np.array_equal(a, b), q
+
+
+def test_small_round_runs_plain_plans(cuda, resident):
+    """A round of fewer queries than the batching threshold runs them one after another with
+    the plain plan, results staged at separate offsets of the page-locked buffer: each equals
+    the query run alone, also with views (copy=False) that must not overlap."""
+    import torch
+    reqs = _requests(resident, 3, seed=26)
+    st = torch.cuda.Stream()
+    outs = S.run_round_host(resident, reqs, "cuda", stream=st, stage=S.PinnedStage(1 << 20), copy=False)
+    for q, got in zip(reqs, outs):
+        alone = S.run_alone(resident, q)
+        assert np.array_equal(got[0], alone[0].numpy().view(np.uint32)), q
+        assert np.array_equal(got[1], alone[1].numpy()), q
+        assert np.array_equal(got[2], alone[2].numpy().view(np.uint32)), q

@@ -589,16 +589,22 @@ def _op_setops(ctx, peak, reps):
             no = int(c.item())
             ops["%s_%s" % (name, tag)] = _op_line(a.shape[0] + b.shape[0], (a.shape[0] + b.shape[0] + no) * 4, ms,
                                                   peak, out=no, note=note)
-            if name == "intersect":   # the tuner's other variants (4; one-pass 1 and 3) beside the default
-                for v, suffix in ((4, "two_pass_16_per_thread"), (1, "one_pass"), (3, "one_pass_16_per_thread")):
-                    R.tune_force(2, v)
-                    try:
-                        ms = _time_ms(run, reps)
-                    finally:
-                        R.tune_force(2, -1)
-                    ops["%s_%s_%s" % (name, tag, suffix)] = _op_line(a.shape[0] + b.shape[0],
-                                                                     (a.shape[0] + b.shape[0] + no) * 4, ms, peak,
-                                                                     out=no, note=note)
+            # the tuner's other variants beside the default (the warp-segment form, 16 items per
+            # thread): the warp-segment form with 8 (5) and the two-pass form (6) for every
+            # operator, the two-pass form with 16 items per thread (4) and the one-pass form (1, 3)
+            # for the intersection
+            variants = ((5, "warp_segment_8_per_thread"), (6, "two_pass"))
+            if name == "intersect":
+                variants += ((4, "two_pass_16_per_thread"), (1, "one_pass"), (3, "one_pass_16_per_thread"))
+            for v, suffix in variants:
+                R.tune_force(2, v)
+                try:
+                    ms = _time_ms(run, reps)
+                finally:
+                    R.tune_force(2, -1)
+                ops["%s_%s_%s" % (name, tag, suffix)] = _op_line(a.shape[0] + b.shape[0],
+                                                                 (a.shape[0] + b.shape[0] + no) * 4, ms, peak,
+                                                                 out=no, note=note)
     return ops
 
 
@@ -873,7 +879,7 @@ def batched_benchmark(dev, nq, reps=3):
     batch_ms = statistics.median(ms)
     keys, sums, counts, total = plan.result()
     per = B.split_by_query(keys, sums, counts, min(nq, 8))
-    ok = all(torch.equal(per[q][0], plain[q][0] & B.QUERY_KEY_MASK) and torch.equal(per[q][1], plain[q][1])
+    ok = all(torch.equal(per[q][0], B.unfold(plain[q][0])[0]) and torch.equal(per[q][1], plain[q][1])
              and torch.equal(per[q][2], plain[q][2]) for q in range(len(plain)))
     nbytes = plan.nbytes()
     del plan

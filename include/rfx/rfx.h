@@ -166,6 +166,16 @@ rfx_status rfx_sort_pairs(void* keys, void* values, uint64_t n, uint32_t key_byt
                           uint32_t value_bytes, uint32_t begin_bit, uint32_t end_bit,
                           uint32_t flags, void* workspace, size_t workspace_bytes, void* stream);
 
+/* rfx_sort_pairs out of place: keys_in (and values_in) sorted into keys (and values), the
+ * inputs left as they are (the first digit pass reads them; no copy is made).  Inputs and
+ * outputs must not overlap; same workspace as rfx_sort_pairs.  No reference counterpart
+ * (the reference's sorts work in place); a plan that must keep its input, such as a
+ * replayed batched plan, uses it instead of a copy followed by an in-place sort. */
+rfx_status rfx_sort_pairs_from(const void* keys_in, const void* values_in, void* keys, void* values,
+                               uint64_t n, uint32_t key_bytes, uint32_t value_bytes,
+                               uint32_t begin_bit, uint32_t end_bit, uint32_t flags,
+                               void* workspace, size_t workspace_bytes, void* stream);
+
 /* redfox::sort_pair / sort_key of b40cSort.cu:58 / :828 with the reference's argument
  * meaning: the key container follows key_bits (<=8: 1 byte, <=16: 2, <=32: 4, <=64: 8),
  * the value container follows value_type (a DataType code), the sort covers bits

@@ -1,10 +1,12 @@
 """Batched execution: many independent sort + join + aggregate queries in one launch per
 operator, and the whole batched plan captured as a CUDA graph.
 
-The queries are folded into one relation by putting the query id above each query's key
-(key' = q << 21 | key, the per-query key domains |R|/4 being below 2^21): sorting on the
-composite key sorts every query, the sort-merge join on it joins every query with itself
-only, and the aggregate groups per (query, key).  The join and the aggregate on its key run
+The queries are folded into one relation by putting the query id below each query's key
+(key' = key << 9 | q, the per-query key domains |R|/4 being below 2^21 and q below 2^9), and
+the relation holds the queries in query order.  A stable sort on the key's 21 bits alone
+therefore leaves equal keys in query order, i.e. it sorts on the whole composite key in
+three 8-bit digit passes (the query bits need none); the sort-merge join on the composite
+joins every query with itself only, and the aggregate groups per (key, query).  The join and the aggregate on its key run
 as one operator (rfx_join_aggregate: per key, the join's SUM and COUNT from the two sides'
 sorted runs, no join rows written) in both forms, batched and plain.  Tiles of all queries then share the
 persistent kernels' dynamic tile queues (the device work queue), so a 10^4-row query and an
@@ -22,8 +24,21 @@ from .workloads import SEED_BASE
 C3_QUERIES = 512
 C3_MIN, C3_MAX = 10_000, 8_000_000
 C3_SEED = SEED_BASE + 3
-QUERY_SHIFT = 21               # query id bits start here in the 32-bit key field
-QUERY_KEY_MASK = (1 << QUERY_SHIFT) - 1
+QUERY_BITS = 9                 # the query id: the low bits of the 32-bit key field
+QUERY_MASK = (1 << QUERY_BITS) - 1
+KEY_BITS = 21                  # the per-query key above it
+R_SORT_BITS = (32 + QUERY_BITS, 32 + QUERY_BITS + KEY_BITS)   # R rows: the key field is bits 32..63
+S_SORT_BITS = (64 + QUERY_BITS, 64 + QUERY_BITS + KEY_BITS)   # S rows: the foreign key is bits 64..95
+
+
+def fold(key, q):
+    """The key field of query q's row with key `key`."""
+    return (key << QUERY_BITS) | q
+
+
+def unfold(field):
+    """(key, query id) of key fields (integers or tensors)."""
+    return field >> QUERY_BITS, field & QUERY_MASK
 
 
 def _mix64(x):
@@ -50,8 +65,8 @@ def query_sizes(nq=C3_QUERIES, lo=C3_MIN, hi=C3_MAX, seed=C3_SEED):
 
 
 def gen_batch(sizes, device="cuda"):
-    """Concatenated R (8-byte rows) and S (16-byte rows) of all queries with the query id in
-    the key's high bits, plus per-query row offsets."""
+    """Concatenated R (8-byte rows) and S (16-byte rows) of all queries, in query order, with
+    the query id folded into the key field (fold()), plus per-query row offsets."""
     import torch
     nr_tot = sum(s[0] for s in sizes)
     ns_tot = sum(s[1] for s in sizes)
@@ -65,8 +80,8 @@ def gen_batch(sizes, device="cuda"):
         r64 = rq.view(torch.int64).view(nr)
         keys = (r64 >> 32) & 0xFFFFFFFF
         s64 = sq.view(torch.int64).view(ns, 2)
-        s64[:, 1] = keys[s64[:, 1]] | (q << QUERY_SHIFT)
-        r64 |= (q << QUERY_SHIFT) << 32
+        s64[:, 1] = fold(keys[s64[:, 1]], q)
+        r64.copy_((fold(keys, q) << 32) | (r64 & 0xFFFFFFFF))
         r_all[r_off[-1]:r_off[-1] + nr] = rq
         s_all[s_off[-1]:s_off[-1] + ns] = sq
         r_off.append(r_off[-1] + nr)
@@ -86,8 +101,8 @@ class BatchedPlan:
         self.nr, self.ns = r_all.shape[0], s_all.shape[0]
         self.r = torch.empty_like(r_all)
         self.s = torch.empty_like(s_all)
-        self.rsort = R.Sorter(self.nr, 8, 0, 32, 64, device=dev)
-        self.ssort = R.Sorter(self.ns, 16, 0, 64, 96, device=dev)
+        self.rsort = R.Sorter(self.nr, 8, 0, *R_SORT_BITS, device=dev)
+        self.ssort = R.Sorter(self.ns, 16, 0, *S_SORT_BITS, device=dev)
         self.ja = R.JoinAggregate(self.ns, 4, device=dev)
         self.graph = None
 
@@ -108,11 +123,10 @@ class BatchedPlan:
                                                           self.ja.counts, self.ja.ws, self.rsort.ws, self.ssort.ws))
 
     def run(self, stream=None):
-        """Enqueue the whole plan (no host synchronisation)."""
-        self.r.copy_(self.r_in)
-        self.s.copy_(self.s_in)
-        self.rsort(self.r, stream=stream)
-        self.ssort(self.s, stream=stream)
+        """Enqueue the whole plan (no host synchronisation).  The sorts read the inputs and
+        write the plan's own buffers, so the inputs stay as they are for the next replay."""
+        self.rsort(self.r, stream=stream, src_keys=self.r_in)
+        self.ssort(self.s, stream=stream, src_keys=self.s_in)
         self.ja(self.r, 32, self.s, 64, 0, 64, stream=stream)
 
     def capture(self):
@@ -138,21 +152,23 @@ class BatchedPlan:
 
 
 def split_by_query(keys, sums, counts, nq):
-    """Batched groups -> per-query (keys, sums, counts) with the query bits removed."""
+    """Batched groups (ordered by key, then query) -> per-query (keys, sums, counts) for
+    queries 0 .. nq - 1, keys without the query bits, in key order."""
     import torch
-    q = (keys.to(torch.int64) >> QUERY_SHIFT)
-    bounds = torch.searchsorted(q, torch.arange(nq + 1, device=keys.device))
+    k64 = keys.to(torch.int64) & 0xFFFFFFFF
+    key, q = unfold(k64)
     out = []
     for i in range(nq):
-        a, b = int(bounds[i]), int(bounds[i + 1])
-        out.append((keys[a:b] & QUERY_KEY_MASK, sums[a:b], counts[a:b]))
+        m = q == i
+        out.append((key[m].to(keys.dtype), sums[m], counts[m]))
     return out
 
 
 def plain_query(r_all, s_all, r_off, s_off, q, stream=None):
     """Query q alone through the plain plan (one launch sequence, the group count read
-    back).  Returns (keys, sums, counts, join rows)."""
+    back): the same sorts on the key's bits, the same join-aggregate.  Returns (keys with
+    the query bits, sums, counts, join rows)."""
     import torch
     keys, sums, counts = PL.join_aggregate_fused(r_all[r_off[q]:r_off[q + 1]], s_all[s_off[q]:s_off[q + 1]],
-                                                 stream=stream)
+                                                 stream=stream, r_bits=R_SORT_BITS, s_bits=S_SORT_BITS)
     return keys, sums, counts, int(counts.to(torch.int64).sum())

@@ -20,6 +20,8 @@ namespace rfx {
 
 template <int W>
 rfx_status launch_aggregate(const AggLaunch&);
+template <int W>
+rfx_status preload_aggregate();
 
 namespace {
 
@@ -29,9 +31,21 @@ constexpr size_t kScratchWords = (size_t)kMaxGroups * (kMaxSum + 1);
 static __device__ __align__(256) unsigned long long g_scratch[kScratchWords + 1];
 
 // In host code `g_scratch` only names a host-side stand-in; the device address comes from
-// cudaGetSymbolAddress, taken once per device with that device current.
+// cudaGetSymbolAddress, taken once per device with that device current.  The same first
+// call loads every kernel the entry can launch (CUDA otherwise loads each on its first
+// launch, taking device memory then), so that later calls change nothing in device memory.
 std::mutex g_mu;
 unsigned long long* g_addr[128] = {nullptr};
+
+rfx_status preload_kernels() {
+  rfx_status st;
+  if ((st = preload_aggregate<1>()) != RFX_OK || (st = preload_aggregate<2>()) != RFX_OK ||
+      (st = preload_aggregate<4>()) != RFX_OK || (st = preload_aggregate<8>()) != RFX_OK ||
+      (st = preload_aggregate<16>()) != RFX_OK || (st = preload_aggregate<32>()) != RFX_OK ||
+      (st = preload_aggregate<64>()) != RFX_OK)
+    return st;
+  return RFX_OK;
+}
 
 rfx_status scratch_address(unsigned long long** out) {
   int dev = 0;
@@ -45,6 +59,8 @@ rfx_status scratch_address(unsigned long long** out) {
       (void)cudaGetLastError();
       return RFX_ERR_CUDA;
     }
+    const rfx_status st = preload_kernels();
+    if (st != RFX_OK) return st;
     g_addr[dev] = static_cast<unsigned long long*>(p);
   }
   *out = g_addr[dev];

@@ -100,11 +100,12 @@ RowLayout row_layout(void* ws, uint64_t n, uint32_t row_bytes) {
 }
 
 // The chunked staged reduce: one look-back record per chunk (at most one chunk per
-// resident block), and scratch for n / 16 groups (plus a floor for small inputs): a chunk
-// whose groups do not fit its share runs its rows a second time.
+// resident block), and scratch for n / 4 groups (plus a floor for small inputs): a chunk
+// whose groups do not fit its share -- more than one group per 4 rows -- runs its rows a
+// second time, writing directly.
 constexpr uint64_t kMaxChunks = 4096;
 constexpr int kChunkStages = 3;
-constexpr uint64_t kChunkRowsPerSlot = 16;
+constexpr uint64_t kChunkRowsPerSlot = 4;
 
 struct ChunkLayout {
   SegRecord* records;

@@ -94,8 +94,20 @@ rfx_status launch_aggregate(const AggLaunch& a) {
   return RFX_OK;
 }
 
+// Loads both aggregate kernels of this row width (CUDA loads a kernel on its first launch
+// by default, which takes device memory): a caller that must not allocate on later calls
+// loads them up front.
+template <int WIN>
+rfx_status preload_aggregate() {
+  cudaFuncAttributes attr;
+  RFX_CUDA_TRY(cudaFuncGetAttributes(&attr, (const void*)scan_aggregate_kernel<WIN, true>));
+  RFX_CUDA_TRY(cudaFuncGetAttributes(&attr, (const void*)scan_aggregate_kernel<WIN, false>));
+  return RFX_OK;
+}
+
 #define RFX_INSTANTIATE_SCAN(W)                                              \
   template rfx_status launch_compact<W>(int, uint32_t, const ScanLaunch&); \
-  template rfx_status launch_aggregate<W>(const AggLaunch&);
+  template rfx_status launch_aggregate<W>(const AggLaunch&);               \
+  template rfx_status preload_aggregate<W>();
 
 }  // namespace rfx

@@ -14,9 +14,10 @@ bool elem_width(uint32_t e) { return e == 1 || e == 2 || e == 4 || e == 8 || e =
 struct FilterLayout {
   uint64_t* status;
   uint32_t* counter;
-  uint64_t* split;   // 3 words per tile (filled by set_split_kernel)
+  uint64_t* split;   // 3 words per tile, and per tile boundary plus one (set_split_kernel, set_bounds_kernel)
   uint8_t* mask;     // two-pass form: one bit per element
   uint32_t* counts;  // two-pass form: kept elements per tile
+  uint32_t* wcounts; // warp-segment form: kept elements per warp segment
   uint64_t* offsets; // two-pass form: each tile's output offset
   size_t clear;
   size_t total;
@@ -26,14 +27,15 @@ FilterLayout filter_layout(void* ws, uint64_t n) {
   FilterLayout L;
   Carver c(ws);
   const uint64_t tiles = (n + kSetTileMin - 1) / kSetTileMin + 1;
-  const uint64_t mark_tiles = (n + kMarkTile - 1) / kMarkTile + 1;
+  const uint64_t mark_tiles = (n + kSetTileMin - 1) / kSetTileMin + 1;   // tiles of 4 items per thread at the most
   L.status = c.take<uint64_t>(tiles);
   L.counter = c.take<uint32_t>(1);
   L.clear = align_up(c.used, 256);
   c.used = L.clear;
-  L.split = c.take<uint64_t>(3 * tiles);
+  L.split = c.take<uint64_t>(3 * (tiles + 1));
   L.mask = c.take<uint8_t>(mark_tiles * kSetThreads);
   L.counts = c.take<uint32_t>(mark_tiles);
+  L.wcounts = c.take<uint32_t>(mark_tiles * kSegWarps);
   L.offsets = c.take<uint64_t>(mark_tiles);
   L.total = align_up(c.used, 256);
   return L;
@@ -95,24 +97,83 @@ rfx_status launch_two_pass(int mode, SetFilterArgs& a, const FilterLayout& L, cu
   return RFX_OK;
 }
 
-// Variants of intersection / difference / union's B - A: 0 the two-pass form with 8 items
-// per thread; 1, 2, 3 the one-pass form (decoupled look-back) with 8, 4 and 16 items per
-// thread; 4 the two-pass form with 16 items per thread.  Unique and
-// filters whose output overlaps A (in place) always take the one-pass form with 8 items
-// per thread.  The one-pass form's look-back status and tile counter are zeroed before
-// each launch.
+// The warp-segment form's B window capacity (elements per buffer) for n_a elements filtered
+// against n_b: 1.25x the expected window of a tile plus 512, at least 2048, a multiple of 4;
+// 0 when a buffer would exceed 32 KiB (the two-pass form's single window serves those).
+template <int E, int IPT>
+uint32_t seg_wcap(uint64_t na, uint64_t nb) {
+  double want = 1.25 * (double)(kSetThreads * IPT) * ((double)nb / (double)(na ? na : 1)) + 512.0;
+  if (want < 2048.0) want = 2048.0;
+  const uint32_t w = ((uint32_t)(want < 1e9 ? want : 1e9) + 3u) & ~3u;
+  return (uint64_t)seg_buffer_elems<E>(w) * E > 32u * 1024u ? 0u : w;
+}
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+// The warp-segment form (4- and 8-byte elements, 16-byte aligned A and B): bounds per tile
+// boundary, mark (keep bits, counts per tile and per warp segment), offsets and the total,
+// compaction.  Needs no cleared workspace.  Returns RFX_ERR_UNSUPPORTED for inputs it does
+// not take.
+template <int E, int IPT>
+rfx_status launch_seg(int mode, SetFilterArgs& a, const FilterLayout& L, cudaStream_t s) {
+  if constexpr (E != 4 && E != 8) {
+    return RFX_ERR_UNSUPPORTED;
+  } else {
+    constexpr int TILE = kSetThreads * IPT;
+    const uint64_t tiles = (a.na + TILE - 1) / TILE;
+    const uint32_t wcap = seg_wcap<E, IPT>(a.na, a.nb);
+    if (!wcap || (a.na && !aligned16(a.a)) || (a.nb && !aligned16(a.b))) return RFX_ERR_UNSUPPORTED;
+    if (tiles) {
+      const uint64_t work = (tiles + 1) * 32;   // one warp per tile boundary
+      set_bounds_kernel<E, TILE><<<(int)((work + 255) / 256), 256, 0, s>>>(a.a, a.na, a.b, a.nb, L.split);
+      RFX_CUDA_TRY(cudaGetLastError());
+      a.split = L.split;
+      a.wcap = wcap;
+      auto k = mode == KEEP_MATCHED ? set_mark_seg_kernel<E, KEEP_MATCHED, IPT> : set_mark_seg_kernel<E, KEEP_UNMATCHED, IPT>;
+      const size_t smem = 2 * (size_t)seg_buffer_elems<E>(wcap) * E;
+      RFX_CUDA_TRY(allow_smem((const void*)k, smem));
+      const int grid = persistent_grid((const void*)k, kSetThreads, smem, tiles);
+      k<<<grid, kSetThreads, smem, s>>>(a, L.mask, L.counts, L.wcounts);
+      RFX_CUDA_TRY(cudaGetLastError());
+    }
+    set_offsets_kernel<<<1, kOffsetThreads, 0, s>>>(L.counts, tiles, L.offsets, a.d_count);
+    RFX_CUDA_TRY(cudaGetLastError());
+    if (tiles) {
+      const int grid = persistent_grid((const void*)set_compact_seg_kernel<E, IPT>, kSetThreads, 0, tiles);
+      set_compact_seg_kernel<E, IPT><<<grid, kSetThreads, 0, s>>>(a.a, a.na, L.mask, L.offsets, L.wcounts, a.out, a.na);
+      RFX_CUDA_TRY(cudaGetLastError());
+    }
+    return RFX_OK;
+  }
+}
+
+// Variants of intersection / difference / union's B - A: 0 (the default) the warp-segment
+// form with 16 items per thread; 1, 2, 3 the one-pass form (decoupled look-back) with 8, 4
+// and 16 items per thread; 4 the two-pass form with 16 items per thread; 5 the warp-segment
+// form with 8; 6 the two-pass form with 8.  The warp-segment form takes fewer items per
+// thread where a tile's B window would not fit (16 -> 8 -> 4), and the two-pass form with 8
+// items where it does not apply at all.  Unique and filters whose output overlaps A (in
+// place) always take the one-pass form with 8 items per thread.  The one-pass form's
+// look-back status and tile counter are zeroed before each launch.
 template <int E>
 rfx_status launch_filter(int mode, SetFilterArgs& a, cudaStream_t s, const FilterLayout* L, bool in_place) {
   auto run = [&](int v) -> rfx_status {
-    if (v == 0 && L) return launch_two_pass<E, 8>(mode, a, *L, s);
+    if ((v == 0 || v == 5) && L) {
+      rfx_status st = v == 0 ? launch_seg<E, 16>(mode, a, *L, s) : RFX_ERR_UNSUPPORTED;
+      if (st == RFX_ERR_UNSUPPORTED) st = launch_seg<E, 8>(mode, a, *L, s);
+      if (st == RFX_ERR_UNSUPPORTED) st = launch_seg<E, 4>(mode, a, *L, s);
+      if (st != RFX_ERR_UNSUPPORTED) return st;
+      v = 6;
+    }
+    if (v == 6 && L) return launch_two_pass<E, 8>(mode, a, *L, s);
     if (v == 4 && L) return launch_two_pass<E, 16>(mode, a, *L, s);
     if (L) RFX_CUDA_TRY(cudaMemsetAsync(L->status, 0, L->clear, s));
-    if (v <= 1 || mode == KEEP_HEADS) return launch_filter_ipt<E, 8>(mode, a, s);
+    if (v <= 1 || v >= 5 || mode == KEEP_HEADS) return launch_filter_ipt<E, 8>(mode, a, s);
     return v == 2 ? launch_filter_ipt<E, 4>(mode, a, s) : launch_filter_ipt<E, 16>(mode, a, s);
   };
   if (mode == KEEP_HEADS || !L) return run(1);
   if (in_place) return run(1);
-  return run(tune_pick(TUNE_SET_FILTER, ((uint64_t)E << 8) | (uint64_t)mode, a.na + a.nb, 5, run, s));
+  return run(tune_pick(TUNE_SET_FILTER, ((uint64_t)E << 8) | (uint64_t)mode, a.na + a.nb, 7, run, s));
 }
 
 rfx_status dispatch_filter(uint32_t e, int mode, SetFilterArgs& a, cudaStream_t s, const FilterLayout* L = nullptr,
@@ -129,8 +190,25 @@ rfx_status dispatch_filter(uint32_t e, int mode, SetFilterArgs& a, cudaStream_t 
 
 template <int E>
 rfx_status launch_merge(const void* a, uint64_t na, const void* d, uint64_t nd_max, const uint64_t* d_nd, void* out,
-                        uint64_t* d_count, cudaStream_t s) {
+                        uint64_t* d_count, uint64_t* mp, cudaStream_t s) {
   const uint64_t tiles = (na + nd_max + kMergeTile - 1) / kMergeTile;
+  if constexpr (E == 4 || E == 8) {
+    // the staged merge: partitions of every tile first, then the tiles
+    if (mp && aligned16(a) && aligned16(d) && aligned16(out)) {
+      const uint64_t work = (tiles + 1) * 32;   // one warp per tile boundary
+      merge_partition_kernel<E><<<(int)((work + 255) / 256), 256, 0, s>>>(
+          static_cast<const uint8_t*>(a), na, static_cast<const uint8_t*>(d), nd_max, d_nd, mp);
+      RFX_CUDA_TRY(cudaGetLastError());
+      const size_t smem = merge_staged_smem<E>();
+      RFX_CUDA_TRY(allow_smem((const void*)merge_staged_kernel<E>, smem));
+      const int grid = persistent_grid((const void*)merge_staged_kernel<E>, kSetThreads, smem, tiles ? tiles : 1);
+      merge_staged_kernel<E><<<grid, kSetThreads, smem, s>>>(static_cast<const uint8_t*>(a), na,
+                                                              static_cast<const uint8_t*>(d), nd_max, d_nd, mp,
+                                                              static_cast<uint8_t*>(out), d_count);
+      RFX_CUDA_TRY(cudaGetLastError());
+      return RFX_OK;
+    }
+  }
   const int grid = persistent_grid((const void*)merge_kernel<E>, kSetThreads, 0, tiles ? tiles : 1);
   merge_kernel<E><<<grid, kSetThreads, 0, s>>>(static_cast<const uint8_t*>(a), na, static_cast<const uint8_t*>(d),
                                                nd_max, d_nd, static_cast<uint8_t*>(out), d_count);
@@ -139,13 +217,13 @@ rfx_status launch_merge(const void* a, uint64_t na, const void* d, uint64_t nd_m
 }
 
 rfx_status dispatch_merge(uint32_t e, const void* a, uint64_t na, const void* d, uint64_t nd_max, const uint64_t* d_nd,
-                          void* out, uint64_t* d_count, cudaStream_t s) {
+                          void* out, uint64_t* d_count, uint64_t* mp, cudaStream_t s) {
   switch (e) {
-    case 1: return launch_merge<1>(a, na, d, nd_max, d_nd, out, d_count, s);
-    case 2: return launch_merge<2>(a, na, d, nd_max, d_nd, out, d_count, s);
-    case 4: return launch_merge<4>(a, na, d, nd_max, d_nd, out, d_count, s);
-    case 8: return launch_merge<8>(a, na, d, nd_max, d_nd, out, d_count, s);
-    case 16: return launch_merge<16>(a, na, d, nd_max, d_nd, out, d_count, s);
+    case 1: return launch_merge<1>(a, na, d, nd_max, d_nd, out, d_count, mp, s);
+    case 2: return launch_merge<2>(a, na, d, nd_max, d_nd, out, d_count, mp, s);
+    case 4: return launch_merge<4>(a, na, d, nd_max, d_nd, out, d_count, mp, s);
+    case 8: return launch_merge<8>(a, na, d, nd_max, d_nd, out, d_count, mp, s);
+    case 16: return launch_merge<16>(a, na, d, nd_max, d_nd, out, d_count, mp, s);
     default: return RFX_ERR_UNSUPPORTED;
   }
 }
@@ -166,6 +244,7 @@ struct SetLayout {
   FilterLayout f;
   uint8_t* diff;
   uint64_t* d_nd;
+  uint64_t* mp;   // union: where each merge tile's first diagonal crosses A
   size_t total;
 };
 
@@ -178,6 +257,7 @@ SetLayout set_layout(void* ws, uint32_t op, uint64_t na, uint64_t nb, uint32_t e
   c.used = L.f.total;
   L.diff = op == RFX_SET_UNION ? c.take<uint8_t>(nb * e) : nullptr;
   L.d_nd = op == RFX_SET_UNION ? c.take<uint64_t>(1) : nullptr;
+  L.mp = op == RFX_SET_UNION ? c.take<uint64_t>((na + nb + kMergeTile - 1) / kMergeTile + 2) : nullptr;
   L.total = align_up(c.used, 256);
   return L;
 }
@@ -212,7 +292,7 @@ rfx_status set_op_impl(uint32_t op, void* out, uint64_t* d_count, const void* a,
     f.d_count = L.d_nd;
     rfx_status st = dispatch_filter(e, KEEP_UNMATCHED, f, s, &L.f);
     if (st != RFX_OK) return st;
-    return dispatch_merge(e, a, na, L.diff, nb, L.d_nd, out, d_count, s);
+    return dispatch_merge(e, a, na, L.diff, nb, L.d_nd, out, d_count, L.mp, s);
   }
   f.a = static_cast<const uint8_t*>(a);
   f.na = na;

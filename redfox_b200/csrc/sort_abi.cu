@@ -81,16 +81,35 @@ thread_local uint32_t t_host_trivial[kMaxSortPasses];
 
 rfx_status sort_pairs_impl(void* keys, void* vals, uint64_t n, uint32_t kb, uint32_t vb, uint32_t begin_bit,
                            uint32_t end_bit, void* ws, size_t ws_bytes, cudaStream_t stream, bool skip_trivial,
-                           int* passes_run) {
+                           int* passes_run, const void* src_keys = nullptr, const void* src_vals = nullptr) {
   if (passes_run) *passes_run = 0;
   if (!valid_width(kb) || !valid_vwidth(vb)) return RFX_ERR_UNSUPPORTED;
   if (end_bit > kb * 8 || begin_bit > end_bit) return RFX_ERR_INVALID;
+  if (src_keys && (n == 0 || !keys || (vb && (!vals || !src_vals)))) return n == 0 ? RFX_OK : RFX_ERR_INVALID;
+  if (src_keys && (n <= 1 || begin_bit == end_bit)) {
+    // nothing to order: the output is a copy of the input
+    RFX_CUDA_TRY(cudaMemcpyAsync(keys, src_keys, n * kb, cudaMemcpyDeviceToDevice, stream));
+    if (vb) RFX_CUDA_TRY(cudaMemcpyAsync(vals, src_vals, n * vb, cudaMemcpyDeviceToDevice, stream));
+    return RFX_OK;
+  }
   if (n <= 1 || begin_bit == end_bit) return RFX_OK;
   if (n >= (1ull << 30)) return RFX_ERR_UNSUPPORTED;  // 30-bit look-back counts
   if (!keys || (vb && !vals)) return RFX_ERR_INVALID;
   if (reinterpret_cast<uintptr_t>(keys) % std::min<uint32_t>(kb, 16) ||
       (vb && reinterpret_cast<uintptr_t>(vals) % std::min<uint32_t>(vb, 16)))
     return RFX_ERR_INVALID;
+  if (src_keys && (reinterpret_cast<uintptr_t>(src_keys) % std::min<uint32_t>(kb, 16) ||
+                   (vb && reinterpret_cast<uintptr_t>(src_vals) % std::min<uint32_t>(vb, 16))))
+    return RFX_ERR_INVALID;
+  if (src_keys) {
+    // source and destination must not overlap
+    const uintptr_t a = reinterpret_cast<uintptr_t>(src_keys), b = reinterpret_cast<uintptr_t>(keys);
+    if (a < b + n * kb && b < a + n * kb) return RFX_ERR_INVALID;
+    if (vb) {
+      const uintptr_t c = reinterpret_cast<uintptr_t>(src_vals), d = reinterpret_cast<uintptr_t>(vals);
+      if (c < d + n * vb && d < c + n * vb) return RFX_ERR_INVALID;
+    }
+  }
   SortLayout L = layout(ws, n, kb, vb, begin_bit, end_bit);
   if (!ws || ws_bytes < L.total) return RFX_ERR_WORKSPACE;
   uint32_t* err = device_error_word();
@@ -107,6 +126,9 @@ rfx_status sort_pairs_impl(void* keys, void* vals, uint64_t n, uint32_t kb, uint
     std::memset(&s, 0, sizeof(s));
     s.keys = cur_k;
     s.vals = cur_v;
+    const bool from_src = src_keys && lo == begin_bit;   // the first 128-bit chunk reads the source
+    s.src_keys = from_src ? static_cast<const uint8_t*>(src_keys) : nullptr;
+    s.src_vals = from_src && vb ? static_cast<const uint8_t*>(src_vals) : nullptr;
     s.alt_keys = oth_k;
     s.alt_vals = oth_v;
     s.alt2_keys = L.alt2_keys;
@@ -128,6 +150,11 @@ rfx_status sort_pairs_impl(void* keys, void* vals, uint64_t n, uint32_t kb, uint
     rfx_status st = dispatch(kb, s, vb);
     if (st != RFX_OK) return st;
     if (passes_run) *passes_run += s.executed;
+    if (from_src && s.executed == 0) {
+      // every pass was trivial: the output is a copy of the input
+      RFX_CUDA_TRY(cudaMemcpyAsync(cur_k, src_keys, n * kb, cudaMemcpyDeviceToDevice, stream));
+      if (vb) RFX_CUDA_TRY(cudaMemcpyAsync(cur_v, src_vals, n * vb, cudaMemcpyDeviceToDevice, stream));
+    }
     if (s.in_alt) {
       std::swap(cur_k, oth_k);
       std::swap(cur_v, oth_v);
@@ -195,6 +222,15 @@ extern "C" rfx_status rfx_sort_pairs(void* keys, void* values, uint64_t n, uint3
                                      size_t workspace_bytes, void* stream) {
   return sort_pairs_impl(keys, values, n, key_bytes, value_bytes, begin_bit, end_bit, workspace, workspace_bytes,
                          as_stream(stream), (flags & RFX_SORT_SKIP_TRIVIAL) != 0, nullptr);
+}
+
+extern "C" rfx_status rfx_sort_pairs_from(const void* keys_in, const void* values_in, void* keys, void* values,
+                                          uint64_t n, uint32_t key_bytes, uint32_t value_bytes, uint32_t begin_bit,
+                                          uint32_t end_bit, uint32_t flags, void* workspace, size_t workspace_bytes,
+                                          void* stream) {
+  if (n && !keys_in) return RFX_ERR_INVALID;
+  return sort_pairs_impl(keys, values, n, key_bytes, value_bytes, begin_bit, end_bit, workspace, workspace_bytes,
+                         as_stream(stream), (flags & RFX_SORT_SKIP_TRIVIAL) != 0, nullptr, keys_in, values_in);
 }
 
 extern "C" rfx_status rfx_b40c_sort_pair(void* keys, void* values, uint64_t n, uint64_t key_bits, uint64_t value_type) {

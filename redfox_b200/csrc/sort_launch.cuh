@@ -12,6 +12,8 @@ namespace rfx {
 struct SortPlan {
   uint8_t* keys;
   uint8_t* vals;
+  const uint8_t* src_keys;   // when set, the first pass and the histogram read these instead
+  const uint8_t* src_vals;   // of keys / vals, which then only receive (out-of-place sort)
   uint8_t* alt_keys;
   uint8_t* alt_vals;
   uint8_t* alt2_keys;   // a second pair of alternate buffers (may be null): an odd number
@@ -60,7 +62,8 @@ rfx_status run_sort_kv(SortPlan& s) {
     auto hk = sort_histogram_kernel<K>;
     const uint64_t blocks = (s.n + kSortThreads * 8 - 1) / (kSortThreads * 8);
     const int grid = persistent_grid((const void*)hk, kSortThreads, 0, blocks ? blocks : 1);
-    hk<<<grid, kSortThreads, 0, s.stream>>>(s.keys, s.n, s.begin_bit, s.end_bit, s.passes, s.ghist, s.trivial, s.done);
+    hk<<<grid, kSortThreads, 0, s.stream>>>(s.src_keys ? s.src_keys : s.keys, s.n, s.begin_bit, s.end_bit, s.passes,
+                                            s.ghist, s.trivial, s.done);
     RFX_CUDA_TRY(cudaGetLastError());
   }
   uint32_t triv[kMaxSortPasses] = {0};
@@ -120,8 +123,18 @@ rfx_status run_sort_kv(SortPlan& s) {
     kb[j] = at_keys ? s.keys : at_alt2 ? s.alt2_keys : s.alt_keys;
     vb[j] = at_keys ? s.vals : at_alt2 ? s.alt2_vals : s.alt_vals;
   }
+  if (s.src_keys) {
+    // out of place: the first pass reads the source (never written); a single pass writes
+    // straight into keys / vals
+    kb[0] = const_cast<uint8_t*>(s.src_keys);
+    vb[0] = const_cast<uint8_t*>(s.src_vals);
+    if (npass == 1) {
+      kb[1] = s.keys;
+      vb[1] = s.vals;
+    }
+  }
   s.executed = 0;
-  s.in_alt = kb[npass] != s.keys;
+  s.in_alt = npass ? kb[npass] != s.keys : false;   // no pass at all: the data is where it was
   for (uint32_t p = 0; p < s.passes; ++p) {
     if (triv[p]) continue;
     SortPassArgs a;

@@ -19,8 +19,9 @@ namespace rfx {
 
 enum TuneOp : uint32_t {
   TUNE_REDUCE_ROWS = 1,   // rfx_reduce_tuples, TMA-staged: chunked, or look-back per 256- / 128-line tile
-  TUNE_SET_FILTER = 2,    // set intersection / difference / union's B - A: two passes (mark, compact) with
-                          // 8 or 16 items per thread, or one pass with 8, 4 or 16
+  TUNE_SET_FILTER = 2,    // set intersection / difference / union's B - A: warp segments (bounds, mark,
+                          // compact) with 16 or 8 items per thread, two passes with 16 or 8, or one pass
+                          // with 8, 4 or 16
   TUNE_SCAN_COMPACT = 3,  // plan-specialised select / project: items per thread
   TUNE_SCAN_AGGREGATE = 4,  // plan-specialised filter-aggregate: rows per thread per iteration
   TUNE_SORT_PASS = 5,     // radix sort pass: per tile; onesweep (TMA stages + look-back warp; 3 tile sizes);

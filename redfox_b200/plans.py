@@ -47,15 +47,15 @@ def join_aggregate(r, s, stream=None):
     return keys, sums, counts, total
 
 
-def join_aggregate_fused(r, s, stream=None):
+def join_aggregate_fused(r, s, stream=None, r_bits=(32, 64), s_bits=(64, 96)):
     """The same plan with the join and the aggregate as one operator: sort R, sort S, then
     SUM(amount) and COUNT per key straight from the sorted relations (rfx_join_aggregate;
-    the join rows are never written).  Returns (keys u32, sums int64, counts u32) -- the
-    bytes join_aggregate returns."""
-    r = r.clone()
-    s = s.clone()
-    R.sort_pairs(r, begin_bit=32, end_bit=64, stream=stream)
-    R.sort_pairs(s, begin_bit=64, end_bit=96, stream=stream)
+    the join rows are never written).  r_bits / s_bits: the bit ranges the sorts order on
+    (by default the whole key fields; a narrower range where the key's other bits are known
+    to be constant).  Returns (keys u32, sums int64, counts u32) -- the bytes join_aggregate
+    returns."""
+    r, _ = R.sorted_copy(r, begin_bit=r_bits[0], end_bit=r_bits[1], stream=stream)
+    s, _ = R.sorted_copy(s, begin_bit=s_bits[0], end_bit=s_bits[1], stream=stream)
     return R.join_aggregate(r, 32, s, 64, 0, 64, 4, stream=stream)
 
 

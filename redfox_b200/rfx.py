@@ -79,6 +79,7 @@ def _load():
         "rfx_gen_uniform_rows": (st, [P, u64, P, u64, P, P, P]),
         "rfx_sort_workspace": (sz, [u64, u32, u32, u32, u32]),
         "rfx_sort_pairs": (st, [P, P, u64, u32, u32, u32, u32, u32, P, sz, P]),
+        "rfx_sort_pairs_from": (st, [P, P, P, P, u64, u32, u32, u32, u32, u32, P, sz, P]),
         "rfx_b40c_sort_pair": (st, [P, P, u64, u64, u64]),
         "rfx_b40c_sort_key": (st, [P, u64, u64]),
         "rfx_mgpu_sort_pair": (st, [P, P, u64, u64, u64]),
@@ -297,7 +298,14 @@ class Sorter:
         self.wsb = LIB.rfx_sort_workspace(n, key_bytes, value_bytes, self.begin, self.end)
         self.ws = _empty_bytes(self.wsb, device)
 
-    def __call__(self, keys, values=None, flags=0, stream=None):
+    def __call__(self, keys, values=None, flags=0, stream=None, src_keys=None, src_values=None):
+        """Sort keys (and values) in place, or, with src_keys (and src_values), sort those
+        into keys (and values) and leave them as they are."""
+        if src_keys is not None:
+            check("rfx_sort_pairs_from", LIB.rfx_sort_pairs_from(
+                _ptr(src_keys), _ptr(src_values), _ptr(keys), _ptr(values), self.n, self.kb, self.vb, self.begin,
+                self.end, flags, _ptr(self.ws), self.wsb, _stream(stream)))
+            return
         check("rfx_sort_pairs", LIB.rfx_sort_pairs(_ptr(keys), _ptr(values), self.n, self.kb, self.vb, self.begin,
                                                    self.end, flags, _ptr(self.ws), self.wsb, _stream(stream)))
 
@@ -308,6 +316,17 @@ def sort_pairs(keys, values=None, begin_bit=0, end_bit=None, flags=0, stream=Non
     s = Sorter(n, _width(keys), 0 if values is None else _width(values), begin_bit, end_bit, device=keys.device)
     s(keys, values, flags, stream)
     return keys, values
+
+
+def sorted_copy(keys, values=None, begin_bit=0, end_bit=None, flags=0, stream=None):
+    """New tensors holding keys (and values) sorted; the inputs are left as they are."""
+    import torch
+    n = keys.shape[0]
+    out_k = torch.empty_like(keys)
+    out_v = None if values is None else torch.empty_like(values)
+    s = Sorter(n, _width(keys), 0 if values is None else _width(values), begin_bit, end_bit, device=keys.device)
+    s(out_k, out_v, flags, stream, src_keys=keys, src_values=values)
+    return out_k, out_v
 
 
 # ---------------------------------------------------------------------------- reduce

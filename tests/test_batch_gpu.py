@@ -1,6 +1,6 @@
-"""The batched form: many join + aggregate queries folded into one plan (query id above the
-key) give, per query, exactly the plain per-query plan's result and the oracle's, eagerly
-and through CUDA graph replay."""
+"""The batched form: many join + aggregate queries folded into one plan (query id below the
+key, queries in order) give, per query, exactly the plain per-query plan's result and the
+oracle's, eagerly and through CUDA graph replay."""
 import numpy as np
 import pytest
 
@@ -15,14 +15,17 @@ def test_query_sizes_are_deterministic_and_in_range():
     assert all(1000 <= x <= 50_000 for q in a for x in q)
     full = B.query_sizes()
     assert len(full) == B.C3_QUERIES
-    # the per-query key domain |R|/4 must stay below the query-id bits
-    assert max(r for r, _ in full) // 4 <= B.QUERY_KEY_MASK
-    assert (B.C3_QUERIES - 1) << B.QUERY_SHIFT < 1 << 32
+    # the per-query key domain |R|/4 must fit the key bits, the query ids the query bits,
+    # and both the 32-bit key field
+    assert max(r for r, _ in full) // 4 <= 1 << B.KEY_BITS
+    assert B.C3_QUERIES - 1 <= B.QUERY_MASK
+    assert B.QUERY_BITS + B.KEY_BITS <= 32
+    assert B.unfold(B.fold(12345, 67)) == (12345, 67)
 
 
 def _per_query(r_all, s_all, r_off, s_off, q):
     keys, sums, counts, total = B.plain_query(r_all, s_all, r_off, s_off, q)
-    return keys & B.QUERY_KEY_MASK, sums, counts, total
+    return B.unfold(keys)[0], sums, counts, total
 
 
 @pytest.mark.gpu
@@ -45,7 +48,7 @@ def test_batched_equals_plain_and_oracle(cuda):
             ek, es, ec, et = join_aggregate_oracle(to_np(r_all[r_off[q]:r_off[q + 1]]),
                                                    to_np(s_all[s_off[q]:s_off[q + 1]]))
             assert et == pt
-            assert np.array_equal(to_np(bk).view(np.uint32), ek & B.QUERY_KEY_MASK)
+            assert np.array_equal(to_np(bk).view(np.uint32), ek >> np.uint32(B.QUERY_BITS))
             assert np.array_equal(to_np(bs), es)
             assert np.array_equal(to_np(bc).view(np.uint32), ec)
     assert totals == total

@@ -84,7 +84,7 @@ def test_batched_64_queries_full_size_law_bit_exact(cuda):
         ek, es, ec, et = join_aggregate_oracle(hr[r_off[q]:r_off[q + 1]], hs[s_off[q]:s_off[q + 1]])
         etotal += et
         bk, bs, bc = per[q]
-        assert np.array_equal(to_np(bk).view(np.uint32), ek & np.uint32(B.QUERY_KEY_MASK)), q
+        assert np.array_equal(to_np(bk).view(np.uint32), ek >> np.uint32(B.QUERY_BITS)), q
         assert np.array_equal(to_np(bs), es), q
         assert np.array_equal(to_np(bc).view(np.uint32), ec), q
     assert total == etotal
@@ -100,5 +100,5 @@ def test_oracle_generator_matches_for_batched_inputs(cuda):
         dom = max(1, nr // 4)
         key = O.uniform(nr, B.C3_SEED + 16 + 2 * q, 0, 0, dom)
         pay = O.uniform(nr, B.C3_SEED + 16 + 2 * q, 1, 0, 1 << 32)
-        exp = ((key | np.uint64(q << B.QUERY_SHIFT)) << np.uint64(32)) | pay
+        exp = (((key << np.uint64(B.QUERY_BITS)) | np.uint64(q)) << np.uint64(32)) | pay
         assert np.array_equal(hr[r_off[q]:r_off[q + 1]], exp)

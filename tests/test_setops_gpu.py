@@ -107,13 +107,14 @@ def test_reference_compatible_set_entries(cuda):
                                       P(db.data_ptr()), P(db.data_ptr()), 99) == R.ERR_UNSUPPORTED
 
 
-@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("variant", [0, 1, 2, 3, 4, 5, 6])
 @pytest.mark.parametrize("dtype", [np.uint32, np.uint64])
 def test_set_filter_variants(cuda, variant, dtype):
-    """The two-pass form (variants 0 and 4: 8 and 16 items per thread) and each items-per-
-    thread variant of the one-pass form (pinned through the tuner) give the STL results,
-    across tile boundaries of every variant (1024 / 2048 / 4096 elements) and with runs of
-    equal values that cross tiles."""
+    """Every variant pinned through the tuner -- the warp-segment form (0 and 5: 16 and 8
+    items per thread, fewer where a tile's window would not fit), the one-pass form (1, 2,
+    3) and the two-pass form (4 and 6: 16 and 8) -- gives the STL results, across tile
+    boundaries of every variant (1024 / 2048 / 4096 elements) and with runs of equal values
+    that cross warp segments and tiles."""
     try:
         R.tune_force(2, variant)
         rng = np.random.default_rng(variant * 10 + np.dtype(dtype).itemsize)
@@ -124,6 +125,40 @@ def test_set_filter_variants(cuda, variant, dtype):
             for op, ref in ((R.SET_UNION, O.set_union), (R.SET_DIFFERENCE, O.set_difference),
                             (R.SET_INTERSECTION, O.set_intersection)):
                 assert np.array_equal(to_np(R.set_op(op, da, db)), ref(a, b)), (op, na, nb)
+        assert R.device_status() == R.OK
+    finally:
+        R.tune_force(2, -1)
+
+
+@pytest.mark.parametrize("variant", [0, 5])
+def test_set_filter_segments_edges(cuda, variant):
+    """The warp-segment form on its edge cases: a run in B far longer than a tile's window
+    capacity (that tile's items search B in global memory), runs of one value across whole
+    tiles of A, many duplicates on both sides, inputs not 16-byte aligned (the two-pass form
+    takes those) and an empty B, with B shorter and longer than A; every result is the STL
+    one."""
+    try:
+        R.tune_force(2, variant)
+        rng = np.random.default_rng(50 + variant)
+        a = np.sort(np.concatenate([rng.integers(0, 1 << 20, 200_000), np.full(30_000, 777_777)])).astype(np.uint32)
+        b = np.sort(np.concatenate([rng.integers(0, 1 << 20, 50_000), np.full(60_000, 777_777),
+                                    np.full(9_000, 5)])).astype(np.uint32)
+        a2 = np.sort(np.concatenate([rng.integers(0, 1 << 20, 500_000), np.full(30_000, 777_777)])).astype(np.uint32)
+        b2 = np.sort(np.concatenate([rng.integers(0, 1 << 20, 20_000), np.full(60_000, 777_777),
+                                     np.full(9_000, 5)])).astype(np.uint32)
+        a3 = np.sort(rng.integers(0, 300, 100_000)).astype(np.uint32)
+        b3 = np.sort(rng.integers(0, 300, 20_000)).astype(np.uint32)
+        cases = [(a, b), (a[3:], b[1:]), (a, b[:0]), (np.full(20_000, 9, np.uint32), np.full(7_001, 9, np.uint32)),
+                 (a2, b2), (a3, b3), (a3.astype(np.uint64), b3.astype(np.uint64)), (b2, a2)]
+        for x, y in cases:
+            dx, dy = _dev(x, cuda), _dev(y, cuda)
+            for op, ref in ((R.SET_UNION, O.set_union), (R.SET_DIFFERENCE, O.set_difference),
+                            (R.SET_INTERSECTION, O.set_intersection)):
+                assert np.array_equal(to_np(R.set_op(op, dx, dy)), ref(x, y)), (op, len(x), len(y))
+        # misaligned views of the same arrays
+        da, db = _dev(a, cuda), _dev(b, cuda)
+        for op, ref in ((R.SET_DIFFERENCE, O.set_difference), (R.SET_INTERSECTION, O.set_intersection)):
+            assert np.array_equal(to_np(R.set_op(op, da[1:], db[3:])), ref(a[1:], b[3:]))
         assert R.device_status() == R.OK
     finally:
         R.tune_force(2, -1)

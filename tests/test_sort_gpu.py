@@ -173,3 +173,43 @@ def test_sort_unaligned_slice_uses_per_tile_pass(cuda):
     R.sort_pairs(sub, begin_bit=0, end_bit=64)
     assert np.array_equal(to_np(sub), O.sort_pairs(keys[1:], begin_bit=0, end_bit=64))
     assert torch.equal(d[0], _dev(keys[0], cuda))
+
+
+@pytest.mark.parametrize("kb,vb,begin,end", [(4, 0, 0, 8), (4, 0, 0, 16), (8, 8, 8, 32), (16, 0, 64, 96),
+                                             (8, 4, 0, 64), (16, 16, 0, 128), (64, 0, 0, 200)])
+@pytest.mark.parametrize("n", [1, 33, 100003])
+def test_sort_from_leaves_input_and_matches_in_place(cuda, kb, vb, begin, end, n):
+    """rfx_sort_pairs_from sorts the input into other buffers (one to four passes, values,
+    keys over 128 bits) with the in-place sort's result and leaves the input as it was."""
+    import torch
+    keys = _keys(n, kb, seed=kb + vb + n + end)
+    vals = _keys(n, vb, seed=7 + n) if vb else None
+    dk = _dev(keys, cuda)
+    dv = _dev(vals, cuda) if vb else None
+    ok, ov = R.sorted_copy(dk, dv, begin_bit=begin, end_bit=end)
+    assert np.array_equal(to_np(dk), keys)
+    if vb:
+        assert np.array_equal(to_np(dv), vals)
+    ek = _dev(keys, cuda)
+    ev = _dev(vals, cuda) if vb else None
+    R.sort_pairs(ek, ev, begin_bit=begin, end_bit=end)
+    assert torch.equal(ok, ek)
+    if vb:
+        assert torch.equal(ov, ev)
+    assert R.device_status() == R.OK
+
+
+def test_sort_from_all_trivial_and_overlap(cuda):
+    """Every digit constant with the skip flag: the output is a copy of the input.  Input
+    and output overlapping: rejected."""
+    import torch
+    keys = np.zeros((5000, 4), np.uint8)
+    keys[:, 0] = np.arange(5000) % 256
+    dk = _dev(keys, cuda)
+    out = torch.empty_like(dk)
+    s = R.Sorter(5000, 4, 0, 8, 32, device=cuda)
+    s(out, None, 1, None, src_keys=dk)
+    assert np.array_equal(to_np(out), keys)
+    st = R.LIB.rfx_sort_pairs_from(R._ptr(dk), None, R._ptr(dk[100:]), None, 4000, 4, 0, 0, 32, 0, R._ptr(s.ws), s.wsb,
+                                   R._stream())
+    assert st == R.ERR_INVALID

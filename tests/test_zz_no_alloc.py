@@ -37,9 +37,8 @@ def _free_bytes():
 
 def _noalloc(fa, rows, n, expect_error=0):
     """One call of the no-allocation entry with fa's descriptors; returns host results.
-    After the first call on a device (which looks the array's address up, and may make
-    the CUDA runtime load the library's module that holds it), a call must not change the
-    device's free memory."""
+    After the first call on a device (which looks the array's address up and loads every
+    kernel the entry can launch), a call must not change the device's free memory."""
     import torch
     dev = rows.device
     keys = torch.full((fa.G,), -1, dtype=torch.int64, device=dev)

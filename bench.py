@@ -554,6 +554,23 @@ def _op_join(ctx, peak, reps):
         R.tune_force(1, -1)
     ops["reduce_by_key_19M_rows_tile_lookback"] = _op_line(total, total * 16 + groups * 16, ms, peak, groups=groups,
                                                            note="look-back per 256-line tile (tuner variant 2)")
+    # dense groups: 60M 16-byte rows (key U[0, 6M) at bits 64..95, 64-bit value), sorted on
+    # the key, about 10 rows per group (the group density of the batched plan's reduce)
+    dense = R.gen_uniform_rows(60_000_000, [32, 64], 0x5EED0301, [0, 100], [6_000_000, 10_000_000], device=ctx.dev)
+    R.sort_pairs(dense, begin_bit=64, end_bit=96)
+    dn = dense.shape[0]
+    dkeys = torch.empty(dn, dtype=torch.int32, device=ctx.dev)
+    dsum = torch.empty(dn, dtype=torch.int64, device=ctx.dev)
+    dcnt = torch.empty(dn, dtype=torch.int32, device=ctx.dev)
+    dwsb = R.LIB.rfx_reduce_by_key_workspace(dn)
+    dws = R._empty_bytes(dwsb, ctx.dev)
+    ms = _time_ms(lambda: R.check("rt", R.LIB.rfx_reduce_tuples(R._ptr(dense), dn, None, 16, 64, 0, 64, R._ptr(dkeys), 4,
+                                                                R._ptr(dsum), R._ptr(dcnt), R._ptr(g), R._ptr(dws), dwsb,
+                                                                R._stream())), reps)
+    dg = int(g.item())
+    ops["reduce_by_key_60M_rows_dense_groups"] = _op_line(dn, dn * 16 + dg * 16, ms, peak, groups=dg,
+                                                          note="about 10 rows per group; inputs larger than L2")
+    del dense, dkeys, dsum, dcnt, dws
     # join + aggregate on the key as one operator (no join rows)
     ja = R.JoinAggregate(nr, 4, device=ctx.dev)
     ms = _time_ms(lambda: ja(rs, 32, ss, 64, 0, 64), reps)

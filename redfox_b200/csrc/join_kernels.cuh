@@ -73,9 +73,9 @@ __device__ __forceinline__ uint64_t block_exclusive_u64(uint64_t x, uint64_t* s_
 
 // Right-side keys a block's left keys can match, staged in dynamic shared memory of
 // FindBoundsArgs::window_bytes (at most kFbWindowBytes): u32 keys when the right
-// container has at most 4 bytes, u64 when the key (container >> shift) has at most 64
-// bits, u128 otherwise.  A window that does not fit falls back to searches in global
-// memory.
+// container has at most 4 bytes (or, for the join-aggregate, its key (container >> shift)
+// at most 32 bits), u64 when the key has at most 64 bits, u128 otherwise.  A window that
+// does not fit falls back to searches in global memory.
 constexpr uint32_t kFbWindowBytes = 64 * 1024;
 
 // First index in [lo, n) of the sorted window with w[i] >= k (strict: > k).
@@ -114,7 +114,13 @@ __global__ void __launch_bounds__(kJoinThreads) find_bounds_kernel(const FindBou
   using W = std::conditional_t<(RE <= 4), uint32_t, uint64_t>;
   W* s_win = reinterpret_cast<W*>(fb_window);
   u128* s_win128 = reinterpret_cast<u128*>(fb_window);
+  uint32_t* s_win32 = reinterpret_cast<uint32_t*>(fb_window);
   const bool narrow = RE <= 4 || (uint32_t)RE * 8u - a.rshift <= 64u;
+  // the join-aggregate's wider containers whose key (container >> shift) has at most 32
+  // bits: a u32 window, twice the keys in the same shared memory (its window is the
+  // largest one, sized without the group count; the plain find_bounds sizes its window
+  // from the two sides' lengths and keeps the wider type, which measured faster there)
+  const bool n32 = GROUP && RE > 4 && (uint32_t)RE * 8u - a.rshift <= 32u;
   const uint64_t WB = a.window_bytes;
   __shared__ uint64_t s_warp[kJoinThreads / 32];
   __shared__ uint64_t s_prefix;
@@ -145,9 +151,12 @@ __global__ void __launch_bounds__(kJoinThreads) find_bounds_kernel(const FindBou
     }
     __syncthreads();
     const uint64_t wlo = s_lo, wn = s_hi > s_lo ? s_hi - s_lo : 0;
-    const bool staged = wn * (narrow ? sizeof(W) : 16u) <= WB;
+    const bool staged = wn * (n32 ? 4u : narrow ? sizeof(W) : 16u) <= WB;
     // a few loads in flight per thread while staging (one round trip per key otherwise)
-    if (staged && narrow)
+    if (staged && n32)
+      block_stage<8>(wn, t, kJoinThreads, [&](uint64_t x) { return (uint32_t)R.key(wlo + x); },
+                     [&](uint64_t x, uint32_t v) { s_win32[x] = v; });
+    else if (staged && narrow)
       block_stage<(sizeof(W) == 4 ? 8 : 4)>(wn, t, kJoinThreads, [&](uint64_t x) { return (W)R.key(wlo + x); },
                                              [&](uint64_t x, W v) { s_win[x] = v; });
     else if (staged)
@@ -179,7 +188,16 @@ __global__ void __launch_bounds__(kJoinThreads) find_bounds_kernel(const FindBou
         // the thread's keys ascend: the first is searched in the whole window, the next
         // ones gallop forward from the previous key's upper bound
         const uint32_t from = j == 0 ? 0u : (uint32_t)(phi - wlo);
-        if (staged && narrow) {
+        if (staged && n32) {
+          if ((k >> 32) != 0) {
+            l = h = wlo + wn;
+          } else {
+            const uint32_t lw = j == 0 ? smem_bound_t<false>(s_win32, 0u, (uint32_t)wn, (uint32_t)k)
+                                       : smem_gallop_t<false>(s_win32, from, (uint32_t)wn, (uint32_t)k);
+            l = wlo + lw;
+            h = wlo + smem_gallop_t<true>(s_win32, lw, (uint32_t)wn, (uint32_t)k);
+          }
+        } else if (staged && narrow) {
           // compares in the window's type (a larger left key lies above the whole window)
           if ((k >> (8 * sizeof(W))) != 0) {
             l = h = wlo + wn;

@@ -313,6 +313,15 @@ rfx_status launch_chunks(const void* rows, uint64_t n, const RowReduceArgs& a, c
 // sub-chunk of whole tiles.
 constexpr int kWarpChunkWarps = 8;
 constexpr int kWarpChunkStages = 3;
+// On inputs above kWarpChunkSpreadBytes, tiles of a warp's sub-chunk at the most (256 KB),
+// unless that would take more than kMaxChunks chunks: one sub-chunk per resident warp spreads
+// the warps streaming at once over the whole input, a page apart each, and on inputs of many
+// GB the address translations miss (a 10 GB reduce ran at half speed); smaller sub-chunks,
+// claimed in order, keep them within a few hundred MB.  Below that size the per-chunk costs
+// of smaller sub-chunks outweigh it (a 0.96 GB reduce: 0.35 ms with one sub-chunk per warp,
+// 0.44 ms with 256 KB ones).
+constexpr uint64_t kWarpChunkMaxTiles = 64;
+constexpr uint64_t kWarpChunkSpreadBytes = 2ull << 30;
 
 template <int RB, int SHAPE>
 rfx_status launch_warps(const void* rows, uint64_t n, const RowReduceArgs& a, const ChunkLayout& L,
@@ -333,6 +342,10 @@ rfx_status launch_warps(const void* rows, uint64_t n, const RowReduceArgs& a, co
   const uint64_t want = tiles ? (tiles + W - 1) / W : 1;
   const uint64_t grid = (uint64_t)persistent_grid((const void*)k, W * 32, smem, want);
   ca.tiles_per_chunk = tiles ? (tiles + grid * W - 1) / (grid * W) : 1;   // tiles per warp
+  if (n * RB > kWarpChunkSpreadBytes && ca.tiles_per_chunk > kWarpChunkMaxTiles) {
+    const uint64_t floor_tpc = (tiles + kMaxChunks * W - 1) / (kMaxChunks * W);
+    ca.tiles_per_chunk = floor_tpc > kWarpChunkMaxTiles ? floor_tpc : kWarpChunkMaxTiles;
+  }
   const uint64_t blocks = tiles ? (tiles + ca.tiles_per_chunk * W - 1) / (ca.tiles_per_chunk * W) : 1;
   if (blocks > kMaxChunks) return RFX_ERR_UNSUPPORTED;
   const uint64_t cap = L.slots / (blocks * W);

@@ -132,3 +132,22 @@ def test_noalloc_rejects_oversized_plan_like_the_workspace_entry(cuda):
         C.addressof(fa.sf), 3, out.data_ptr(), out.data_ptr(), out.data_ptr(), out.data_ptr(), ws.data_ptr(),
         ws.numel(), stream)
     assert st == st_ws == R.ERR_UNSUPPORTED
+
+
+def test_noalloc_second_device_after_first(cuda):
+    """A 1024-group plan (the shared-table kernel, more than 48 KB of dynamic shared memory)
+    on device 0, then on device 1: the shared-memory opt-in is made per device, so the second
+    device's launch succeeds and matches.  Needs two GPUs."""
+    import torch
+    if torch.cuda.device_count() < 2:
+        pytest.skip("needs two GPUs")
+    n = 200_000
+    widths = [8, 8, 32, 32]
+    for d in (0, 1):
+        with torch.cuda.device(d):
+            dev = torch.device("cuda:%d" % d)
+            rows = R.gen_uniform_rows(n, widths, 4321, [0, 0, 0, 0], [32, 32, 1000, 2**32], device=dev)
+            fa = R.FilterAggregate(n, widths, [(R.LT, (R.OPND_VAR, 2), (R.OPND_CONST, 900), R.I32)], [], [0, 1],
+                                   [32, 32], [2, 3], device=dev)
+            _compare(fa, rows, n)
+            torch.cuda.synchronize()

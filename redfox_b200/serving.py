@@ -330,23 +330,26 @@ def split_round(gk, gs, gc, nq, stream=None, stage=None, copy=True):
             for i in range(nq)]
 
 
-def run_round_host(res, queries, device="cuda", stream=None, stage=None, copy=True, batch_min=8):
+def run_round_host(res, queries, device="cuda", stream=None, stage=None, copy=True, batch_min=8, on_done=None):
     """A round end to end: lists generated, queries with and without a list run as two
     batched plans (the intersection applies to the first only), results on the host in
     the order of `queries` (copied out of `stage` unless copy=False).  A round of fewer than
     `batch_min` queries runs them one after another with the plain plan: a batched plan's
-    extra passes (the query byte in every key) cost more than a few queries share."""
+    extra passes (the query byte in every key) cost more than a few queries share; then
+    on_done(i, result), if given, is called as each query's result reaches the host."""
     import contextlib
 
     import numpy as np
     import torch
     if len(queries) < batch_min:
         outs, at = [], 0
-        for q in queries:
+        for i, q in enumerate(queries):
             with torch.cuda.stream(stream) if stream is not None else contextlib.nullcontext():
                 out = run_query(res, q, query_list(q, res.n2, device))
             k, sm, c = to_host(out, stream, stage, copy, at=at)
             outs.append((k.view(np.uint32), sm, c.view(np.uint32)))
+            if on_done is not None:
+                on_done(i, outs[-1])
             at += sum((t.numel() * t.element_size() + 255) // 256 * 256 for t in out)
         return outs
     res_by_q = [None] * len(queries)
@@ -395,7 +398,7 @@ class Server:
         per_query = 20 * min(self.STAGE_GROUPS_PER_QUERY, res.n2)
         self.stages = [PinnedStage(self.max_batch * per_query) for _ in range(slots)]
 
-    def _run(self, i, rnd, keep_results):
+    def _run(self, i, rnd, keep_results, on_done=None):
         import numpy as np
         if self.plain:
             q = rnd[0]
@@ -403,7 +406,7 @@ class Server:
             k, sm, c = to_host(run_query(self.res, q, lst), self.streams[i], self.stages[i], copy=keep_results)
             return [(k.view(np.uint32), sm, c.view(np.uint32))]
         return run_round_host(self.res, rnd, self.device, stream=self.streams[i], stage=self.stages[i],
-                              copy=keep_results)
+                              copy=keep_results, on_done=on_done)
 
     def serve(self, requests, keep_results=False):
         import torch
@@ -428,8 +431,16 @@ class Server:
                         if work[i] is None:
                             return
                         rnd = work[i]
+                    # a query of a small round (plain plans one after another) is done when
+                    # its own result is on the host; the others when the round's are
+                    early = {}
+
+                    def on_done(j, host, rnd=rnd, early=early):
+                        early[j] = time.perf_counter() - t0
+                        rnd[j].result = host if keep_results else (int(host[0].shape[0]),)
+
                     try:
-                        outs = self._run(i, rnd, keep_results)
+                        outs = self._run(i, rnd, keep_results, on_done)
                         for q, host in zip(rnd, outs):
                             q.result = host if keep_results else (int(host[0].shape[0]),)
                     except Exception as e:  # reported after the run
@@ -437,8 +448,8 @@ class Server:
                     done = time.perf_counter() - t0
                     with cv:
                         self.round_log.append((len(rnd), rnd[0].start, done))
-                        for q in rnd:
-                            q.done = done
+                        for j, q in enumerate(rnd):
+                            q.done = early.get(j, done)
                             sch.complete(q)
                         work[i] = None
                         busy[i] = False

@@ -15,10 +15,10 @@ struct FilterLayout {
   uint64_t* status;
   uint32_t* counter;
   uint64_t* split;   // 3 words per tile, and per tile boundary plus one (set_split_kernel, set_bounds_kernel)
-  uint8_t* mask;     // two-pass form: one bit per element
-  uint32_t* counts;  // two-pass form: kept elements per tile
+  uint8_t* mask;     // two-pass and warp-segment forms: one bit per element
+  uint32_t* counts;  // two-pass and warp-segment forms: kept elements per tile
   uint32_t* wcounts; // warp-segment form: kept elements per warp segment
-  uint64_t* offsets; // two-pass form: each tile's output offset
+  uint64_t* offsets; // two-pass and warp-segment forms: each tile's output offset
   size_t clear;
   size_t total;
 };

@@ -19,8 +19,9 @@
 namespace rfx {
 
 constexpr int kSetThreads = 256;
-// Items per thread: 8 by default, 4 and 16 as the tuner's alternatives (unique always 8);
-// elements up to 8 bytes live in 64-bit registers.
+// Items per thread of the one-pass and two-pass forms: 8, with 4 and 16 as the tuner's
+// alternatives (unique always 8); elements up to 8 bytes live in 64-bit registers.  The
+// warp-segment form takes 16 (8 or 4 where a tile's window would not fit).
 constexpr int kSetIPT = 8;
 constexpr int kSetTile = kSetThreads * kSetIPT;
 constexpr int kSetTileMin = kSetThreads * 4;   // the smallest tile: workspace sizing
@@ -41,7 +42,7 @@ struct SetFilterArgs {
   uint64_t nb;
   const uint8_t* prev;   // KEEP_HEADS: element before each tile (saved before in-place writes)
   const uint64_t* split; // KEEP_(UN)MATCHED: per tile (run start of its first element, B window)
-  uint32_t wcap;         // two-pass form: B window capacity (elements of dynamic shared memory)
+  uint32_t wcap;         // two-pass and warp-segment forms: B window capacity (elements of dynamic shared memory)
   uint8_t* out;
   uint64_t* d_count;
   uint64_t* status;

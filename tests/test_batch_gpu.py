@@ -70,3 +70,19 @@ def test_graph_replay_reproduces_eager(cuda):
         k1, s1, c1, t1 = plan.result()
         assert t1 == t0
         assert torch.equal(k1, k0) and torch.equal(s1, s0) and torch.equal(c1, c0)
+
+
+def test_split_by_query_on_host_tensors():
+    """Groups ordered by (key, query) -- what the stable sort on the key bits leaves -- split
+    into per-query groups in key order, the query bits removed (host tensors, no GPU)."""
+    import torch
+    pairs = sorted([(k, q) for k in (3, 9, 1 << 20, (1 << 21) - 1) for q in (0, 2, 5)])
+    keys = torch.tensor([B.fold(k, q) for k, q in pairs], dtype=torch.int64).to(torch.int32)
+    sums = torch.arange(len(pairs), dtype=torch.int64)
+    counts = torch.arange(len(pairs), dtype=torch.int32) + 1
+    per = B.split_by_query(keys, sums, counts, 6)
+    for q in range(6):
+        k, s, c = per[q]
+        want = [i for i, (_, qq) in enumerate(pairs) if qq == q]
+        assert k.tolist() == [pairs[i][0] for i in want]
+        assert s.tolist() == want and c.tolist() == [i + 1 for i in want]
